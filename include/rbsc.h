@@ -1,0 +1,201 @@
+/*
+ * rbsc.h -- C ABI of librbsc, a B200 (sm_100a) implementation of rbsc's
+ * colour-refinement hot path: the coarsest backward-equivalence (lumpable)
+ * partition of a weighted directed graph, i.e. 1-WL colour refinement over
+ * successor multisets.
+ *
+ * The reference exposes this path only as a process (src/rbsc/rbsc.cu:182-497:
+ * arcs-cuda text on stdin, `rbsc [edge_batch_size] [gpus]`, three lines on
+ * stdout).  The entry points below are what that process is made of, split at
+ * the places a caller binding the path through an FFI needs; each one names
+ * the part of the reference it replaces.  The `rbsc` CLI built from
+ * rbsc_b200/csrc/cli.cpp keeps the reference's process surface on top of them.
+ *
+ * Conventions
+ *   - Plain C types only; no exceptions cross the ABI.
+ *   - Every call that can fail returns an rbsc_status (0 = OK, < 0 = error);
+ *     rbsc_last_error(ctx) gives the message of the last failure on that
+ *     context (ctx may be NULL for failures of rbsc_ctx_create).
+ *   - Host pointers are owned by the caller.  Device memory is owned by the
+ *     library (per context / per graph) unless a function says otherwise.
+ *   - A context is used by one host thread at a time; different contexts may
+ *     be used concurrently.
+ *   - Graph: N nodes (N < 2^31), M arcs, CSR where row u lists the heads v of
+ *     the arcs (u, wt, v) -- the reference's arcs grouped by their start
+ *     (rbsc.cu:168-180 requires that grouping).  Weights are optional uint64
+ *     (absent = 1), summed modulo 2^64 (rbsc.cu:173, 80-87).
+ *   - Output labels are canonical: each node carries the smallest node id of
+ *     its block.
+ */
+#ifndef RBSC_H
+#define RBSC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RBSC_ABI_VERSION 1
+
+typedef int32_t rbsc_status;
+#define RBSC_OK 0
+#define RBSC_ERR_INVALID (-1)        /* bad argument / malformed graph           */
+#define RBSC_ERR_CUDA (-2)           /* a CUDA runtime call failed               */
+#define RBSC_ERR_OOM (-3)            /* device or pinned memory exhausted        */
+#define RBSC_ERR_NOT_CONVERGED (-4)  /* max_rounds passes without a fixpoint     */
+#define RBSC_ERR_DEVICE (-5)         /* a kernel reported an error flag          */
+#define RBSC_ERR_PARSE (-6)          /* malformed arcs-cuda text                 */
+#define RBSC_ERR_TOO_LARGE (-7)      /* N >= 2^31 or a size beyond a stated limit */
+#define RBSC_ERR_BUSY (-8)           /* serving: admission queue full            */
+
+typedef struct rbsc_ctx rbsc_ctx;
+typedef struct rbsc_graph rbsc_graph;
+
+/* Relabel strategies for the per-round "(old colour, signature) -> new colour"
+ * step (reference: the two radix sorts + scan of rbsc.cu:384-396). */
+#define RBSC_RELABEL_HASH 0   /* lock-free hash table, one probe per node (default) */
+#define RBSC_RELABEL_SORT 1   /* hand-written LSD radix sort of (colour, signature, node) */
+
+typedef struct {
+    int32_t relabel;          /* RBSC_RELABEL_*                                          */
+    int32_t verify;           /* 1 (default): exact collision check at every fixpoint   */
+    uint32_t max_rounds;      /* 0 = no limit beyond N + 1                               */
+    int32_t use_graph;        /* 1 (default): round loop as one CUDA graph with a
+                                 device-side while node; 0 = host-driven loop           */
+    uint64_t seed;            /* hash salt seed                                          */
+    int32_t test_hash_bits;   /* TEST HOOK: keep only the low k bits of every signature
+                                 (0 = off).  Forces hash collisions so the exact check
+                                 and repair path can be exercised.                      */
+    int32_t reserved[7];
+} rbsc_opts;
+
+typedef struct {
+    uint32_t rounds;          /* signature passes until the block count stopped
+                                 changing (count before pass 1 = #distinct initial
+                                 colours; rbsc.cu:339, 354-425)                         */
+    uint32_t blocks;          /* blocks of the final partition (rbsc.cu:494 "nodes")   */
+    uint32_t done;            /* 1 = coarsest partition (rbsc.cu:493)                   */
+    uint32_t verified;        /* 1 = the exact stability check passed                   */
+    uint32_t repairs;         /* exact-check failures that were split and re-refined   */
+    uint32_t initial_blocks;  /* distinct initial colours                               */
+    double time_s;            /* wall time of the call, as rbsc.cu:272-490 measures it */
+    double device_ms;         /* device time of the refinement (CUDA events)            */
+    double verify_ms;         /* device time of the exact check(s)                       */
+    double h2d_ms;            /* host->device copies inside the call                    */
+    double d2h_ms;            /* device->host copies inside the call                    */
+    uint64_t h2d_bytes;
+    uint64_t d2h_bytes;
+    uint32_t round_blocks[64];/* block count before pass 1 and after passes 1..63       */
+    uint64_t kernel_launches; /* kernels of this library launched by the call            */
+} rbsc_stats;
+
+/* Per-kernel device time of one refinement, measured with CUDA events around
+ * every launch on the library's stream (host-driven loop, same kernels and
+ * same work as the graph-captured loop). */
+typedef struct {
+    uint32_t passes;          /* hashed passes timed                                     */
+    double signature_ms;      /* total over the passes: k_signature                     */
+    double insert_ms;         /* k_insert (or the sort-based relabel's sorts)            */
+    double relabel_ms;        /* k_relabel                                               */
+    double other_ms;          /* table clear + fixpoint kernels                          */
+    double total_ms;          /* whole refinement, including the exact check             */
+} rbsc_kernel_times;
+
+/* A CSR graph.  `offsets` has n+1 entries of `offset_bytes` (4 or 8) bytes;
+ * `indices` has m entries; `weights` is NULL or has m entries. */
+typedef struct {
+    uint32_t n;
+    uint64_t m;
+    const void* offsets;
+    int32_t offset_bytes;
+    const uint32_t* indices;
+    const uint64_t* weights;
+} rbsc_csr;
+
+/* A host CSR owned by the library (filled by the parser and the generators). */
+typedef struct {
+    uint32_t n;
+    uint64_t m;
+    uint64_t* offsets;        /* n+1 */
+    uint32_t* indices;        /* m   */
+    uint64_t* weights;        /* m, or NULL when every weight is 1 */
+} rbsc_host_graph;
+
+/* ---- library / context --------------------------------------------------- */
+
+int32_t rbsc_abi_version(void);
+void rbsc_opts_default(rbsc_opts* opts);
+
+/* Creates a context on CUDA device `device` (replaces the per-GPU setup of
+ * rbsc.cu:234-270).  Returns NULL on failure; see rbsc_last_error(NULL). */
+rbsc_ctx* rbsc_ctx_create(int32_t device, const rbsc_opts* opts);
+void rbsc_ctx_destroy(rbsc_ctx* ctx);
+const char* rbsc_last_error(const rbsc_ctx* ctx);
+rbsc_status rbsc_ctx_set_opts(rbsc_ctx* ctx, const rbsc_opts* opts);
+
+/* ---- one-shot refinement (the reference's whole single-batch path) -------- */
+
+/* Refines a host CSR: copies it to the device, refines to the fixpoint,
+ * checks the result exactly, copies the labels back.  Replaces rbsc.cu:341-445
+ * (H2D, round loop, D2H, host relabel) for edge_batch_size >= M.
+ * init_colors: NULL (one initial block) or n uint32 colours (any values).
+ * out_labels: NULL or n uint32 (canonical labels).  stats: NULL or filled. */
+rbsc_status rbsc_refine(rbsc_ctx* ctx, const rbsc_csr* host_graph, const uint32_t* init_colors,
+                        uint32_t* out_labels, rbsc_stats* stats);
+
+/* ---- resident graphs ---------------------------------------------------- */
+
+/* Copies a host CSR to the device and builds the per-graph tiling once
+ * (replaces rbsc.cu:341-344 and the per-batch setup of 345-352). */
+rbsc_status rbsc_graph_upload(rbsc_ctx* ctx, const rbsc_csr* host_graph, rbsc_graph** out);
+/* Same from a CSR already in device memory (pointers into this context's
+ * device); the arrays are copied, the caller keeps ownership of its own. */
+rbsc_status rbsc_graph_from_device(rbsc_ctx* ctx, const rbsc_csr* device_graph, rbsc_graph** out);
+void rbsc_graph_free(rbsc_graph* g);
+rbsc_status rbsc_graph_info(const rbsc_graph* g, uint32_t* n, uint64_t* m);
+/* Device pointers of the resident CSR (offsets are uint64). */
+rbsc_status rbsc_graph_device_csr(const rbsc_graph* g, const uint64_t** d_offsets,
+                                  const uint32_t** d_indices);
+
+/* Refines a resident graph; init/out are HOST pointers (either may be NULL). */
+rbsc_status rbsc_graph_refine(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* init_colors,
+                              uint32_t* out_labels, rbsc_stats* stats);
+/* Refines a resident graph; init/out are DEVICE pointers (either may be NULL).
+ * No host<->device copies of graph-sized data happen inside this call. */
+rbsc_status rbsc_graph_refine_device(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init_colors,
+                                     uint32_t* d_out_labels, rbsc_stats* stats);
+/* Measurement entry point (no counterpart in the reference, which times the
+ * whole run with std::chrono, rbsc.cu:272, 489-490): refines like
+ * rbsc_graph_refine_device, with CUDA events around every kernel launch. */
+rbsc_status rbsc_graph_profile(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init_colors,
+                               rbsc_kernel_times* times, rbsc_stats* stats);
+/* Initial colours floor(log2(out_degree + 1)) written to d_colors (n uint32),
+ * computed on the device from the resident offsets. */
+rbsc_status rbsc_graph_degree_colors(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* d_colors);
+
+/* ---- input formats (reference: read_graph, rbsc.cu:156-180) -------------- */
+
+/* Parses arcs-cuda text ("N\nM\n" + M lines "u wt v", arcs grouped by u;
+ * webgraph-rs cli/src/to/arcscuda.rs:61-66) into a host CSR.  Unlike the
+ * reference reader it stops at end of input, rejects non-digits, out-of-range
+ * node ids, fewer than M arcs and arcs not grouped by source. */
+rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_graph* out);
+void rbsc_host_graph_free(rbsc_host_graph* g);
+
+/* ---- synthetic workloads (stand-ins for the reference's LAW graphs) ------ */
+
+/* Directed R-MAT: 2^scale nodes, edge_factor * 2^scale generated arcs with
+ * quadrant probabilities (a, b, c, 1-a-b-c); duplicates and self-loops removed;
+ * rows sorted.  Counter-based: the same (scale, ef, a, b, c, seed) gives the
+ * same graph on the host and on the device. */
+rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_factor, double a,
+                                 double b, double c, uint64_t seed, rbsc_graph** out);
+rbsc_status rbsc_gen_rmat_host(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                               uint64_t seed, int32_t threads, rbsc_host_graph* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RBSC_H */

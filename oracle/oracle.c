@@ -1,0 +1,305 @@
+/*
+ * oracle.c -- CPU restatement of rbsc's colour-refinement path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker that the CUDA product
+ * path is compared against; nothing in the product (librbsc, the CLI, the
+ * Python package) links, loads or calls it.  Only tests/, the smoke check and
+ * the CPU-baseline leg of bench.py use it.
+ *
+ * Parity status: pinned.  Its results are checked against the outputs of the
+ * reference programs themselves (src/rsc/rsc.cpp and the Valmari minimiser in
+ * src/part_ref, compiled unmodified from their sources by oracle/Makefile) on
+ * the fixtures in tests/golden/.
+ *
+ * Problem (src/part_ref/MDP_minimize.cc:56-64, src/rsc/rsc.cpp:71-144):
+ * a graph is a list of weighted arcs (u, wt, v) grouped by u (CSR row u = the
+ * arcs whose start is u).  Two nodes are equivalent iff they are in the same
+ * block of the current partition and, for every block C, the sums of the
+ * weights of their arcs into C are equal.  The result is the coarsest stable
+ * refinement of the initial partition (all nodes in one block unless initial
+ * colours are given).
+ *
+ * Two restatements live here:
+ *   orc_refine_exact  -- exact refinement: each round every node's signature
+ *                        is (old block, sorted list of (successor block,
+ *                        summed weight)), compared exactly, never hashed.
+ *   orc_refine_rsc    -- the reference CPU program's own randomised loop
+ *                        (rsc.cpp:63-144): hashed sums, lexicographic sort of
+ *                        (sum, old colour), dense ranks, stop when the block
+ *                        count stops changing.
+ *
+ * Labels returned by both are canonical: every node is labelled with the
+ * smallest node id of its block.
+ *
+ * Round count, "GPU convention" (src/rbsc/rbsc.cu:339, 354-425): rounds =
+ * number of signature passes until a pass leaves the block count unchanged,
+ * the count before the first pass being the number of distinct initial
+ * colours.  rsc.cpp:104-144 starts its count at N instead; orc_refine_rsc
+ * reports both.
+ */
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+
+/* ------------------------------------------------------------------ */
+/* index merge sort with a context comparator (stable)                 */
+/* ------------------------------------------------------------------ */
+typedef int (*orc_cmp_fn)(uint32_t a, uint32_t b, const void* ctx);
+
+static void msort_idx(uint32_t* a, uint32_t* tmp, size_t n, orc_cmp_fn cmp, const void* ctx)
+{
+    for (size_t width = 1; width < n; width *= 2) {
+        for (size_t lo = 0; lo < n; lo += 2 * width) {
+            size_t mid = lo + width < n ? lo + width : n;
+            size_t hi = lo + 2 * width < n ? lo + 2 * width : n;
+            size_t i = lo, j = mid, k = lo;
+            while (i < mid && j < hi) {
+                if (cmp(a[j], a[i], ctx) < 0) tmp[k++] = a[j++];
+                else tmp[k++] = a[i++];
+            }
+            while (i < mid) tmp[k++] = a[i++];
+            while (j < hi) tmp[k++] = a[j++];
+        }
+        memcpy(a, tmp, n * sizeof(uint32_t));
+    }
+}
+
+/* ------------------------------------------------------------------ */
+/* canonical labels                                                    */
+/* ------------------------------------------------------------------ */
+
+/* ctx points at a `const uint32_t*` label array */
+static int cmp_lab(uint32_t a, uint32_t b, const void* ctx)
+{
+    const uint32_t* l = *(const uint32_t* const*)ctx;
+    return l[a] < l[b] ? -1 : (l[a] > l[b] ? 1 : 0);
+}
+
+/* Relabel an arbitrary labelling so that each block carries the smallest node
+ * id in it.  Labels may be any uint32 values.  Returns the number of blocks. */
+uint32_t orc_canonicalize(uint32_t n, const uint32_t* in, uint32_t* out)
+{
+    if (n == 0) return 0;
+    uint32_t* ord = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* tmp = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+    /* sort node ids by label, stable -> first of each run is the minimum */
+    const uint32_t* c = in;
+    msort_idx(ord, tmp, n, cmp_lab, &c);
+    uint32_t blocks = 0, rep = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        if (i == 0 || in[ord[i]] != in[ord[i - 1]]) { rep = ord[i]; ++blocks; }
+        out[ord[i]] = rep;
+    }
+    free(ord); free(tmp);
+    return blocks;
+}
+
+/* ------------------------------------------------------------------ */
+/* exact refinement                                                    */
+/* ------------------------------------------------------------------ */
+typedef struct {
+    const uint32_t* cur;     /* old labels                               */
+    const uint64_t* sstart;  /* per node: start of its compressed list   */
+    const uint32_t* slen;    /* per node: number of (label, weight) runs */
+    const uint32_t* slab;    /* run labels                               */
+    const uint64_t* swt;     /* run weight sums (mod 2^64)               */
+} exact_ctx;
+
+static int cmp_exact(uint32_t a, uint32_t b, const void* vctx)
+{
+    const exact_ctx* c = (const exact_ctx*)vctx;
+    if (c->cur[a] != c->cur[b]) return c->cur[a] < c->cur[b] ? -1 : 1;
+    if (c->slen[a] != c->slen[b]) return c->slen[a] < c->slen[b] ? -1 : 1;
+    const uint32_t* la = c->slab + c->sstart[a];
+    const uint32_t* lb = c->slab + c->sstart[b];
+    const uint64_t* wa = c->swt + c->sstart[a];
+    const uint64_t* wb = c->swt + c->sstart[b];
+    for (uint32_t i = 0; i < c->slen[a]; ++i) {
+        if (la[i] != lb[i]) return la[i] < lb[i] ? -1 : 1;
+        if (wa[i] != wb[i]) return wa[i] < wb[i] ? -1 : 1;
+    }
+    return 0;
+}
+
+typedef struct { uint32_t lab; uint64_t w; } lw_pair;
+
+static int cmp_lw(const void* x, const void* y)
+{
+    const lw_pair* a = (const lw_pair*)x;
+    const lw_pair* b = (const lw_pair*)y;
+    return a->lab < b->lab ? -1 : (a->lab > b->lab ? 1 : 0);
+}
+
+/*
+ * Exact coarsest stable refinement.
+ *   off[n+1], idx[m]: CSR (row u = successors of u), wt[m] optional (NULL =
+ *   unit weights), init[n] optional initial colours (NULL = one block).
+ *   labels_out[n]: canonical labels (min node id per block).
+ *   round_blocks (optional, max_rounds+1 entries): block count before the
+ *   first pass (index 0) and after every pass.
+ * Returns 0, or -1 if max_rounds passes did not reach a fixpoint.
+ */
+int orc_refine_exact(uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt,
+                     const uint32_t* init, uint32_t* labels_out, uint32_t* rounds_out,
+                     uint32_t* blocks_out, uint32_t* round_blocks, uint32_t max_rounds)
+{
+    *rounds_out = 0; *blocks_out = 0;
+    if (n == 0) { if (round_blocks) round_blocks[0] = 0; return 0; }
+    uint64_t m = off[n];
+    uint32_t* cur = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* nxt = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* ord = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* tmp = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint64_t* sstart = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    uint32_t* slen = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* slab = (uint32_t*)malloc(sizeof(uint32_t) * (m ? m : 1));
+    uint64_t* swt = (uint64_t*)malloc(sizeof(uint64_t) * (m ? m : 1));
+    lw_pair* row = (lw_pair*)malloc(sizeof(lw_pair) * (m ? m : 1));
+
+    uint32_t prev;
+    if (init) prev = orc_canonicalize(n, init, cur);
+    else { for (uint32_t i = 0; i < n; ++i) cur[i] = 0; prev = 1; }
+    if (round_blocks) round_blocks[0] = prev;
+
+    int status = -1;
+    uint32_t r = 0;
+    while (r < max_rounds) {
+        /* compressed, sorted successor-block lists */
+        for (uint32_t u = 0; u < n; ++u) {
+            uint64_t b = off[u], e = off[u + 1], d = e - b;
+            for (uint64_t k = 0; k < d; ++k) {
+                row[k].lab = cur[idx[b + k]];
+                row[k].w = wt ? wt[b + k] : 1u;
+            }
+            qsort(row, (size_t)d, sizeof(lw_pair), cmp_lw);
+            uint32_t len = 0;
+            sstart[u] = b;
+            for (uint64_t k = 0; k < d;) {
+                uint32_t lab = row[k].lab;
+                uint64_t s = 0;
+                while (k < d && row[k].lab == lab) { s += row[k].w; ++k; }
+                if (s != 0) { slab[b + len] = lab; swt[b + len] = s; ++len; }
+            }
+            slen[u] = len;
+        }
+        exact_ctx c = { cur, sstart, slen, slab, swt };
+        for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+        msort_idx(ord, tmp, n, cmp_exact, &c);
+        uint32_t blocks = 0, rep = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i == 0 || cmp_exact(ord[i - 1], ord[i], &c) != 0) { rep = ord[i]; ++blocks; }
+            nxt[ord[i]] = rep;
+        }
+        ++r;
+        if (round_blocks) round_blocks[r] = blocks;
+        uint32_t* sw = cur; cur = nxt; nxt = sw;
+        if (blocks == prev) { status = 0; break; }
+        prev = blocks;
+    }
+    memcpy(labels_out, cur, sizeof(uint32_t) * n);
+    *rounds_out = r;
+    *blocks_out = orc_canonicalize(n, cur, labels_out);
+    free(cur); free(nxt); free(ord); free(tmp); free(sstart); free(slen);
+    free(slab); free(swt); free(row);
+    return status;
+}
+
+/* ------------------------------------------------------------------ */
+/* restatement of the reference CPU loop (rsc.cpp)                     */
+/* ------------------------------------------------------------------ */
+
+/* rsc.cpp:63-69: bijective 64-bit mixer (SplitMix64 finaliser, then x5,
+ * rotate left by 7, x9). */
+uint64_t orc_rsc_randomize(uint64_t z)
+{
+    z += 0x9e3779b97f4a7c15ULL;
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ULL;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebULL;
+    z = (z ^ (z >> 31)) * 5u;
+    return ((z << 7) | (z >> 57)) * 9u;
+}
+
+typedef struct { const uint64_t* z; const uint64_t* w; } rsc_ctx;
+
+static int cmp_rsc(uint32_t a, uint32_t b, const void* vctx)
+{
+    const rsc_ctx* c = (const rsc_ctx*)vctx;
+    if (c->z[a] != c->z[b]) return c->z[a] < c->z[b] ? -1 : 1;
+    if (c->w[a] != c->w[b]) return c->w[a] < c->w[b] ? -1 : 1;
+    return 0;
+}
+
+/*
+ * rsc.cpp:103-144 restated: w = 1 for every node (or the dense rank of the
+ * given initial colour), z = 0; each round z[u] = sum over u's arcs of
+ * randomize(w[v] + it) * wt (rows without arcs keep z = 0), order the nodes by
+ * (z, w), give each distinct pair its dense rank, it += 1; stop when the count
+ * is unchanged.  rounds_gpu uses the count of distinct initial colours as the
+ * starting count, rounds_cpu uses N as rsc.cpp:108-109 does.
+ */
+int orc_refine_rsc(uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt,
+                   const uint32_t* init, uint32_t* labels_out, uint32_t* rounds_gpu,
+                   uint32_t* rounds_cpu, uint32_t* blocks_out, uint32_t max_rounds)
+{
+    *rounds_gpu = *rounds_cpu = *blocks_out = 0;
+    if (n == 0) return 0;
+    uint64_t* w = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    uint64_t* z = (uint64_t*)calloc(n, sizeof(uint64_t));
+    uint32_t* ord = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* tmp = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* lab = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t count0 = 1;
+    if (init) {
+        /* dense rank of the initial colour, in increasing colour order */
+        for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+        const uint32_t* c = init;
+        msort_idx(ord, tmp, n, cmp_lab, &c);
+        uint64_t rank = 1;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i && init[ord[i]] != init[ord[i - 1]]) ++rank;
+            w[ord[i]] = rank;
+        }
+        count0 = (uint32_t)rank;
+    } else {
+        for (uint32_t i = 0; i < n; ++i) w[i] = 1;
+    }
+    uint64_t it = 0;
+    uint32_t prev_cpu = n, prev_gpu = count0, count = count0;
+    int status = -1;
+    int gpu_done = 0;
+    while (it < max_rounds) {
+        for (uint32_t u = 0; u < n; ++u) {
+            if (off[u] == off[u + 1]) continue;     /* z stays as it was */
+            uint64_t s = 0;
+            for (uint64_t k = off[u]; k < off[u + 1]; ++k)
+                s += orc_rsc_randomize(w[idx[k]] + it) * (wt ? wt[k] : 1u);
+            z[u] = s;
+        }
+        for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+        rsc_ctx c = { z, w };
+        msort_idx(ord, tmp, n, cmp_rsc, &c);
+        uint64_t rank = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i && cmp_rsc(ord[i - 1], ord[i], &c) != 0) ++rank;
+            lab[ord[i]] = (uint32_t)rank;
+        }
+        for (uint32_t i = 0; i < n; ++i) w[i] = lab[i];
+        count = (uint32_t)rank + 1;
+        ++it;
+        if (!gpu_done) {
+            if (count == prev_gpu) { *rounds_gpu = (uint32_t)it; gpu_done = 1; }
+            prev_gpu = count;
+        }
+        if (count == prev_cpu) { status = 0; break; }
+        prev_cpu = count;
+    }
+    /* the CPU convention can stop one pass before the GPU one (round 1 already
+     * yields N blocks); the partition is then final, so one more pass would
+     * confirm it */
+    if (!gpu_done) *rounds_gpu = (uint32_t)it + 1;
+    *rounds_cpu = (uint32_t)it;
+    *blocks_out = orc_canonicalize(n, lab, labels_out);
+    free(w); free(z); free(ord); free(tmp); free(lab);
+    return status;
+}

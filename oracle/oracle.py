@@ -1,0 +1,253 @@
+"""Python front end of the oracle -- TEST INFRASTRUCTURE ONLY.
+
+The checker that the CUDA product path is compared against.  Only tests/,
+``__graft_entry__.smoke()`` and the CPU-baseline leg of ``bench.py`` import
+this module; the product (``rbsc_b200``, ``librbsc.so``, the ``rbsc`` CLI)
+never does.
+
+Two kinds of oracle are reachable from here:
+
+* ``refine_exact`` / ``refine_rsc``: the C restatement in ``oracle.c``
+  (built into ``liboracle.so``);
+* ``run_ref_rsc`` / ``run_ref_valmari``: the reference programs themselves,
+  compiled unmodified from their sources into ``oracle/_ref/`` by
+  ``oracle/Makefile`` (``src/rsc/rsc.cpp`` and ``src/part_ref``).
+
+All labels returned are canonical: each node carries the smallest node id of
+its block.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+REF_RSC = os.path.join(REF_DIR, "ref_rsc")
+REF_VALMARI = os.path.join(REF_DIR, "ref_valmari")
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+
+
+def build(ref: str | None = None) -> None:
+    """Run oracle/Makefile (liboracle.so, and oracle/_ref when the reference
+    tree is present)."""
+    cmd = ["make", "-s", "-C", HERE]
+    if ref:
+        cmd.append(f"REF={ref}")
+    subprocess.run(cmd, check=True)
+
+
+_lib = None
+
+
+def _load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        lib = ctypes.CDLL(LIB_PATH)
+        lib.orc_refine_exact.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p, _u32p,
+                                         _u32p, _u32p, _u32p, ctypes.c_uint32]
+        lib.orc_refine_exact.restype = ctypes.c_int
+        lib.orc_refine_rsc.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p, _u32p,
+                                       _u32p, _u32p, _u32p, ctypes.c_uint32]
+        lib.orc_refine_rsc.restype = ctypes.c_int
+        lib.orc_canonicalize.argtypes = [ctypes.c_uint32, _u32p, _u32p]
+        lib.orc_canonicalize.restype = ctypes.c_uint32
+        lib.orc_rsc_randomize.argtypes = [ctypes.c_uint64]
+        lib.orc_rsc_randomize.restype = ctypes.c_uint64
+        _lib = lib
+    return _lib
+
+
+def _p32(a):
+    return None if a is None else a.ctypes.data_as(_u32p)
+
+
+def _p64(a):
+    return None if a is None else a.ctypes.data_as(_u64p)
+
+
+@dataclass
+class OracleResult:
+    labels: np.ndarray      # canonical labels (min node id per block), uint32
+    blocks: int
+    rounds: int             # rounds, GPU convention
+    rounds_cpu: int | None = None
+    round_blocks: list | None = None
+    status: int = 0
+
+
+def _csr(off, idx, wt):
+    off = np.ascontiguousarray(off, dtype=np.uint64)
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    if idx.size == 0:
+        idx = np.zeros(1, dtype=np.uint32)
+    wt = None if wt is None else np.ascontiguousarray(wt, dtype=np.uint64)
+    if wt is not None and wt.size == 0:
+        wt = np.zeros(1, dtype=np.uint64)
+    return off, idx, wt
+
+
+def refine_exact(off, idx, wt=None, init=None, max_rounds: int | None = None) -> OracleResult:
+    """Exact coarsest stable refinement (oracle.c: orc_refine_exact)."""
+    lib = _load()
+    n = len(off) - 1
+    off, idx, wt = _csr(off, idx, wt)
+    init = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+    if max_rounds is None:
+        max_rounds = n + 2
+    labels = np.zeros(max(n, 1), dtype=np.uint32)
+    rounds = ctypes.c_uint32()
+    blocks = ctypes.c_uint32()
+    rb = np.zeros(max_rounds + 1, dtype=np.uint32)
+    st = lib.orc_refine_exact(n, _p64(off), _p32(idx), _p64(wt), _p32(init), _p32(labels),
+                              ctypes.byref(rounds), ctypes.byref(blocks), _p32(rb), max_rounds)
+    return OracleResult(labels[:n].copy(), blocks.value, rounds.value, None,
+                        [int(x) for x in rb[: rounds.value + 1]], st)
+
+
+def refine_rsc(off, idx, wt=None, init=None, max_rounds: int | None = None) -> OracleResult:
+    """The reference CPU loop restated (oracle.c: orc_refine_rsc)."""
+    lib = _load()
+    n = len(off) - 1
+    off, idx, wt = _csr(off, idx, wt)
+    init = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+    if max_rounds is None:
+        max_rounds = n + 2
+    labels = np.zeros(max(n, 1), dtype=np.uint32)
+    rg, rc, bl = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    st = lib.orc_refine_rsc(n, _p64(off), _p32(idx), _p64(wt), _p32(init), _p32(labels),
+                            ctypes.byref(rg), ctypes.byref(rc), ctypes.byref(bl), max_rounds)
+    return OracleResult(labels[:n].copy(), bl.value, rg.value, rc.value, None, st)
+
+
+def canonicalize(labels) -> tuple[np.ndarray, int]:
+    lib = _load()
+    lab = np.ascontiguousarray(labels, dtype=np.uint32)
+    out = np.zeros(max(lab.size, 1), dtype=np.uint32)
+    b = lib.orc_canonicalize(lab.size, _p32(lab if lab.size else out), _p32(out))
+    return out[: lab.size].copy(), int(b)
+
+
+def rsc_randomize(x: int) -> int:
+    return int(_load().orc_rsc_randomize(x))
+
+
+# ---------------------------------------------------------------------------
+# text formats of the reference
+# ---------------------------------------------------------------------------
+
+def arcs_cuda_text(off, idx, wt=None) -> bytes:
+    """arcs-cuda text (webgraph-rs cli/src/to/arcscuda.rs:61-66):
+    "N\\nM\\n" then one "u wt v" line per arc, grouped by u."""
+    off = np.asarray(off, dtype=np.uint64)
+    idx = np.asarray(idx, dtype=np.uint32)
+    n = len(off) - 1
+    m = int(off[-1]) if n >= 0 else 0
+    deg = np.diff(off.astype(np.int64))
+    src = np.repeat(np.arange(n, dtype=np.int64), deg)
+    w = np.ones(m, dtype=np.uint64) if wt is None else np.asarray(wt, dtype=np.uint64)
+    lines = [f"{n}\n{m}\n"]
+    if m:
+        lines.append("\n".join(f"{a} {b} {c}" for a, b, c in zip(src.tolist(), w.tolist(), idx[:m].tolist())))
+        lines.append("\n")
+    return "".join(lines).encode()
+
+
+def mdp_text(off, idx, wt=None, init=None) -> bytes:
+    """Valmari MDP text (src/part_ref/MDP_read.cc:51-63), the conversion that
+    valmari-adapter:9-16 performs, extended with <blocks> for initial colours."""
+    off = np.asarray(off, dtype=np.uint64)
+    idx = np.asarray(idx, dtype=np.uint32)
+    n = len(off) - 1
+    m = int(off[-1])
+    deg = np.diff(off.astype(np.int64))
+    src = np.repeat(np.arange(n, dtype=np.int64), deg)
+    w = np.ones(m, dtype=np.uint64) if wt is None else np.asarray(wt, dtype=np.uint64)
+    blocks = []
+    if init is not None:
+        init = np.asarray(init, dtype=np.uint32)
+        colours = sorted(set(init.tolist()))
+        # block 1 = the remaining states (MDP_read.cc:58-59): the first colour
+        for c in colours[1:]:
+            members = (np.nonzero(init == c)[0] + 1).tolist()
+            blocks.append(" ".join(map(str, members)) + " 0")
+    nb = 1 + len(blocks)
+    out = [f"{n} 0 0 {m} {nb}\n"]
+    if m:
+        out.append("\n".join(f"{a + 1} {b} {c + 1}" for a, b, c in zip(src.tolist(), w.tolist(), idx[:m].tolist())))
+        out.append("\n")
+    if blocks:
+        out.append("\n".join(blocks) + "\n")
+    return "".join(out).encode()
+
+
+def _parse_ref_output(txt: str):
+    lines = txt.strip().split("\n")
+    t = float(lines[0])
+    done = int(lines[1])
+    nodes = int(lines[2])
+    rounds = None
+    labels = None
+    for ln in lines[3:]:
+        if ln.startswith("rounds "):
+            rounds = int(ln.split()[1])
+        elif ln.startswith("labels"):
+            labels = np.array([int(x) for x in ln.split()[1:]], dtype=np.uint64)
+    return t, done, nodes, rounds, labels
+
+
+def _canon_u64(labels: np.ndarray) -> np.ndarray:
+    _, inv = np.unique(labels, return_inverse=True)
+    out, _ = canonicalize(inv.astype(np.uint32))
+    return out
+
+
+def run_ref_rsc(off, idx, wt=None, timeout: float = 600.0) -> OracleResult:
+    """Run the reference rsc (src/rsc/rsc.cpp, unmodified) on a graph.
+    Uniform initial colours only: rsc.cpp:118-121 fixes w = 1."""
+    if not os.path.exists(REF_RSC):
+        raise FileNotFoundError(REF_RSC)
+    txt = subprocess.run([REF_RSC], input=arcs_cuda_text(off, idx, wt), capture_output=True,
+                         timeout=timeout, check=True).stdout.decode()
+    t, done, nodes, rounds, labels = _parse_ref_output(txt)
+    n = len(off) - 1
+    lab = _canon_u64(labels) if n else np.zeros(0, dtype=np.uint32)
+    res = OracleResult(lab, nodes, rounds_gpu_from_cpu(rounds, nodes, n), rounds)
+    res.time_s = t
+    return res
+
+
+def rounds_gpu_from_cpu(rounds_cpu: int, blocks: int, n: int) -> int:
+    """rsc.cpp starts its block count at N (rsc.cpp:108-109); the GPU program
+    starts at 1 (rbsc.cu:339).  They differ only when the first pass already
+    yields N blocks (rsc stops one pass earlier) or a single block (rsc runs
+    one pass more)."""
+    if rounds_cpu == 1 and blocks == n and n != 1:
+        return 2
+    if rounds_cpu == 2 and blocks == 1 and n != 1:
+        return 1
+    return rounds_cpu
+
+
+def run_ref_valmari(off, idx, wt=None, init=None, timeout: float = 600.0) -> OracleResult:
+    """Run Valmari's minimiser (src/part_ref, unmodified) on a graph; initial
+    colours go in as MDP <blocks>."""
+    if not os.path.exists(REF_VALMARI):
+        raise FileNotFoundError(REF_VALMARI)
+    txt = subprocess.run([REF_VALMARI], input=mdp_text(off, idx, wt, init), capture_output=True,
+                         timeout=timeout, check=True).stdout.decode()
+    t, done, nodes, rounds, labels = _parse_ref_output(txt)
+    n = len(off) - 1
+    lab = _canon_u64(labels) if n else np.zeros(0, dtype=np.uint32)
+    res = OracleResult(lab, nodes, -1, None)
+    res.time_s = t
+    return res

@@ -1,0 +1,281 @@
+"""rbsc_b200 -- B200 (sm_100a) colour refinement with rbsc's surface.
+
+Computes the coarsest backward-equivalence (lumpable) partition of a weighted
+directed graph -- 1-WL colour refinement over successor multisets -- the path
+that src/rbsc/rbsc.cu implements with CUB in the reference.
+
+Host mirror of the reference's interface.  The reference is a process
+(``<arcs-cuda text> | rbsc [edge_batch_size] [gpus]`` printing ``time``,
+``done`` and ``nodes``, src/rbsc/rbsc.cu:182-497); this module exposes the
+same path as calls over the C ABI of include/rbsc.h:
+
+* :func:`run` -- text in, ``(time, done, nodes)`` out, like one reference run;
+* :class:`Context` / :class:`Graph` -- resident graphs, repeated refinements,
+  labels and statistics;
+* :func:`parse_arcs`, :func:`gen_rmat_host` -- input formats and workloads.
+
+Every call goes through librbsc.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import RELABEL_HASH, RELABEL_SORT, RbscError
+
+__all__ = ["Context", "Graph", "Result", "RbscError", "run", "parse_arcs", "gen_rmat_host",
+           "RELABEL_HASH", "RELABEL_SORT", "degree_bucket_colors"]
+
+RMAT_ABC = (0.57, 0.19, 0.19)
+
+
+@dataclass
+class Result:
+    """One refinement: canonical labels (smallest node id of each block) and
+    the counters the reference prints (``nodes`` = blocks, ``done``) plus the
+    round count and timings."""
+    labels: np.ndarray | None
+    blocks: int
+    rounds: int
+    done: int
+    verified: int
+    repairs: int
+    initial_blocks: int
+    time_s: float
+    device_ms: float
+    verify_ms: float
+    h2d_ms: float
+    d2h_ms: float
+    h2d_bytes: int
+    d2h_bytes: int
+    round_blocks: list = field(default_factory=list)
+    kernel_launches: int = 0
+
+
+def _result(st: _lib.Stats, labels) -> Result:
+    rb = [int(st.round_blocks[i]) for i in range(min(64, st.rounds + 1))]
+    return Result(labels, int(st.blocks), int(st.rounds), int(st.done), int(st.verified), int(st.repairs),
+                  int(st.initial_blocks), float(st.time_s), float(st.device_ms), float(st.verify_ms),
+                  float(st.h2d_ms), float(st.d2h_ms), int(st.h2d_bytes), int(st.d2h_bytes), rb,
+                  int(st.kernel_launches))
+
+
+def _check(lib, status: int, ctx=None):
+    if status != _lib.RBSC_OK:
+        msg = lib.rbsc_last_error(ctx)
+        raise RbscError(status, msg.decode() if msg else "")
+
+
+def _csr(off, idx, wt):
+    off = np.ascontiguousarray(off)
+    if off.dtype not in (np.uint64, np.int64, np.uint32, np.int32):
+        off = off.astype(np.uint64)
+    ob = off.dtype.itemsize
+    idx = np.ascontiguousarray(idx, dtype=np.uint32)
+    wt = None if wt is None else np.ascontiguousarray(wt, dtype=np.uint64)
+    n = len(off) - 1
+    m = int(off[-1]) if n >= 0 else 0
+    c = _lib.Csr()
+    c.n = n
+    c.m = m
+    c.offsets = off.ctypes.data
+    c.offset_bytes = ob
+    c.indices = idx.ctypes.data if idx.size else None
+    c.weights = wt.ctypes.data if (wt is not None and wt.size) else None
+    return c, (off, idx, wt)
+
+
+class Context:
+    """A device context (one CUDA device, one stream).  Options mirror
+    ``rbsc_opts`` of include/rbsc.h."""
+
+    def __init__(self, device: int = 0, relabel: int = RELABEL_HASH, verify: bool = True, max_rounds: int = 0,
+                 use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0):
+        self._lib = _lib.load()
+        o = _lib.Opts()
+        self._lib.rbsc_opts_default(ctypes.byref(o))
+        o.relabel = relabel
+        o.verify = 1 if verify else 0
+        o.max_rounds = max_rounds
+        o.use_graph = 1 if use_graph else 0
+        o.seed = seed
+        o.test_hash_bits = test_hash_bits
+        self._opts = o
+        h = self._lib.rbsc_ctx_create(device, ctypes.byref(o))
+        if not h:
+            raise RbscError(-2, self._lib.rbsc_last_error(None).decode())
+        self._h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rbsc_ctx_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_opts(self, **kw):
+        for k, v in kw.items():
+            if k == "verify" or k == "use_graph":
+                v = 1 if v else 0
+            setattr(self._opts, k, v)
+        _check(self._lib, self._lib.rbsc_ctx_set_opts(self._h, ctypes.byref(self._opts)), self._h)
+
+    def refine(self, off, idx, wt=None, init=None, labels: bool = True) -> Result:
+        """One-shot refinement of a host CSR (rbsc_refine)."""
+        c, keep = _csr(off, idx, wt)
+        init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+        out = np.zeros(max(c.n, 1), dtype=np.uint32) if labels else None
+        st = _lib.Stats()
+        _check(self._lib, self._lib.rbsc_refine(self._h, ctypes.byref(c),
+                                                None if init_a is None else init_a.ctypes.data,
+                                                None if out is None else out.ctypes.data, ctypes.byref(st)), self._h)
+        return _result(st, None if out is None else out[: c.n])
+
+    def upload(self, off, idx, wt=None) -> "Graph":
+        c, keep = _csr(off, idx, wt)
+        h = ctypes.c_void_p()
+        _check(self._lib, self._lib.rbsc_graph_upload(self._h, ctypes.byref(c), ctypes.byref(h)), self._h)
+        return Graph(self, h)
+
+    def from_device(self, n: int, m: int, d_off: int, d_idx: int, d_wt: int | None = None,
+                    offset_bytes: int = 8) -> "Graph":
+        c = _lib.Csr()
+        c.n, c.m, c.offsets, c.offset_bytes, c.indices, c.weights = n, m, d_off, offset_bytes, d_idx, d_wt
+        h = ctypes.c_void_p()
+        _check(self._lib, self._lib.rbsc_graph_from_device(self._h, ctypes.byref(c), ctypes.byref(h)), self._h)
+        return Graph(self, h)
+
+    def gen_rmat(self, scale: int, edge_factor: int, a=RMAT_ABC[0], b=RMAT_ABC[1], c=RMAT_ABC[2],
+                 seed: int = 1) -> "Graph":
+        """R-MAT graph generated directly in device memory."""
+        h = ctypes.c_void_p()
+        _check(self._lib, self._lib.rbsc_gen_rmat_device(self._h, scale, edge_factor, a, b, c, seed,
+                                                         ctypes.byref(h)), self._h)
+        return Graph(self, h)
+
+
+class Graph:
+    """A graph resident in device memory (rbsc_graph)."""
+
+    def __init__(self, ctx: Context, handle):
+        self.ctx = ctx
+        self._h = handle
+        n = ctypes.c_uint32()
+        m = ctypes.c_uint64()
+        ctx._lib.rbsc_graph_info(handle, ctypes.byref(n), ctypes.byref(m))
+        self.n = int(n.value)
+        self.m = int(m.value)
+
+    def free(self):
+        if getattr(self, "_h", None):
+            self.ctx._lib.rbsc_graph_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+    def refine(self, init=None, labels: bool = True) -> Result:
+        lib = self.ctx._lib
+        init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+        out = np.zeros(max(self.n, 1), dtype=np.uint32) if labels else None
+        st = _lib.Stats()
+        _check(lib, lib.rbsc_graph_refine(self.ctx._h, self._h, None if init_a is None else init_a.ctypes.data,
+                                          None if out is None else out.ctypes.data, ctypes.byref(st)), self.ctx._h)
+        return _result(st, None if out is None else out[: self.n])
+
+    def refine_device(self, d_init: int | None = None, d_out: int | None = None) -> Result:
+        """Refinement with device-resident initial colours / labels (raw
+        device addresses, e.g. ``tensor.data_ptr()``)."""
+        lib = self.ctx._lib
+        st = _lib.Stats()
+        _check(lib, lib.rbsc_graph_refine_device(self.ctx._h, self._h, d_init, d_out, ctypes.byref(st)), self.ctx._h)
+        return _result(st, None)
+
+    def profile(self, d_init: int | None = None):
+        """Refinement with CUDA events around every kernel (rbsc_graph_profile):
+        returns (per-kernel times dict, Result)."""
+        lib = self.ctx._lib
+        kt = _lib.KernelTimes()
+        st = _lib.Stats()
+        _check(lib, lib.rbsc_graph_profile(self.ctx._h, self._h, d_init, ctypes.byref(kt), ctypes.byref(st)),
+               self.ctx._h)
+        times = {k: getattr(kt, k) for k, _ in _lib.KernelTimes._fields_}
+        return times, _result(st, None)
+
+    def degree_colors_device(self, d_out: int):
+        lib = self.ctx._lib
+        _check(lib, lib.rbsc_graph_degree_colors(self.ctx._h, self._h, d_out), self.ctx._h)
+
+    def device_csr(self):
+        lib = self.ctx._lib
+        o = ctypes.c_void_p()
+        i = ctypes.c_void_p()
+        _check(lib, lib.rbsc_graph_device_csr(self._h, ctypes.byref(o), ctypes.byref(i)), self.ctx._h)
+        return o.value, i.value
+
+
+def _host_graph_to_numpy(lib, hg: _lib.HostGraph):
+    n, m = int(hg.n), int(hg.m)
+    off = np.ctypeslib.as_array(hg.offsets, shape=(n + 1,)).copy()
+    idx = np.ctypeslib.as_array(hg.indices, shape=(max(m, 1),))[:m].copy() if m else np.zeros(0, np.uint32)
+    wt = None
+    if bool(hg.weights):
+        wt = np.ctypeslib.as_array(hg.weights, shape=(max(m, 1),))[:m].copy()
+    lib.rbsc_host_graph_free(ctypes.byref(hg))
+    return off, idx, wt
+
+
+def parse_arcs(text: bytes):
+    """arcs-cuda text -> (offsets uint64, indices uint32, weights uint64 | None)."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    st = lib.rbsc_parse_arcs(text, len(text), ctypes.byref(hg))
+    _check(lib, st, None)
+    return _host_graph_to_numpy(lib, hg)
+
+
+def gen_rmat_host(scale: int, edge_factor: int, a=RMAT_ABC[0], b=RMAT_ABC[1], c=RMAT_ABC[2], seed: int = 1,
+                  threads: int = 0):
+    """The device generator's graph, built on the host: (offsets, indices)."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    _check(lib, lib.rbsc_gen_rmat_host(scale, edge_factor, a, b, c, seed, threads, ctypes.byref(hg)), None)
+    off, idx, _ = _host_graph_to_numpy(lib, hg)
+    return off, idx
+
+
+def degree_bucket_colors(off) -> np.ndarray:
+    """floor(log2(out_degree + 1)) as uint32 (the initial colours of the R-MAT-24 workload)."""
+    x = np.diff(np.asarray(off, dtype=np.int64)) + 1
+    out = np.zeros(x.shape, dtype=np.uint32)
+    for sh in (32, 16, 8, 4, 2, 1):
+        big = x >= (1 << sh)
+        out[big] += sh
+        x = np.where(big, x >> sh, x)
+    return out
+
+
+def run(text: bytes, edge_batch_size: int | None = None, gpus: int = 1, device: int = 0):
+    """One reference-style run: arcs-cuda text -> (time_s, done, nodes), the
+    three values rbsc.cu:492-494 prints."""
+    off, idx, wt = parse_arcs(text)
+    with Context(device) as ctx:
+        r = ctx.refine(off, idx, wt, labels=False)
+    return r.time_s, r.done, r.blocks

@@ -1,0 +1,153 @@
+"""ctypes binding of librbsc.so (include/rbsc.h).
+
+The library is loaded from this package directory only; there is no fallback:
+if it is missing or cannot be loaded, every entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "librbsc.so")
+CLI_PATH = os.path.join(PKG, "rbsc")
+
+RBSC_OK = 0
+STATUS_NAMES = {
+    0: "RBSC_OK",
+    -1: "RBSC_ERR_INVALID",
+    -2: "RBSC_ERR_CUDA",
+    -3: "RBSC_ERR_OOM",
+    -4: "RBSC_ERR_NOT_CONVERGED",
+    -5: "RBSC_ERR_DEVICE",
+    -6: "RBSC_ERR_PARSE",
+    -7: "RBSC_ERR_TOO_LARGE",
+    -8: "RBSC_ERR_BUSY",
+}
+
+RELABEL_HASH = 0
+RELABEL_SORT = 1
+
+# every symbol include/rbsc.h declares (checked by the CPU test suite)
+EXPORTED = [
+    "rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_last_error",
+    "rbsc_ctx_set_opts", "rbsc_refine", "rbsc_graph_upload", "rbsc_graph_from_device", "rbsc_graph_free",
+    "rbsc_graph_info", "rbsc_graph_device_csr", "rbsc_graph_refine", "rbsc_graph_refine_device",
+    "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
+    "rbsc_gen_rmat_host", "rbsc_graph_profile",
+]
+
+
+class Opts(ctypes.Structure):
+    _fields_ = [
+        ("relabel", ctypes.c_int32),
+        ("verify", ctypes.c_int32),
+        ("max_rounds", ctypes.c_uint32),
+        ("use_graph", ctypes.c_int32),
+        ("seed", ctypes.c_uint64),
+        ("test_hash_bits", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 7),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("rounds", ctypes.c_uint32),
+        ("blocks", ctypes.c_uint32),
+        ("done", ctypes.c_uint32),
+        ("verified", ctypes.c_uint32),
+        ("repairs", ctypes.c_uint32),
+        ("initial_blocks", ctypes.c_uint32),
+        ("time_s", ctypes.c_double),
+        ("device_ms", ctypes.c_double),
+        ("verify_ms", ctypes.c_double),
+        ("h2d_ms", ctypes.c_double),
+        ("d2h_ms", ctypes.c_double),
+        ("h2d_bytes", ctypes.c_uint64),
+        ("d2h_bytes", ctypes.c_uint64),
+        ("round_blocks", ctypes.c_uint32 * 64),
+        ("kernel_launches", ctypes.c_uint64),
+    ]
+
+
+class KernelTimes(ctypes.Structure):
+    _fields_ = [
+        ("passes", ctypes.c_uint32),
+        ("signature_ms", ctypes.c_double),
+        ("insert_ms", ctypes.c_double),
+        ("relabel_ms", ctypes.c_double),
+        ("other_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+    ]
+
+
+class Csr(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint32),
+        ("m", ctypes.c_uint64),
+        ("offsets", ctypes.c_void_p),
+        ("offset_bytes", ctypes.c_int32),
+        ("indices", ctypes.c_void_p),
+        ("weights", ctypes.c_void_p),
+    ]
+
+
+class HostGraph(ctypes.Structure):
+    _fields_ = [
+        ("n", ctypes.c_uint32),
+        ("m", ctypes.c_uint64),
+        ("offsets", ctypes.POINTER(ctypes.c_uint64)),
+        ("indices", ctypes.POINTER(ctypes.c_uint32)),
+        ("weights", ctypes.POINTER(ctypes.c_uint64)),
+    ]
+
+
+_lib = None
+
+
+def load():
+    """Loads librbsc.so from the package directory (raises if absent)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"librbsc.so not built ({LIB_PATH}); run `python -m rbsc_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    vp = ctypes.c_void_p
+    lib.rbsc_abi_version.restype = ctypes.c_int32
+    lib.rbsc_opts_default.argtypes = [P(Opts)]
+    lib.rbsc_ctx_create.argtypes = [ctypes.c_int32, P(Opts)]
+    lib.rbsc_ctx_create.restype = vp
+    lib.rbsc_ctx_destroy.argtypes = [vp]
+    lib.rbsc_last_error.argtypes = [vp]
+    lib.rbsc_last_error.restype = ctypes.c_char_p
+    lib.rbsc_ctx_set_opts.argtypes = [vp, P(Opts)]
+    lib.rbsc_refine.argtypes = [vp, P(Csr), vp, vp, P(Stats)]
+    lib.rbsc_graph_upload.argtypes = [vp, P(Csr), P(vp)]
+    lib.rbsc_graph_from_device.argtypes = [vp, P(Csr), P(vp)]
+    lib.rbsc_graph_free.argtypes = [vp]
+    lib.rbsc_graph_info.argtypes = [vp, P(ctypes.c_uint32), P(ctypes.c_uint64)]
+    lib.rbsc_graph_device_csr.argtypes = [vp, P(vp), P(vp)]
+    lib.rbsc_graph_refine.argtypes = [vp, vp, vp, vp, P(Stats)]
+    lib.rbsc_graph_refine_device.argtypes = [vp, vp, vp, vp, P(Stats)]
+    lib.rbsc_graph_degree_colors.argtypes = [vp, vp, vp]
+    lib.rbsc_graph_profile.argtypes = [vp, vp, vp, P(KernelTimes), P(Stats)]
+    lib.rbsc_parse_arcs.argtypes = [ctypes.c_char_p, ctypes.c_size_t, P(HostGraph)]
+    lib.rbsc_host_graph_free.argtypes = [P(HostGraph)]
+    lib.rbsc_gen_rmat_device.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_uint64, P(vp)]
+    lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
+    for name in EXPORTED:
+        if name not in ("rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy",
+                        "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):
+            getattr(lib, name).restype = ctypes.c_int32
+    _lib = lib
+    return lib
+
+
+class RbscError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")

@@ -1,0 +1,133 @@
+// cli.cpp -- the `rbsc` command, with the reference's process surface
+// (src/rbsc/rbsc.cu:182-497):
+//
+//   <arcs-cuda text on stdin> | rbsc [edge_batch_size] [gpus]
+//
+// stdout: exactly three lines, as rbsc.cu:492-494 prints them -- the
+// refinement time in seconds ("%lf"), done (1 = coarsest partition), and the
+// number of blocks.  On failure a message goes to stdout and the exit code is
+// EXIT_FAILURE, as the reference's CHECK_* macros do (rbsc.cu:15-47).
+//
+// edge_batch_size: accepted for compatibility.  The whole graph is refined in
+// device memory whatever its value (the result is always the coarsest
+// partition, done = 1).  gpus: accepted; one process drives one GPU (device 0
+// unless RBSC_DEVICE is set).
+//
+// Extra options (after the positional ones; none changes the three lines):
+//   --dump-partition FILE   write the canonical label of every node, one per line
+//   --init-colors FILE      initial colours, one uint32 per line (N lines)
+//   --stats                 print a JSON line with rounds and timings to stderr
+//   --relabel sort|hash     relabel strategy (default hash)
+#include <cinttypes>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rbsc.h"
+
+static bool read_all(FILE* f, std::string& s)
+{
+    char buf[1 << 16];
+    size_t k;
+    while ((k = fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, k);
+    return !ferror(f);
+}
+
+int main(int argc, char** argv)
+{
+    const char* dump = nullptr;
+    const char* init_path = nullptr;
+    bool want_stats = false;
+    int relabel = RBSC_RELABEL_HASH;
+    std::vector<const char*> pos;
+    for (int i = 1; i < argc; ++i) {
+        if (!std::strcmp(argv[i], "--dump-partition") && i + 1 < argc) dump = argv[++i];
+        else if (!std::strcmp(argv[i], "--init-colors") && i + 1 < argc) init_path = argv[++i];
+        else if (!std::strcmp(argv[i], "--stats")) want_stats = true;
+        else if (!std::strcmp(argv[i], "--relabel") && i + 1 < argc) relabel = !std::strcmp(argv[++i], "sort") ? RBSC_RELABEL_SORT : RBSC_RELABEL_HASH;
+        else pos.push_back(argv[i]);
+    }
+    // positional arguments, as rbsc.cu:204-205 reads them
+    unsigned long long edge_batch = pos.size() >= 1 ? std::strtoull(pos[0], nullptr, 10) : 0;
+    unsigned long long gpus = pos.size() >= 2 ? std::strtoull(pos[1], nullptr, 10) : 1;
+    (void)edge_batch;
+    (void)gpus;
+
+    std::string text;
+    if (!read_all(stdin, text)) {
+        std::printf("failed to read standard input\n");
+        return EXIT_FAILURE;
+    }
+    rbsc_host_graph hg;
+    if (rbsc_parse_arcs(text.data(), text.size(), &hg) != RBSC_OK) {
+        std::printf("input error: %s\n", rbsc_last_error(nullptr));
+        return EXIT_FAILURE;
+    }
+    text.clear();
+    text.shrink_to_fit();
+
+    std::vector<uint32_t> init;
+    if (init_path) {
+        FILE* f = std::fopen(init_path, "r");
+        if (!f) {
+            std::printf("cannot open %s\n", init_path);
+            return EXIT_FAILURE;
+        }
+        unsigned long v;
+        while (std::fscanf(f, "%lu", &v) == 1) init.push_back((uint32_t)v);
+        std::fclose(f);
+        if (init.size() != hg.n) {
+            std::printf("%s: expected %u colours, read %zu\n", init_path, hg.n, init.size());
+            return EXIT_FAILURE;
+        }
+    }
+
+    const char* dev_env = std::getenv("RBSC_DEVICE");
+    rbsc_opts opts;
+    rbsc_opts_default(&opts);
+    opts.relabel = relabel;
+    rbsc_ctx* ctx = rbsc_ctx_create(dev_env ? std::atoi(dev_env) : 0, &opts);
+    if (!ctx) {
+        std::printf("CUDA setup failed: %s\n", rbsc_last_error(nullptr));
+        return EXIT_FAILURE;
+    }
+    rbsc_csr csr;
+    csr.n = hg.n;
+    csr.m = hg.m;
+    csr.offsets = hg.offsets;
+    csr.offset_bytes = 8;
+    csr.indices = hg.indices;
+    csr.weights = hg.weights;
+    std::vector<uint32_t> labels(hg.n);
+    rbsc_stats st;
+    rbsc_status rc = rbsc_refine(ctx, &csr, init.empty() ? nullptr : init.data(), hg.n ? labels.data() : nullptr, &st);
+    if (rc != RBSC_OK) {
+        std::printf("refinement failed: %s\n", rbsc_last_error(ctx));
+        rbsc_ctx_destroy(ctx);
+        return EXIT_FAILURE;
+    }
+    std::printf("%lf\n", st.time_s);
+    std::printf("%u\n", st.done);
+    std::printf("%lu\n", (unsigned long)st.blocks);
+    if (want_stats)
+        std::fprintf(stderr,
+                     "{\"rounds\": %u, \"blocks\": %u, \"initial_blocks\": %u, \"verified\": %u, \"repairs\": %u, "
+                     "\"device_ms\": %.4f, \"verify_ms\": %.4f, \"h2d_ms\": %.4f, \"d2h_ms\": %.4f, \"time_s\": %.6f}\n",
+                     st.rounds, st.blocks, st.initial_blocks, st.verified, st.repairs, st.device_ms, st.verify_ms, st.h2d_ms,
+                     st.d2h_ms, st.time_s);
+    if (dump) {
+        FILE* f = std::fopen(dump, "w");
+        if (!f) {
+            std::printf("cannot write %s\n", dump);
+            rbsc_ctx_destroy(ctx);
+            return EXIT_FAILURE;
+        }
+        for (uint32_t i = 0; i < hg.n; ++i) std::fprintf(f, "%u\n", labels[i]);
+        std::fclose(f);
+    }
+    rbsc_ctx_destroy(ctx);
+    rbsc_host_graph_free(&hg);
+    return 0;
+}

@@ -1,0 +1,69 @@
+// common.cuh -- shared constants, hash functions and small device helpers.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace rbsc {
+
+// Colour words: bits 0..30 = label (smallest node id of the block),
+// bit 31 = the block is a singleton.  Singleton blocks never split again, so
+// their nodes skip the relabel table.
+constexpr uint32_t kSingleton = 0x80000000u;
+constexpr uint32_t kLabelMask = 0x7fffffffu;
+// Relabel-table value word: bits 0..30 = smallest member, bit 31 = the key was
+// seen from more than one node (block is not a singleton).
+constexpr uint32_t kJoined = 0x80000000u;
+
+// Edges per signature tile and threads per tile CTA.
+constexpr int kTileThreads = 256;
+constexpr int kEdgesPerThread = 8;
+constexpr uint32_t kTileEdges = kTileThreads * kEdgesPerThread;  // 2048
+
+constexpr int kNodeThreads = 256;
+
+constexpr uint64_t kGolden = 0x9e3779b97f4a7c15ull;
+
+// MurmurHash3 64-bit finaliser (Austin Appleby, public domain): a bijection
+// on uint64 with full avalanche.  Used as the per-arc term of the signature.
+__host__ __device__ __forceinline__ uint64_t fmix64(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdull;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ull;
+    k ^= k >> 33;
+    return k;
+}
+
+// MurmurHash3 32-bit finaliser (same source): second, independent term.
+__host__ __device__ __forceinline__ uint32_t fmix32(uint32_t h)
+{
+    h ^= h >> 16;
+    h *= 0x85ebca6bu;
+    h ^= h >> 13;
+    h *= 0xc2b2ae35u;
+    h ^= h >> 16;
+    return h;
+}
+
+// Per-pass salts.  Pass r hashes colour c as fmix64(c ^ salt1(r)) and
+// fmix32(c ^ salt2(r)); a fresh salt per pass decorrelates the passes.
+__host__ __device__ __forceinline__ uint64_t pass_salt1(uint64_t seed, uint32_t r)
+{
+    return fmix64(seed + (uint64_t)(r + 1) * kGolden);
+}
+__host__ __device__ __forceinline__ uint32_t pass_salt2(uint64_t seed, uint32_t r)
+{
+    return (uint32_t)(fmix64(~seed + (uint64_t)(r + 7) * 0xd1b54a32d192ed03ull) >> 32);
+}
+
+template <typename T> __host__ __device__ __forceinline__ T ceil_div(T a, T b) { return (a + b - 1) / b; }
+
+// Kernels enqueued by the calling host thread (reported in rbsc_stats).
+inline uint64_t& launch_counter()
+{
+    static thread_local uint64_t c = 0;
+    return c;
+}
+
+}  // namespace rbsc

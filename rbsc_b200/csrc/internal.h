@@ -1,0 +1,94 @@
+// internal.h -- definitions shared by the host translation units of librbsc.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <cuda_runtime.h>
+
+#include "../../include/rbsc.h"
+
+namespace rbsc {
+struct RoundState;
+struct Entry;
+}
+
+struct rbsc_ctx {
+    int device = 0;
+    rbsc_opts opts{};
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {};
+    int sm_count = 148;
+    std::string err;
+};
+
+struct rbsc_graph {
+    rbsc_ctx* ctx = nullptr;
+    uint32_t n = 0;
+    uint64_t m = 0;
+    bool weighted = false;
+    bool off32 = false;         // roff stored as uint32 (M < 2^32)
+    uint64_t* d_off = nullptr;  // n+1 per-node arc offsets
+    uint32_t* d_idx = nullptr;  // arc heads, padded to whole tiles
+    uint64_t* d_wt = nullptr;   // weights (padded) or null
+    uint32_t K = 0;             // non-empty rows
+    uint32_t* d_rows = nullptr;
+    void* d_roff = nullptr;
+    uint32_t ntiles = 0;
+    uint32_t* d_tile_row = nullptr;
+    uint32_t nsplit = 0;
+    uint32_t* d_split = nullptr;
+
+    // refinement state (allocated on first refine, reused)
+    bool bufs = false;
+    uint32_t* d_col[2] = {nullptr, nullptr};
+    uint32_t* d_initlab = nullptr;
+    unsigned long long* d_sig1 = nullptr;
+    uint32_t* d_sig2 = nullptr;
+    uint32_t* d_slot = nullptr;
+    uint32_t* d_out = nullptr;
+    uint32_t* d_init = nullptr;
+    rbsc::Entry* d_tab = nullptr;
+    uint32_t log2tab = 0;
+    uint32_t next_stamp = 1;
+    rbsc::RoundState* d_st = nullptr;
+    rbsc::RoundState* h_st = nullptr;  // pinned mirror
+    void* d_small = nullptr;           // 256 B of counters
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+
+    // exact check
+    uint32_t* d_vflag = nullptr;
+    uint64_t* d_vdeg = nullptr;
+    uint32_t* d_fail = nullptr;
+    unsigned long long* d_keys[2] = {nullptr, nullptr};
+    unsigned long long* d_vals[2] = {nullptr, nullptr};
+    uint64_t key_cap = 0;
+
+    // sort-based relabel
+    bool sr_bufs = false;
+    unsigned long long* d_sr_keys[2] = {nullptr, nullptr};
+    uint32_t* d_sr_perm[2] = {nullptr, nullptr};
+    uint32_t* d_sr_head = nullptr;
+    uint32_t* d_sr_gstart = nullptr;
+    void* d_sr_tmp = nullptr;
+    size_t sr_tmp_bytes = 0;
+
+    // device-side round loop
+    cudaGraph_t loop_graph = nullptr;
+    cudaGraphExec_t loop_exec = nullptr;
+    int loop_relabel = -1;
+    uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop
+};
+
+rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);
+rbsc_status rbsc_cuda_fail(rbsc_ctx* ctx, cudaError_t e, const char* what, int line);
+rbsc_status dev_alloc(rbsc_ctx* ctx, void** p, size_t bytes);
+rbsc_status ensure_temp(rbsc_ctx* ctx, rbsc_graph* g, size_t bytes);
+rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g);
+rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted);
+rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init, uint32_t* d_out, rbsc_stats* stats,
+                            rbsc_kernel_times* kt);
+
+// sort-based relabel (sortrelabel.cu)
+rbsc_status ensure_sort_relabel_bufs(rbsc_ctx* ctx, rbsc_graph* g);
+rbsc_status launch_sort_relabel(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s);
+void sortrelabel_release(rbsc_graph* g);

@@ -1,0 +1,869 @@
+// rbsc.cu -- host side of librbsc: contexts, resident graphs, the refinement
+// driver (device-resident round loop in a CUDA graph with a while node), the
+// exact check + repair, and the C ABI of include/rbsc.h.
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/rbsc.h"
+#include "common.cuh"
+#include "prep_kernels.cuh"
+#include "radix.cuh"
+#include "refine_kernels.cuh"
+#include "scan.cuh"
+#include "verify_kernels.cuh"
+#include "internal.h"
+
+using namespace rbsc;
+
+namespace {
+thread_local std::string g_global_error;
+}
+
+// ---------------------------------------------------------------------------
+// errors
+// ---------------------------------------------------------------------------
+rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (ctx) ctx->err = buf;
+    else g_global_error = buf;
+    return code;
+}
+
+rbsc_status rbsc_cuda_fail(rbsc_ctx* ctx, cudaError_t e, const char* what, int line)
+{
+    const rbsc_status code = (e == cudaErrorMemoryAllocation) ? RBSC_ERR_OOM : RBSC_ERR_CUDA;
+    return rbsc_fail(ctx, code, "%s failed (line %d): %s (%d)", what, line, cudaGetErrorString(e), (int)e);
+}
+
+#define CK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return rbsc_cuda_fail(ctx, e_, #call, __LINE__); \
+    } while (0)
+
+#define CKS(call)                           \
+    do {                                    \
+        rbsc_status s_ = (call);            \
+        if (s_ != RBSC_OK) return s_;       \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// device buffers
+// ---------------------------------------------------------------------------
+rbsc_status dev_alloc(rbsc_ctx* ctx, void** p, size_t bytes)
+{
+    *p = nullptr;
+    if (bytes == 0) bytes = 16;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return rbsc_fail(ctx, RBSC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return RBSC_OK;
+}
+
+static void dev_free(void*& p)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+rbsc_status ensure_temp(rbsc_ctx* ctx, rbsc_graph* g, size_t bytes)
+{
+    if (g->tmp_bytes >= bytes) return RBSC_OK;
+    dev_free(g->d_tmp);
+    g->tmp_bytes = 0;
+    CKS(dev_alloc(ctx, &g->d_tmp, bytes));
+    g->tmp_bytes = bytes;
+    return RBSC_OK;
+}
+
+static unsigned grid_for(uint64_t n, unsigned threads) { return (unsigned)std::max<uint64_t>(1, ceil_div<uint64_t>(n, threads)); }
+
+// ---------------------------------------------------------------------------
+// context
+// ---------------------------------------------------------------------------
+extern "C" int32_t rbsc_abi_version(void) { return RBSC_ABI_VERSION; }
+
+extern "C" void rbsc_opts_default(rbsc_opts* o)
+{
+    std::memset(o, 0, sizeof *o);
+    o->relabel = RBSC_RELABEL_HASH;
+    o->verify = 1;
+    o->max_rounds = 0;
+    o->use_graph = 1;
+    o->seed = 0x5eed5eed12345678ull;
+    o->test_hash_bits = 0;
+}
+
+extern "C" rbsc_ctx* rbsc_ctx_create(int32_t device, const rbsc_opts* opts)
+{
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count == 0) {
+        cudaGetLastError();
+        rbsc_fail(nullptr, RBSC_ERR_CUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+        return nullptr;
+    }
+    if (device < 0 || device >= count) {
+        rbsc_fail(nullptr, RBSC_ERR_INVALID, "device %d out of range (have %d)", device, count);
+        return nullptr;
+    }
+    rbsc_ctx* ctx = new (std::nothrow) rbsc_ctx();
+    if (!ctx) {
+        rbsc_fail(nullptr, RBSC_ERR_OOM, "out of host memory");
+        return nullptr;
+    }
+    ctx->device = device;
+    if (opts) ctx->opts = *opts;
+    else rbsc_opts_default(&ctx->opts);
+    if ((e = cudaSetDevice(device)) != cudaSuccess || (e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking)) != cudaSuccess) {
+        rbsc_fail(nullptr, RBSC_ERR_CUDA, "context setup failed: %s", cudaGetErrorString(e));
+        delete ctx;
+        return nullptr;
+    }
+    for (auto& ev : ctx->ev) cudaEventCreate(&ev);
+    cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
+    return ctx;
+}
+
+extern "C" void rbsc_ctx_destroy(rbsc_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto& ev : ctx->ev) cudaEventDestroy(ev);
+    cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+extern "C" const char* rbsc_last_error(const rbsc_ctx* ctx)
+{
+    return ctx ? ctx->err.c_str() : g_global_error.c_str();
+}
+
+extern "C" rbsc_status rbsc_ctx_set_opts(rbsc_ctx* ctx, const rbsc_opts* opts)
+{
+    if (!ctx || !opts) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    ctx->opts = *opts;
+    return RBSC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// resident graph
+// ---------------------------------------------------------------------------
+static void graph_release_refine(rbsc_graph* g)
+{
+    if (g->loop_exec) cudaGraphExecDestroy(g->loop_exec);
+    if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
+    g->loop_exec = nullptr;
+    g->loop_graph = nullptr;
+    dev_free((void*&)g->d_col[0]);
+    dev_free((void*&)g->d_col[1]);
+    dev_free((void*&)g->d_initlab);
+    dev_free((void*&)g->d_sig1);
+    dev_free((void*&)g->d_sig2);
+    dev_free((void*&)g->d_slot);
+    dev_free((void*&)g->d_tab);
+    dev_free((void*&)g->d_st);
+    dev_free((void*&)g->d_out);
+    dev_free((void*&)g->d_init);
+    dev_free((void*&)g->d_vflag);
+    dev_free((void*&)g->d_vdeg);
+    dev_free((void*&)g->d_fail);
+    dev_free((void*&)g->d_keys[0]);
+    dev_free((void*&)g->d_keys[1]);
+    dev_free((void*&)g->d_vals[0]);
+    dev_free((void*&)g->d_vals[1]);
+    dev_free((void*&)g->d_small);
+    dev_free(g->d_tmp);
+    g->tmp_bytes = 0;
+    g->key_cap = 0;
+    if (g->h_st) cudaFreeHost(g->h_st);
+    g->h_st = nullptr;
+    g->bufs = false;
+    sortrelabel_release(g);
+}
+
+extern "C" void rbsc_graph_free(rbsc_graph* g)
+{
+    if (!g) return;
+    cudaSetDevice(g->ctx->device);
+    cudaStreamSynchronize(g->ctx->stream);
+    graph_release_refine(g);
+    dev_free((void*&)g->d_off);
+    dev_free((void*&)g->d_idx);
+    dev_free((void*&)g->d_wt);
+    dev_free((void*&)g->d_rows);
+    dev_free(g->d_roff);
+    dev_free((void*&)g->d_tile_row);
+    dev_free((void*&)g->d_split);
+    delete g;
+}
+
+extern "C" rbsc_status rbsc_graph_info(const rbsc_graph* g, uint32_t* n, uint64_t* m)
+{
+    if (!g) return RBSC_ERR_INVALID;
+    if (n) *n = g->n;
+    if (m) *m = g->m;
+    return RBSC_OK;
+}
+
+extern "C" rbsc_status rbsc_graph_device_csr(const rbsc_graph* g, const uint64_t** d_offsets, const uint32_t** d_indices)
+{
+    if (!g) return RBSC_ERR_INVALID;
+    if (d_offsets) *d_offsets = g->d_off;
+    if (d_indices) *d_indices = g->d_idx;
+    return RBSC_OK;
+}
+
+// Builds the tiling of a graph whose d_off / d_idx / d_wt are in place.
+rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
+{
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = g->n;
+    const uint64_t m = g->m;
+    g->off32 = m < (1ull << 32);
+    // validation (device-side, one error word)
+    uint32_t* d_err = nullptr;
+    CKS(dev_alloc(ctx, (void**)&d_err, sizeof(uint32_t) * 4));
+    struct Guard { uint32_t*& p; ~Guard() { if (p) cudaFree(p); } } guard{d_err};
+    CK(cudaMemsetAsync(d_err, 0, sizeof(uint32_t) * 4, s));
+    ++rbsc::launch_counter();
+    k_validate<<<grid_for(std::max<uint64_t>(n, 1), 256) > 65535u * 16 ? 65535u * 16 : grid_for(std::max<uint64_t>(n, 1), 256), 256, 0, s>>>(n, m, g->d_off, g->d_idx, d_err);
+    CK(cudaGetLastError());
+    uint32_t herr = 0;
+    CK(cudaMemcpyAsync(&herr, d_err, sizeof herr, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (herr & 3u) return rbsc_fail(ctx, RBSC_ERR_INVALID, "offsets are not a valid CSR (must start at 0, be non-decreasing and end at M)");
+    if (herr & 4u) return rbsc_fail(ctx, RBSC_ERR_INVALID, "an arc head is >= N");
+
+    // non-empty rows
+    CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)n + 1) + 1024));
+    uint32_t* d_pos = nullptr;
+    CKS(dev_alloc(ctx, (void**)&d_pos, sizeof(uint32_t) * ((size_t)n + 1)));
+    struct Guard2 { uint32_t*& p; ~Guard2() { if (p) cudaFree(p); } } guard2{d_pos};
+    ++rbsc::launch_counter();
+    k_nonempty_flags<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, d_pos);
+    CK(cudaGetLastError());
+    CK((exclusive_scan<uint32_t, uint32_t>(d_pos, d_pos, n, d_err + 1, g->d_tmp, s)));
+    uint32_t K = 0;
+    CK(cudaMemcpyAsync(&K, d_err + 1, sizeof K, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    g->K = K;
+    CKS(dev_alloc(ctx, (void**)&g->d_rows, sizeof(uint32_t) * std::max<uint32_t>(K, 1)));
+    CKS(dev_alloc(ctx, &g->d_roff, (g->off32 ? 4 : 8) * ((size_t)K + 1)));
+    if (g->off32) {
+        ++rbsc::launch_counter();
+        k_compact_rows<uint32_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint32_t*)g->d_roff);
+    }
+    else {
+        ++rbsc::launch_counter();
+        k_compact_rows<uint64_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint64_t*)g->d_roff);
+    }
+    CK(cudaGetLastError());
+    // tiles
+    g->ntiles = (uint32_t)ceil_div<uint64_t>(m, kTileEdges);
+    CKS(dev_alloc(ctx, (void**)&g->d_tile_row, sizeof(uint32_t) * ((size_t)g->ntiles + 1)));
+    if (g->off32) {
+        ++rbsc::launch_counter();
+        k_tile_rows<uint32_t><<<grid_for((uint64_t)g->ntiles + 1, 256), 256, 0, s>>>(g->ntiles, K, (const uint32_t*)g->d_roff, g->d_tile_row);
+    }
+    else {
+        ++rbsc::launch_counter();
+        k_tile_rows<uint64_t><<<grid_for((uint64_t)g->ntiles + 1, 256), 256, 0, s>>>(g->ntiles, K, (const uint64_t*)g->d_roff, g->d_tile_row);
+    }
+    CK(cudaGetLastError());
+    // rows split across tiles
+    if (K > 0) {
+        CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)K + 1) + 1024));
+        uint32_t* d_sp = nullptr;
+        CKS(dev_alloc(ctx, (void**)&d_sp, sizeof(uint32_t) * ((size_t)K + 1)));
+        struct Guard3 { uint32_t*& p; ~Guard3() { if (p) cudaFree(p); } } guard3{d_sp};
+        if (g->off32) {
+            ++rbsc::launch_counter();
+            k_split_flags<uint32_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint32_t*)g->d_roff, d_sp);
+        }
+        else {
+            ++rbsc::launch_counter();
+            k_split_flags<uint64_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint64_t*)g->d_roff, d_sp);
+        }
+        CK(cudaGetLastError());
+        CK((exclusive_scan<uint32_t, uint32_t>(d_sp, d_sp, K, d_err + 2, g->d_tmp, s)));
+        uint32_t ns = 0;
+        CK(cudaMemcpyAsync(&ns, d_err + 2, sizeof ns, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        g->nsplit = ns;
+        CKS(dev_alloc(ctx, (void**)&g->d_split, sizeof(uint32_t) * std::max<uint32_t>(ns, 1)));
+        if (g->off32) {
+            ++rbsc::launch_counter();
+            k_split_compact<uint32_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint32_t*)g->d_roff, g->d_rows, d_sp, g->d_split);
+        }
+        else {
+            ++rbsc::launch_counter();
+            k_split_compact<uint64_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint64_t*)g->d_roff, g->d_rows, d_sp, g->d_split);
+        }
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(s));
+    } else {
+        g->nsplit = 0;
+        CKS(dev_alloc(ctx, (void**)&g->d_split, sizeof(uint32_t)));
+    }
+    return RBSC_OK;
+}
+
+static rbsc_status check_csr_args(rbsc_ctx* ctx, const rbsc_csr* c)
+{
+    if (!ctx) return rbsc_fail(nullptr, RBSC_ERR_INVALID, "null context");
+    if (!c) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null graph");
+    if (c->n >= 0x80000000u) return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "N = %u: node ids must be < 2^31", c->n);
+    if (c->offset_bytes != 4 && c->offset_bytes != 8) return rbsc_fail(ctx, RBSC_ERR_INVALID, "offset_bytes must be 4 or 8");
+    if (c->offset_bytes == 4 && c->m >= (1ull << 32)) return rbsc_fail(ctx, RBSC_ERR_INVALID, "M >= 2^32 needs 8-byte offsets");
+    if (!c->offsets) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null offsets");
+    if (c->m > 0 && !c->indices) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null indices");
+    return RBSC_OK;
+}
+
+// Allocates the CSR arrays of g (indices / weights padded to whole tiles).
+rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted)
+{
+    const uint64_t padded = ceil_div<uint64_t>(std::max<uint64_t>(g->m, 1), kTileEdges) * kTileEdges;
+    g->weighted = weighted;
+    CKS(dev_alloc(ctx, (void**)&g->d_off, sizeof(uint64_t) * ((size_t)g->n + 1)));
+    CKS(dev_alloc(ctx, (void**)&g->d_idx, sizeof(uint32_t) * padded));
+    if (padded > g->m) CK(cudaMemsetAsync(g->d_idx + g->m, 0, sizeof(uint32_t) * (padded - g->m), ctx->stream));
+    if (weighted) {
+        CKS(dev_alloc(ctx, (void**)&g->d_wt, sizeof(uint64_t) * padded));
+        if (padded > g->m) CK(cudaMemsetAsync(g->d_wt + g->m, 0, sizeof(uint64_t) * (padded - g->m), ctx->stream));
+    }
+    return RBSC_OK;
+}
+
+static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device, rbsc_graph** out, double* h2d_ms,
+                              uint64_t* h2d_bytes)
+{
+    *out = nullptr;
+    CKS(check_csr_args(ctx, c));
+    CK(cudaSetDevice(ctx->device));
+    rbsc_graph* g = new (std::nothrow) rbsc_graph();
+    if (!g) return rbsc_fail(ctx, RBSC_ERR_OOM, "out of host memory");
+    g->ctx = ctx;
+    g->n = c->n;
+    g->m = c->m;
+    rbsc_status st = graph_alloc_csr(ctx, g, c->weights != nullptr);
+    if (st != RBSC_OK) {
+        rbsc_graph_free(g);
+        return st;
+    }
+    cudaStream_t s = ctx->stream;
+    const cudaMemcpyKind kind = from_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    auto t0 = std::chrono::steady_clock::now();
+    cudaError_t e = cudaSuccess;
+    const size_t offb = (size_t)c->offset_bytes * ((size_t)c->n + 1);
+    uint64_t bytes = offb + sizeof(uint32_t) * c->m + (c->weights ? sizeof(uint64_t) * c->m : 0);
+    if (c->offset_bytes == 8) {
+        e = cudaMemcpyAsync(g->d_off, c->offsets, offb, kind, s);
+    } else {
+        // stage the 32-bit offsets in the (not yet used) index buffer tail? use a scratch buffer
+        void* tmp = nullptr;
+        st = dev_alloc(ctx, &tmp, offb);
+        if (st != RBSC_OK) {
+            rbsc_graph_free(g);
+            return st;
+        }
+        e = cudaMemcpyAsync(tmp, c->offsets, offb, kind, s);
+        if (e == cudaSuccess) {
+            ++rbsc::launch_counter();
+            k_widen_offsets<uint32_t><<<grid_for((uint64_t)c->n + 1, 256), 256, 0, s>>>((uint64_t)c->n + 1, (const uint32_t*)tmp, g->d_off);
+            e = cudaGetLastError();
+        }
+        cudaStreamSynchronize(s);
+        cudaFree(tmp);
+    }
+    if (e == cudaSuccess && c->m) e = cudaMemcpyAsync(g->d_idx, c->indices, sizeof(uint32_t) * c->m, kind, s);
+    if (e == cudaSuccess && c->weights && c->m) e = cudaMemcpyAsync(g->d_wt, c->weights, sizeof(uint64_t) * c->m, kind, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    auto t1 = std::chrono::steady_clock::now();
+    if (h2d_ms) *h2d_ms = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (h2d_bytes) *h2d_bytes = from_device ? 0 : bytes;
+    if (e != cudaSuccess) {
+        rbsc_cuda_fail(ctx, e, "graph copy", __LINE__);
+        rbsc_graph_free(g);
+        return e == cudaErrorMemoryAllocation ? RBSC_ERR_OOM : RBSC_ERR_CUDA;
+    }
+    st = graph_prepare(ctx, g);
+    if (st != RBSC_OK) {
+        rbsc_graph_free(g);
+        return st;
+    }
+    *out = g;
+    return RBSC_OK;
+}
+
+extern "C" rbsc_status rbsc_graph_upload(rbsc_ctx* ctx, const rbsc_csr* host_graph, rbsc_graph** out)
+{
+    if (!out) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null output");
+    return graph_load(ctx, host_graph, false, out, nullptr, nullptr);
+}
+
+extern "C" rbsc_status rbsc_graph_from_device(rbsc_ctx* ctx, const rbsc_csr* device_graph, rbsc_graph** out)
+{
+    if (!out) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null output");
+    return graph_load(ctx, device_graph, true, out, nullptr, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// refinement
+// ---------------------------------------------------------------------------
+static uint32_t log2_ceil(uint64_t x)
+{
+    uint32_t r = 0;
+    while ((1ull << r) < x) ++r;
+    return r;
+}
+
+static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
+{
+    if (g->bufs) return RBSC_OK;
+    const size_t n = std::max<uint32_t>(g->n, 1);
+    CKS(dev_alloc(ctx, (void**)&g->d_col[0], 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_col[1], 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_initlab, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_sig1, 8 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_sig2, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_slot, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_out, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_small, 256));
+    g->log2tab = std::max<uint32_t>(10, log2_ceil(2ull * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
+    CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
+    CK(cudaMallocHost((void**)&g->h_st, sizeof(RoundState)));
+    CK(cudaMemsetAsync(g->d_sig1, 0, 8 * n, ctx->stream));
+    CK(cudaMemsetAsync(g->d_sig2, 0, 4 * n, ctx->stream));
+    CK(cudaMemsetAsync(g->d_tab, 0, sizeof(Entry) << g->log2tab, ctx->stream));
+    g->next_stamp = 1;
+    g->bufs = true;
+    return RBSC_OK;
+}
+
+// CUDA events around the kernels of one pass (profiling only).
+struct PassTimer {
+    cudaEvent_t ev[6];
+};
+
+// Launches the kernels of one hashed pass on stream s (also used for capture).
+static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle,
+                               PassTimer* t = nullptr)
+{
+    const uint32_t n = g->n;
+    const unsigned clear_grid = (unsigned)std::min<uint64_t>(ctx->sm_count * 8ull, grid_for(1ull << g->log2tab, 256));
+    if (t) CK(cudaEventRecord(t->ev[0], s));
+    ++rbsc::launch_counter();
+    k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
+    if (t) CK(cudaEventRecord(t->ev[1], s));
+    if (g->m > 0) {
+        const unsigned tiles = g->ntiles;
+        if (g->off32) {
+            if (g->weighted) {
+                ++rbsc::launch_counter();
+                k_signature<uint32_t, true><<<tiles, kTileThreads, 0, s>>>((const uint32_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            }
+            else {
+                ++rbsc::launch_counter();
+                k_signature<uint32_t, false><<<tiles, kTileThreads, 0, s>>>((const uint32_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            }
+        } else {
+            if (g->weighted) {
+                ++rbsc::launch_counter();
+                k_signature<uint64_t, true><<<tiles, kTileThreads, 0, s>>>((const uint64_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            }
+            else {
+                ++rbsc::launch_counter();
+                k_signature<uint64_t, false><<<tiles, kTileThreads, 0, s>>>((const uint64_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            }
+        }
+    }
+    if (t) CK(cudaEventRecord(t->ev[2], s));
+    if (ctx->opts.relabel == RBSC_RELABEL_SORT) {
+        CKS(launch_sort_relabel(ctx, g, s));
+        if (t) CK(cudaEventRecord(t->ev[3], s));
+    } else {
+        ++rbsc::launch_counter();
+        k_insert<kModeHash><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, nullptr, g->d_tab, g->log2tab, g->d_slot);
+        if (t) CK(cudaEventRecord(t->ev[3], s));
+        ++rbsc::launch_counter();
+        k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
+    }
+    if (t) CK(cudaEventRecord(t->ev[4], s));
+    ++rbsc::launch_counter();
+    k_fixpoint<kModeHash><<<1, 1, 0, s>>>(g->d_st, h, use_handle);
+    if (t) CK(cudaEventRecord(t->ev[5], s));
+    CK(cudaGetLastError());
+    return RBSC_OK;
+}
+
+static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
+{
+    if (g->loop_exec && g->loop_relabel == ctx->opts.relabel) return RBSC_OK;
+    if (g->loop_exec) cudaGraphExecDestroy(g->loop_exec);
+    if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
+    g->loop_exec = nullptr;
+    g->loop_graph = nullptr;
+    CKS(ensure_sort_relabel_bufs(ctx, g));
+    CK(cudaGraphCreate(&g->loop_graph, 0));
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g->loop_graph, 1, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    CK(cudaGraphAddNode(&node, g->loop_graph, nullptr, 0, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    CK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        cudaStreamDestroy(cs);
+        return rbsc_cuda_fail(ctx, e, "cudaStreamBeginCaptureToGraph", __LINE__);
+    }
+    const uint64_t lc0 = rbsc::launch_counter();
+    rbsc_status st = launch_pass(ctx, g, cs, h, 1);
+    g->body_kernels = rbsc::launch_counter() - lc0;
+    rbsc::launch_counter() = lc0;  // captured, not launched
+    cudaGraph_t captured = nullptr;
+    e = cudaStreamEndCapture(cs, &captured);
+    cudaStreamDestroy(cs);
+    if (st != RBSC_OK) return st;
+    if (e != cudaSuccess) return rbsc_cuda_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
+    CK(cudaGraphInstantiate(&g->loop_exec, g->loop_graph, 0));
+    g->loop_relabel = ctx->opts.relabel;
+    return RBSC_OK;
+}
+
+static rbsc_status read_state(rbsc_ctx* ctx, rbsc_graph* g)
+{
+    CK(cudaMemcpyAsync(g->h_st, g->d_st, sizeof(RoundState), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return RBSC_OK;
+}
+
+static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels)
+{
+    if (ctx->opts.use_graph && !kt) {
+        CKS(build_loop_graph(ctx, g));
+        const uint32_t r0 = g->h_st->round;
+        CK(cudaGraphLaunch(g->loop_exec, ctx->stream));
+        CKS(read_state(ctx, g));
+        *graph_kernels += g->body_kernels * (uint64_t)(g->h_st->round - r0);
+    } else {
+        CKS(ensure_sort_relabel_bufs(ctx, g));
+        PassTimer t;
+        if (kt)
+            for (auto& e : t.ev) CK(cudaEventCreate(&e));
+        for (;;) {
+            rbsc_status st = launch_pass(ctx, g, ctx->stream, cudaGraphConditionalHandle(), 0, kt ? &t : nullptr);
+            if (st == RBSC_OK) st = read_state(ctx, g);
+            if (st == RBSC_OK && kt) {
+                float ms[5];
+                for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], t.ev[i], t.ev[i + 1]);
+                kt->passes += 1;
+                kt->other_ms += ms[0] + ms[4];
+                kt->signature_ms += ms[1];
+                kt->insert_ms += ms[2];
+                kt->relabel_ms += ms[3];
+            }
+            if (st != RBSC_OK || g->h_st->done || g->h_st->error) {
+                if (kt)
+                    for (auto& e : t.ev) cudaEventDestroy(e);
+                if (st != RBSC_OK) return st;
+                break;
+            }
+        }
+    }
+    return RBSC_OK;
+}
+
+// Exact check of the current fixpoint.  Returns the number of failing nodes in
+// *nfail (0 = the partition is the coarsest stable one).
+static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t parity, uint32_t* nfail)
+{
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = g->n;
+    const uint32_t* col = g->d_col[parity];
+    if (!g->d_vflag) {
+        CKS(dev_alloc(ctx, (void**)&g->d_vflag, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vdeg, 8 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_fail, 4 * ((size_t)n + 1)));
+    }
+    CKS(ensure_temp(ctx, g, scan_temp_bytes<uint64_t>((uint64_t)n + 1) + 1024));
+    uint64_t* d_tot = (uint64_t*)g->d_small;  // [0] rows (u32 in a u64 slot), [1] keys, [2] nfail
+    CK(cudaMemsetAsync(d_tot, 0, 64, s));
+    ++rbsc::launch_counter();
+    k_verify_mark<<<grid_for(n, 256), 256, 0, s>>>(n, col, g->d_off, g->d_vflag, g->d_vdeg);
+    CK(cudaGetLastError());
+    CK((exclusive_scan<uint32_t, uint32_t>(g->d_vflag, g->d_vflag, n, (uint32_t*)d_tot, g->d_tmp, s)));
+    CK((exclusive_scan<uint64_t, uint64_t>(g->d_vdeg, g->d_vdeg, n, d_tot + 1, g->d_tmp, s)));
+    uint64_t tot[2];
+    CK(cudaMemcpyAsync(tot, d_tot, sizeof tot, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const uint32_t nrows = (uint32_t)tot[0];
+    const uint64_t nkeys = tot[1];
+    if (nkeys >= (1ull << 32)) return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "exact check: %llu arcs in non-singleton rows (limit 2^32)", (unsigned long long)nkeys);
+    if (nkeys > g->key_cap) {
+        dev_free((void*&)g->d_keys[0]);
+        dev_free((void*&)g->d_keys[1]);
+        dev_free((void*&)g->d_vals[0]);
+        dev_free((void*&)g->d_vals[1]);
+        g->key_cap = 0;
+        CKS(dev_alloc(ctx, (void**)&g->d_keys[0], 8 * nkeys));
+        CKS(dev_alloc(ctx, (void**)&g->d_keys[1], 8 * nkeys));
+        if (g->weighted) {
+            CKS(dev_alloc(ctx, (void**)&g->d_vals[0], 8 * nkeys));
+            CKS(dev_alloc(ctx, (void**)&g->d_vals[1], 8 * nkeys));
+        }
+        g->key_cap = nkeys;
+    }
+    const unsigned long long* keys = g->d_keys[0];
+    const unsigned long long* vals = g->weighted ? g->d_vals[0] : nullptr;
+    if (nkeys > 0) {
+        ++rbsc::launch_counter();
+        k_verify_keys<<<grid_for(n, 128), 128, 0, s>>>(n, col, g->d_off, g->d_idx, g->d_wt, g->d_vflag, g->d_vdeg, g->d_keys[0], g->weighted ? g->d_vals[0] : nullptr);
+        CK(cudaGetLastError());
+        CKS(ensure_temp(ctx, g, radix_temp_bytes(nkeys)));
+        const int bits = 31 + (int)log2_ceil(std::max<uint32_t>(nrows, 1));
+        bool in_alt = false;
+        CK(radix_sort<unsigned long long>(g->d_keys[0], g->d_keys[1], g->weighted ? g->d_vals[0] : (unsigned long long*)nullptr,
+                                          g->weighted ? g->d_vals[1] : (unsigned long long*)nullptr, nkeys, 0, bits, g->d_tmp, s, &in_alt));
+        if (in_alt) {
+            keys = g->d_keys[1];
+            vals = g->weighted ? g->d_vals[1] : nullptr;
+        }
+    }
+    CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
+    const unsigned cgrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 16, grid_for((uint64_t)n * 32, 256));
+    ++rbsc::launch_counter();
+    k_verify_compare<<<cgrid, 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->d_vdeg, keys, vals, g->d_fail, (uint32_t*)(d_tot + 2));
+    CK(cudaGetLastError());
+    uint32_t hf = 0;
+    CK(cudaMemcpyAsync(&hf, d_tot + 2, sizeof hf, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    *nfail = hf;
+    return RBSC_OK;
+}
+
+// Splits the nodes that failed the exact check away from their blocks.
+static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
+{
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = g->n;
+    const unsigned clear_grid = (unsigned)std::min<uint64_t>(ctx->sm_count * 8ull, grid_for(1ull << g->log2tab, 256));
+    ++rbsc::launch_counter();
+    k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
+    ++rbsc::launch_counter();
+    k_insert<kModeRepair><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, g->d_fail, g->d_tab, g->log2tab, g->d_slot);
+    ++rbsc::launch_counter();
+    k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, 0, g->d_sig1, g->d_sig2);
+    ++rbsc::launch_counter();
+    k_fixpoint<kModeRepair><<<1, 1, 0, s>>>(g->d_st, cudaGraphConditionalHandle(), 0);
+    CK(cudaGetLastError());
+    return RBSC_OK;
+}
+
+// The whole refinement of a resident graph, device pointers in and out.
+rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init, uint32_t* d_out, rbsc_stats* stats,
+                            rbsc_kernel_times* kt)
+{
+    CK(cudaSetDevice(ctx->device));
+    const uint64_t lc0 = rbsc::launch_counter();
+    uint64_t graph_kernels = 0;
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = g->n;
+    if (stats) std::memset(stats, 0, sizeof *stats);
+    if (n == 0) {
+        if (stats) stats->done = stats->verified = 1;
+        return RBSC_OK;
+    }
+    CKS(ensure_refine_bufs(ctx, g));
+    RoundState& hs = *g->h_st;
+    std::memset(&hs, 0, sizeof hs);
+    hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);
+    hs.seed = ctx->opts.seed;
+    hs.hash_bits = (uint32_t)std::max(0, ctx->opts.test_hash_bits);
+    hs.stamp = g->next_stamp;
+    hs.clear_pending = 0;
+    CK(cudaEventRecord(ctx->ev[0], s));
+    uint32_t parity = 0;
+    if (d_init) {
+        hs.parity = 0;
+        CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(g->d_col[0], 0, 4 * (size_t)n, s));
+        ++rbsc::launch_counter();
+        k_insert<kModeInit><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, d_init, g->d_tab, g->log2tab, g->d_slot);
+        ++rbsc::launch_counter();
+        k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
+        ++rbsc::launch_counter();
+        k_fixpoint<kModeInit><<<1, 1, 0, s>>>(g->d_st, cudaGraphConditionalHandle(), 0);
+        CK(cudaGetLastError());
+        parity = 1;
+    } else {
+        hs.parity = 0;
+        hs.prev = 1;
+        hs.round_blocks[0] = 1;
+        CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
+        ++rbsc::launch_counter();
+        k_fill_uniform<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0]);
+        CK(cudaGetLastError());
+    }
+    ++rbsc::launch_counter();
+    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[parity], g->d_initlab);
+    CK(cudaGetLastError());
+    CKS(read_state(ctx, g));
+    const uint32_t initial_blocks = hs.prev;
+
+    float verify_ms = 0.f;
+    uint32_t repairs = 0;
+    for (;;) {
+        if (hs.error) break;
+        CKS(run_loop(ctx, g, kt, &graph_kernels));
+        if (hs.error) break;
+        if (!ctx->opts.verify) break;
+        CK(cudaEventRecord(ctx->ev[2], s));
+        uint32_t nfail = 0;
+        CKS(verify_fixpoint(ctx, g, hs.parity, &nfail));
+        CK(cudaEventRecord(ctx->ev[3], s));
+        CK(cudaEventSynchronize(ctx->ev[3]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        verify_ms += ms;
+        if (nfail == 0) break;
+        ++repairs;
+        CKS(repair_pass(ctx, g));
+        CKS(read_state(ctx, g));
+    }
+    g->next_stamp = hs.stamp;
+    if (hs.error & kErrProbe) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "relabel table overflow");
+    if (hs.error & kErrRounds) return rbsc_fail(ctx, RBSC_ERR_NOT_CONVERGED, "no fixpoint after %u passes", hs.round);
+    uint32_t* out = d_out ? d_out : g->d_out;
+    ++rbsc::launch_counter();
+    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[hs.parity], out);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[1], s));
+    CK(cudaEventSynchronize(ctx->ev[1]));
+    float total_ms = 0.f;
+    cudaEventElapsedTime(&total_ms, ctx->ev[0], ctx->ev[1]);
+    if (stats) {
+        stats->rounds = hs.round;
+        stats->blocks = hs.prev;
+        stats->done = 1;
+        stats->verified = ctx->opts.verify ? 1u : 0u;
+        stats->repairs = repairs;
+        stats->initial_blocks = initial_blocks;
+        stats->device_ms = total_ms;
+        stats->verify_ms = verify_ms;
+        for (int i = 0; i < 64 && i < kRoundLog; ++i) stats->round_blocks[i] = hs.round_blocks[i];
+        stats->kernel_launches = rbsc::launch_counter() - lc0 + graph_kernels;
+    }
+    if (kt) kt->total_ms = total_ms;
+    return RBSC_OK;
+}
+
+extern "C" rbsc_status rbsc_graph_profile(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init_colors,
+                                          rbsc_kernel_times* times, rbsc_stats* stats)
+{
+    if (!ctx || !g || !times) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    std::memset(times, 0, sizeof *times);
+    return refine_resident(ctx, g, d_init_colors, nullptr, stats, times);
+}
+
+extern "C" rbsc_status rbsc_graph_refine_device(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init_colors,
+                                                uint32_t* d_out_labels, rbsc_stats* stats)
+{
+    if (!ctx || !g) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    auto t0 = std::chrono::steady_clock::now();
+    rbsc_status st = refine_resident(ctx, g, d_init_colors, d_out_labels, stats, nullptr);
+    if (st == RBSC_OK && stats)
+        stats->time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    return st;
+}
+
+extern "C" rbsc_status rbsc_graph_refine(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* init_colors, uint32_t* out_labels,
+                                         rbsc_stats* stats)
+{
+    if (!ctx || !g) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    auto t0 = std::chrono::steady_clock::now();
+    CKS(ensure_refine_bufs(ctx, g));
+    double h2d = 0, d2h = 0;
+    const uint32_t* d_init = nullptr;
+    if (init_colors && g->n) {
+        if (!g->d_init) CKS(dev_alloc(ctx, (void**)&g->d_init, 4 * (size_t)g->n));
+        auto a = std::chrono::steady_clock::now();
+        CK(cudaMemcpyAsync(g->d_init, init_colors, 4 * (size_t)g->n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        h2d = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+        d_init = g->d_init;
+    }
+    CKS(refine_resident(ctx, g, d_init, nullptr, stats, nullptr));
+    if (out_labels && g->n) {
+        auto a = std::chrono::steady_clock::now();
+        CK(cudaMemcpyAsync(out_labels, g->d_out, 4 * (size_t)g->n, cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+        d2h = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a).count();
+    }
+    if (stats) {
+        stats->h2d_ms = h2d;
+        stats->d2h_ms = d2h;
+        stats->h2d_bytes = init_colors ? 4ull * g->n : 0;
+        stats->d2h_bytes = out_labels ? 4ull * g->n : 0;
+        stats->time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return RBSC_OK;
+}
+
+extern "C" rbsc_status rbsc_refine(rbsc_ctx* ctx, const rbsc_csr* host_graph, const uint32_t* init_colors,
+                                   uint32_t* out_labels, rbsc_stats* stats)
+{
+    if (!ctx) return rbsc_fail(nullptr, RBSC_ERR_INVALID, "null context");
+    auto t0 = std::chrono::steady_clock::now();
+    rbsc_graph* g = nullptr;
+    double up_ms = 0;
+    uint64_t up_bytes = 0;
+    CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes));
+    rbsc_status st = rbsc_graph_refine(ctx, g, init_colors, out_labels, stats);
+    rbsc_graph_free(g);
+    if (st == RBSC_OK && stats) {
+        stats->h2d_ms += up_ms;
+        stats->h2d_bytes += up_bytes;
+        stats->time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return st;
+}
+
+extern "C" rbsc_status rbsc_graph_degree_colors(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* d_colors)
+{
+    if (!ctx || !g || !d_colors) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    CK(cudaSetDevice(ctx->device));
+    if (g->n) {
+        ++rbsc::launch_counter();
+        k_degree_colors<<<grid_for(g->n, 256), 256, 0, ctx->stream>>>(g->n, g->d_off, d_colors);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return RBSC_OK;
+}

@@ -1,0 +1,100 @@
+"""C ABI checks that need no GPU: librbsc.so loads, exports every function
+include/rbsc.h declares, and its host-only entry points (arcs-cuda parser,
+host R-MAT generator) behave; the CLI fails loudly without a device."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from rbsc_b200 import _lib, graphs as G
+import rbsc_b200 as R
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    txt = open(os.path.join(ROOT, "include", "rbsc.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(rbsc_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _lib.load()
+    declared = _declared()
+    assert declared, "no declarations found"
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert set(declared) == set(_lib.EXPORTED)
+    assert lib.rbsc_abi_version() == 1
+
+
+def test_exports_via_nm():
+    out = subprocess.run(["nm", "-D", "--defined-only", _lib.LIB_PATH], capture_output=True, text=True).stdout
+    syms = {ln.split()[-1] for ln in out.splitlines() if ln.strip()}
+    for name in _declared():
+        assert name in syms, name
+
+
+def test_no_device_gives_error_not_crash():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    with pytest.raises(R.RbscError):
+        R.Context(0)
+
+
+def test_parse_arcs_roundtrip():
+    off, idx = G.rmat(8, 4, seed=1)
+    from oracle import oracle
+    text = oracle.arcs_cuda_text(off, idx)
+    o2, i2, w2 = R.parse_arcs(text)
+    assert np.array_equal(off, o2) and np.array_equal(idx, i2) and w2 is None
+
+
+def test_parse_weighted_and_unsorted_groups():
+    text = b"4\n5\n2 3 0\n2 1 1\n0 7 3\n3 1 1\n1 1 2\n"
+    off, idx, wt = R.parse_arcs(text)
+    assert off.tolist() == [0, 1, 2, 4, 5]
+    assert idx.tolist() == [3, 2, 0, 1, 1]
+    assert wt.tolist() == [7, 1, 3, 1, 1]
+
+
+@pytest.mark.parametrize("text,msg", [
+    (b"3\n2\n0 1 1\n", "arcs"),                 # fewer arcs than announced
+    (b"3\n1\n0 1 5\n", "range"),                # head out of range
+    (b"3\n2\n0 1 1\n0 x 2\n", "malformed"),     # bad token
+    (b"3\n3\n0 1 1\n1 1 2\n0 1 2\n", "grouped"),  # source 0 split in two runs
+    (b"", "node count"),
+])
+def test_parse_rejects_malformed(text, msg):
+    with pytest.raises(R.RbscError) as e:
+        R.parse_arcs(text)
+    assert msg in str(e.value)
+
+
+def test_parse_no_trailing_newline():
+    off, idx, wt = R.parse_arcs(b"2\n1\n0 1 1")
+    assert off.tolist() == [0, 1, 1] and idx.tolist() == [1]
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(6, 4, 1), (10, 16, 3), (12, 8, 9)])
+def test_host_rmat_matches_numpy(scale, ef, seed):
+    o1, i1 = G.rmat(scale, ef, seed=seed)
+    o2, i2 = R.gen_rmat_host(scale, ef, seed=seed)
+    assert np.array_equal(o1, o2) and np.array_equal(i1, i2)
+
+
+def test_cli_fails_loudly_without_device():
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    r = subprocess.run([_lib.CLI_PATH], input=b"2\n1\n0 1 1\n", capture_output=True, timeout=60)
+    assert r.returncode != 0
+    assert b"CUDA" in r.stdout or b"failed" in r.stdout
+
+
+def test_cli_parse_error_on_stdout():
+    r = subprocess.run([_lib.CLI_PATH], input=b"2\n3\n0 1 1\n", capture_output=True, timeout=60)
+    assert r.returncode != 0 and b"input error" in r.stdout
