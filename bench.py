@@ -1,0 +1,342 @@
+"""bench.py -- colour refinement of R-MAT-24 on B200: edge-rounds/s.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the plain-refinement-at-scale configuration): directed R-MAT scale
+24, edge factor 16, (a, b, c) = (0.57, 0.19, 0.19), duplicates and self-loops
+removed, CSR with int64 offsets and int32 heads, initial colours
+floor(log2(out_degree + 1)), refined to the fixpoint.  Synthetic and seeded:
+the reference's own suite (LAW web graphs) is not available.
+
+One step = one refinement of the resident graph from its initial colours to
+the verified fixpoint (time-to-fixpoint).  metric = arcs x rounds / time.
+The inputs (1 GB of heads, 134 MB of offsets) are larger than the 126 MB L2,
+so no flush is needed between steps.
+
+Multi-GPU: the path does not shard here (one graph, one GPU); N ranks run N
+independent replicas, `value` is the sum over ranks of arcs x rounds divided
+by the slowest rank's time.
+
+--impl reference: the reference's own CPU program (src/rsc/rsc.cpp, compiled
+unmodified into oracle/_ref/ref_rsc) on a bounded sample of the workload
+(R-MAT scale 20, same generator and parameters), timed by its own internal
+refinement timer, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "edge-rounds/s (R-MAT-24 colour refinement to the verified fixpoint)"
+UNIT = "edge-rounds/s"
+SAMPLE_SCALE = 20
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def signature_traffic_per_arc():
+    """DRAM bytes per arc of k_signature from the committed ncu summary
+    (profiles/k_signature_rmat.md, line 'traffic_bytes_per_arc: X'), or None."""
+    p = os.path.join(ROOT, "profiles", "k_signature_rmat.md")
+    try:
+        for ln in open(p):
+            if ln.startswith("traffic_bytes_per_arc:"):
+                return float(ln.split(":")[1])
+    except OSError:
+        pass
+    return None
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "100"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+        time.sleep(0.25)
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.15)
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.f.read().splitlines():
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_baseline_reference(steps: int = 1):
+    """The reference rsc (oracle/_ref/ref_rsc, unmodified rsc.cpp) on the R-MAT
+    scale-20 sample; falls back to the oracle's restatement of rsc when the
+    reference binary was not built.  Returns the cpu_baseline object."""
+    import numpy as np
+    import rbsc_b200 as R
+    from oracle import oracle
+    off, idx = R.gen_rmat_host(SAMPLE_SCALE, 16, seed=1)
+    m = int(off[-1])
+    sample = (f"R-MAT scale {SAMPLE_SCALE}, edge factor 16, same generator ({m} arcs after dedup), "
+              f"uniform initial colours (rsc.cpp:118-121 fixes them); refinement time from the program's own timer")
+    if os.path.exists(oracle.REF_RSC):
+        with tempfile.TemporaryDirectory() as d:
+            path = os.path.join(d, "rmat.txt")
+            oracle.write_arcs_file(path, off, idx)
+            tot_t, tot_er, runs = 0.0, 0.0, []
+            for _ in range(steps):
+                t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
+                tot_t += t
+                tot_er += m * rounds
+                runs.append(dict(time_s=t, rounds=rounds, blocks=blocks, wall_s=round(wall, 3)))
+        return {"value": tot_er / tot_t, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": sample, "runs": runs, "host_cores": os.cpu_count()}
+    t0 = time.perf_counter()
+    r = oracle.refine_rsc(off, idx)
+    t = time.perf_counter() - t0
+    return {"value": m * r.rounds_cpu / t, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
+            "host_cores": os.cpu_count()}
+
+
+def config(n=None, m=None, rounds=None):
+    return {"workload": "rmat24_ef16", "model": "none (graph refinement)", "scale": 24, "edge_factor": 16,
+            "rmat_abc": [0.57, 0.19, 0.19], "nodes": n, "arcs": m, "rounds": rounds,
+            "initial_colors": "floor(log2(out_degree+1))", "offsets": "int64", "indices": "int32",
+            "l2": "no flush: inputs larger than L2 (heads 4 B/arc)", "parallelism": "replicas",
+            "global_batch": 1, "seq_len": None}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return 0
+    import numpy as np
+    import rbsc_b200 as R
+    from oracle import oracle
+    off, idx = R.gen_rmat_host(SAMPLE_SCALE, 16, seed=1)
+    m = int(off[-1])
+    if not os.path.exists(oracle.REF_RSC):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_rsc was not built (reference tree absent at build time)"}))
+        return 0
+    with tempfile.TemporaryDirectory() as d:
+        path = os.path.join(d, "rmat.txt")
+        oracle.write_arcs_file(path, off, idx)
+        for _ in range(args.warmup):
+            oracle.run_ref_rsc_file(path)
+        tot_t, tot_er, rounds = 0.0, 0.0, None
+        for _ in range(args.steps):
+            t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
+            tot_t += t
+            tot_er += m * rounds
+    value = tot_er / tot_t
+    sample = (f"R-MAT scale {SAMPLE_SCALE}, edge factor 16, same generator ({m} arcs), uniform initial colours; "
+              f"each step one full rsc run, refinement time from rsc.cpp's own timer")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+            "config": config(), "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
+                                                 "sample": sample, "host_cores": os.cpu_count()},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "gpu_launches": 0}
+    print(json.dumps(line))
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    import rbsc_b200 as R
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local_rank))
+    ctx = R.Context(local_rank, relabel=R.RELABEL_SORT if args.relabel == "sort" else R.RELABEL_HASH)
+    g = ctx.gen_rmat(args.scale, args.ef, seed=args.seed)
+    n, m = g.n, g.m
+    d_init = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_out = torch.empty(n, dtype=torch.int32, device="cuda")
+    g.degree_colors_device(d_init.data_ptr())
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        r = g.refine_device(d_init.data_ptr(), d_out.data_ptr())
+    barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local_rank)
+    clocks.start()
+    t0 = time.perf_counter()
+    results = []
+    for _ in range(args.steps):
+        results.append(g.refine_device(d_init.data_ptr(), d_out.data_ptr()))
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - t0
+    barrier()
+    clk = clocks.stop()
+    dev_ms = sum(r.device_ms for r in results)
+    rounds = results[0].rounds
+    assert all(r.rounds == rounds and r.blocks == results[0].blocks and r.verified == 1 for r in results)
+    launches = sum(r.kernel_launches for r in results)
+    if dist is not None:
+        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_ms = float(t.item())
+    value = world * m * rounds * args.steps / (dev_ms / 1000.0)
+
+    # per-kernel times (CUDA events around every launch, same work)
+    times, pr = g.profile(d_init.data_ptr())
+    peak, peak_kind = measured_peaks()
+    ob = 8
+    sig_bytes = 8 * m + n * (ob + 8)               # heads + gathered colours per arc; offsets + signature per node
+    sig_ms = times["signature_ms"] / max(1, times["passes"])
+    achieved = sig_bytes / (sig_ms / 1e3) / 1e9
+    tpa = signature_traffic_per_arc()
+    round_bytes = 8 * m + n * (ob + 28)
+    pass_ms = (times["signature_ms"] + times["insert_ms"] + times["relabel_ms"] + times["other_ms"]) / max(1, times["passes"])
+    roofline = {"bound": "hbm", "kernel": "k_signature", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                "traffic": None if tpa is None else tpa * m,
+                "algorithmic_bytes_per_launch": sig_bytes, "launch_ms": sig_ms,
+                "round": {"algorithmic_bytes": round_bytes, "ms": pass_ms,
+                          "achieved_gbs": round_bytes / (pass_ms / 1e3) / 1e9,
+                          "frac": round_bytes / (pass_ms / 1e3) / 1e9 / peak},
+                "kernel_ms_per_pass": {k: v / max(1, times["passes"]) for k, v in times.items()
+                                       if k.endswith("_ms") and k != "total_ms"}}
+
+    # end to end through the C ABI with host buffers (pinned), copies inside the timed region
+    d_off, d_idx = g.device_csr()
+    off_h = torch.empty(n + 1, dtype=torch.int64, pin_memory=True)
+    idx_h = torch.empty(m, dtype=torch.int32, pin_memory=True)
+    init_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
+    out_h = torch.empty(n, dtype=torch.int32, pin_memory=True)
+
+    class _Arr:
+        def __init__(self, p, cnt, ts):
+            self.__cuda_array_interface__ = {"shape": (cnt,), "typestr": ts, "data": (p, False), "version": 3}
+
+    off_h.copy_(torch.as_tensor(_Arr(d_off, n + 1, "<i8"), device="cuda"))
+    idx_h.copy_(torch.as_tensor(_Arr(d_idx, m, "<i4"), device="cuda"))
+    init_h.copy_(d_init)
+    torch.cuda.synchronize()
+    off_np = off_h.numpy().view(np.uint64)
+    idx_np = idx_h.numpy().view(np.uint32)
+    init_np = init_h.numpy().view(np.uint32)
+    out_np = out_h.numpy().view(np.uint32)
+    e2e_res = []
+    ctx.refine(off_np, idx_np, init=init_np, out=out_np)  # warm-up
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_res.append(ctx.refine(off_np, idx_np, init=init_np, out=out_np))
+    e2e_wall = time.perf_counter() - t0
+    e2e_s = sum(r.time_s for r in e2e_res)
+    if dist is not None:
+        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    assert all(r.rounds == rounds and r.blocks == results[0].blocks for r in e2e_res)
+    assert np.array_equal(out_np, d_out.cpu().numpy().view(np.uint32))
+    e2e = {"value": world * m * rounds * args.e2e_steps / e2e_s, "unit": UNIT,
+           "h2d_bytes_per_step": int(e2e_res[0].h2d_bytes), "d2h_bytes_per_step": int(e2e_res[0].d2h_bytes),
+           "ms_per_step": 1000.0 * e2e_s / args.e2e_steps, "steps": args.e2e_steps,
+           "h2d_ms": e2e_res[-1].h2d_ms, "d2h_ms": e2e_res[-1].d2h_ms,
+           "path": "rbsc_refine (C ABI): pinned host CSR + colours in, labels out"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline_reference()
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+                "config": config(n, m, rounds), "time_to_fixpoint_ms": dev_ms / args.steps,
+                "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
+                "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel}
+        print(json.dumps(line))
+    g.free()
+    ctx.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=24)
+    ap.add_argument("--ef", type=int, default=16)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--relabel", choices=["hash", "sort"], default="hash")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local_rank = env_rank()
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -38,6 +38,7 @@
  * reports both.
  */
 #include <stdint.h>
+#include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -203,6 +204,39 @@ int orc_refine_exact(uint32_t n, const uint64_t* off, const uint32_t* idx, const
     free(cur); free(nxt); free(ord); free(tmp); free(sstart); free(slen);
     free(slab); free(swt); free(row);
     return status;
+}
+
+/* ------------------------------------------------------------------ */
+/* arcs-cuda text writer (feeds the reference programs)                */
+/* ------------------------------------------------------------------ */
+
+/* Writes "N\nM\n" + one "u wt v" line per arc (webgraph-rs
+ * cli/src/to/arcscuda.rs:61-66).  Returns 0 or -1. */
+int orc_write_arcs(const char* path, uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt)
+{
+    FILE* f = fopen(path, "w");
+    if (!f) return -1;
+    static char buf[1 << 20];
+    setvbuf(f, buf, _IOFBF, sizeof buf);
+    fprintf(f, "%u\n%llu\n", n, (unsigned long long)off[n]);
+    char line[80];
+    for (uint32_t u = 0; u < n; ++u) {
+        for (uint64_t k = off[u]; k < off[u + 1]; ++k) {
+            /* hand-rolled formatting: fprintf is the bottleneck at 1e8 arcs */
+            char* p = line + sizeof line;
+            *--p = '\n';
+            uint32_t v = idx[k];
+            do { *--p = (char)('0' + v % 10); v /= 10; } while (v);
+            *--p = ' ';
+            uint64_t w = wt ? wt[k] : 1u;
+            do { *--p = (char)('0' + w % 10); w /= 10; } while (w);
+            *--p = ' ';
+            uint32_t s = u;
+            do { *--p = (char)('0' + s % 10); s /= 10; } while (s);
+            fwrite(p, 1, (size_t)(line + sizeof line - p), f);
+        }
+    }
+    return fclose(f) == 0 ? 0 : -1;
 }
 
 /* ------------------------------------------------------------------ */

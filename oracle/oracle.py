@@ -63,6 +63,8 @@ def _load():
         lib.orc_canonicalize.restype = ctypes.c_uint32
         lib.orc_rsc_randomize.argtypes = [ctypes.c_uint64]
         lib.orc_rsc_randomize.restype = ctypes.c_uint64
+        lib.orc_write_arcs.argtypes = [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p, _u64p]
+        lib.orc_write_arcs.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -188,6 +190,31 @@ def mdp_text(off, idx, wt=None, init=None) -> bytes:
     if blocks:
         out.append("\n".join(blocks) + "\n")
     return "".join(out).encode()
+
+
+def write_arcs_file(path: str, off, idx, wt=None) -> None:
+    """arcs-cuda text of a CSR, written by C (fast enough for 1e8 arcs)."""
+    off, idx, wt = _csr(off, idx, wt)
+    n = len(off) - 1
+    if _load().orc_write_arcs(path.encode(), n, _p64(off), _p32(idx), _p64(wt)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def run_ref_rsc_file(path: str, timeout: float = 3600.0):
+    """Runs the reference rsc on an arcs-cuda file; returns (internal refinement
+    time in s, blocks, rounds in rsc's own convention, wall time in s)."""
+    import time
+    t0 = time.perf_counter()
+    with open(path, "rb") as f:
+        txt = subprocess.run([REF_RSC], stdin=f, capture_output=True, timeout=timeout, check=True).stdout.decode()
+    wall = time.perf_counter() - t0
+    lines = txt.split("\n")
+    rounds = None
+    for ln in lines[3:]:
+        if ln.startswith("rounds "):
+            rounds = int(ln.split()[1])
+            break
+    return float(lines[0]), int(lines[2]), rounds, wall
 
 
 def _parse_ref_output(txt: str):

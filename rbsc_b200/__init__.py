@@ -134,11 +134,15 @@ class Context:
             setattr(self._opts, k, v)
         _check(self._lib, self._lib.rbsc_ctx_set_opts(self._h, ctypes.byref(self._opts)), self._h)
 
-    def refine(self, off, idx, wt=None, init=None, labels: bool = True) -> Result:
-        """One-shot refinement of a host CSR (rbsc_refine)."""
+    def refine(self, off, idx, wt=None, init=None, labels: bool = True, out=None) -> Result:
+        """One-shot refinement of a host CSR (rbsc_refine).  `out`: optional
+        preallocated uint32 array (e.g. in pinned memory) for the labels."""
         c, keep = _csr(off, idx, wt)
         init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
-        out = np.zeros(max(c.n, 1), dtype=np.uint32) if labels else None
+        if out is not None:
+            assert out.dtype == np.uint32 and out.flags.c_contiguous and out.size >= c.n
+        elif labels:
+            out = np.zeros(max(c.n, 1), dtype=np.uint32)
         st = _lib.Stats()
         _check(self._lib, self._lib.rbsc_refine(self._h, ctypes.byref(c),
                                                 None if init_a is None else init_a.ctypes.data,
