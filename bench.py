@@ -149,8 +149,8 @@ def cpu_baseline_reference(steps: int = 1):
             "host_cores": os.cpu_count()}
 
 
-def config(n=None, m=None, rounds=None):
-    return {"workload": "rmat24_ef16", "model": "none (graph refinement)", "scale": 24, "edge_factor": 16,
+def config(n=None, m=None, rounds=None, scale=24, ef=16):
+    return {"workload": f"rmat{scale}_ef{ef}", "model": "none (graph refinement)", "scale": scale, "edge_factor": ef,
             "rmat_abc": [0.57, 0.19, 0.19], "nodes": n, "arcs": m, "rounds": rounds,
             "initial_colors": "floor(log2(out_degree+1))", "offsets": "int64", "indices": "int32",
             "l2": "no flush: inputs larger than L2 (heads 4 B/arc)", "parallelism": "replicas",
@@ -306,7 +306,7 @@ def run_ours(args, rank, world, local_rank):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": config(n, m, rounds), "time_to_fixpoint_ms": dev_ms / args.steps,
+                "config": config(n, m, rounds, args.scale, args.ef), "time_to_fixpoint_ms": dev_ms / args.steps,
                 "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel}

@@ -36,6 +36,7 @@ struct rbsc_graph {
     uint32_t* d_tile_row = nullptr;
     uint32_t nsplit = 0;
     uint32_t* d_split = nullptr;
+    uint8_t* d_head8 = nullptr;  // row-head bitmap, one bit per arc
 
     // refinement state (allocated on first refine, reused)
     bool bufs = false;

@@ -212,6 +212,7 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
     dev_free(g->d_roff);
     dev_free((void*&)g->d_tile_row);
     dev_free((void*&)g->d_split);
+    dev_free((void*&)g->d_head8);
     delete g;
 }
 
@@ -288,6 +289,20 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
         k_tile_rows<uint64_t><<<grid_for((uint64_t)g->ntiles + 1, 256), 256, 0, s>>>(g->ntiles, K, (const uint64_t*)g->d_roff, g->d_tile_row);
     }
     CK(cudaGetLastError());
+    // row-head bitmap (one bit per arc, padded to whole tiles)
+    {
+        const size_t hbytes = ((size_t)g->ntiles * kTileEdges) / 8 + 16;
+        CKS(dev_alloc(ctx, (void**)&g->d_head8, hbytes));
+        CK(cudaMemsetAsync(g->d_head8, 0, hbytes, s));
+        if (K > 0) {
+            ++rbsc::launch_counter();
+            if (g->off32)
+                k_head_bits<uint32_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint32_t*)g->d_roff, (uint32_t*)g->d_head8);
+            else
+                k_head_bits<uint64_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint64_t*)g->d_roff, (uint32_t*)g->d_head8);
+            CK(cudaGetLastError());
+        }
+    }
     // rows split across tiles
     if (K > 0) {
         CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)K + 1) + 1024));
@@ -477,25 +492,11 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (t) CK(cudaEventRecord(t->ev[1], s));
     if (g->m > 0) {
         const unsigned tiles = g->ntiles;
-        if (g->off32) {
-            if (g->weighted) {
-                ++rbsc::launch_counter();
-                k_signature<uint32_t, true><<<tiles, kTileThreads, 0, s>>>((const uint32_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
-            }
-            else {
-                ++rbsc::launch_counter();
-                k_signature<uint32_t, false><<<tiles, kTileThreads, 0, s>>>((const uint32_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
-            }
-        } else {
-            if (g->weighted) {
-                ++rbsc::launch_counter();
-                k_signature<uint64_t, true><<<tiles, kTileThreads, 0, s>>>((const uint64_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
-            }
-            else {
-                ++rbsc::launch_counter();
-                k_signature<uint64_t, false><<<tiles, kTileThreads, 0, s>>>((const uint64_t*)g->d_roff, g->d_rows, g->d_tile_row, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
-            }
-        }
+        ++rbsc::launch_counter();
+        if (g->weighted)
+            k_signature<true><<<tiles, kTileThreads, 0, s>>>(g->d_rows, g->d_tile_row, g->d_head8, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+        else
+            k_signature<false><<<tiles, kTileThreads, 0, s>>>(g->d_rows, g->d_tile_row, g->d_head8, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
     }
     if (t) CK(cudaEventRecord(t->ev[2], s));
     if (ctx->opts.relabel == RBSC_RELABEL_SORT) {

@@ -111,135 +111,244 @@ __device__ __forceinline__ uint32_t table_insert(Entry* tab, uint32_t log2size, 
 }
 
 // ---------------------------------------------------------------------------
-// k_signature: edge-balanced tiles.  Tile t holds arcs [t*2048, (t+1)*2048);
-// thread i of the tile CTA owns 8 consecutive arcs, loads their heads with two
-// 16-byte loads, gathers the 8 head colours, hashes them and folds them into
-// per-row partial sums.  A row wholly inside one thread's 8 arcs is written
-// directly; a row shared by threads goes through a shared-memory accumulator;
-// a row that crosses a tile edge is added to global memory atomically (its
-// signature was zeroed by the previous pass).  Sums are modulo 2^64 / 2^32, so
-// the split into partial sums does not change the result.
+// Per-arc term of the signature: an injective function of the head colour c
+// (the multiply by an odd constant, the xor-shift and the second multiply are
+// all bijections of uint64), salted per pass.  t1 feeds the 64-bit sum, t2 a
+// second, independent-looking 32-bit sum.
 // ---------------------------------------------------------------------------
-template <typename OffT, bool WEIGHTED>
-static __global__ void __launch_bounds__(kTileThreads) k_signature(const OffT* __restrict__ roff, const uint32_t* __restrict__ rows,
-                                                            const uint32_t* __restrict__ tile_row,
-                                                            const uint32_t* __restrict__ idx,
-                                                            const uint64_t* __restrict__ wt, uint64_t m,
-                                                            const RoundState* __restrict__ st,
-                                                            const uint32_t* __restrict__ col0, const uint32_t* __restrict__ col1,
-                                                            unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
+__device__ __forceinline__ void arc_terms(uint32_t c, uint64_t salt, uint64_t& t1, uint32_t& t2)
 {
-    __shared__ uint32_t s_off[kTileEdges + 1];
-    __shared__ unsigned long long s_acc1[kTileEdges];
-    __shared__ uint32_t s_acc2[kTileEdges];
+    uint64_t y = (uint64_t)(c ^ (uint32_t)salt) * 0x9e3779b97f4a7c15ull;
+    y ^= y >> 32;
+    y *= 0xd6e8feb86659fd93ull;
+    y ^= y >> 32;
+    t1 = y + (salt >> 32);
+    t2 = (uint32_t)(y >> 32) * 0x2545f491u + (uint32_t)y * ((uint32_t)y | 1u);
+}
 
-    const uint32_t r = st->round;
+// Block-wide scans over the 256 threads of a tile CTA.
+struct TileScanSmem {
+    uint32_t heads[kTileThreads / 32];
+    uint32_t flag[kTileThreads / 32];
+    unsigned long long v1[kTileThreads / 32];
+    uint32_t v2[kTileThreads / 32];
+    unsigned long long c1[kTileThreads];
+    uint32_t c2[kTileThreads];
+};
+
+// exclusive prefix over the block of n (per thread)
+__device__ __forceinline__ uint32_t tile_excl_scan(TileScanSmem& sm, uint32_t n)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t h = n;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, h, d);
+        if (lane >= d) h += o;
+    }
+    if (lane == 31) sm.heads[warp] = h;
+    __syncthreads();
+    uint32_t base = 0;
+    for (int w = 0; w < warp; ++w) base += sm.heads[w];
+    return base + h - n;
+}
+
+// inclusive segmented prefix of (v1, v2) over the block, a segment starting at
+// every thread whose flag is set; also returns the previous thread's result
+// (cin), i.e. what arrives at this thread's first arc
+__device__ __forceinline__ void tile_seg_scan(TileScanSmem& sm, bool flag, uint64_t v1, uint32_t v2, uint64_t& c1,
+                                              uint32_t& c2, uint64_t& cin1, uint32_t& cin2)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t f = flag ? 1u : 0u;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t fo = __shfl_up_sync(0xffffffffu, f, d);
+        const uint64_t vo1 = __shfl_up_sync(0xffffffffu, v1, d);
+        const uint32_t vo2 = __shfl_up_sync(0xffffffffu, v2, d);
+        if (lane >= d) {
+            if (!f) {
+                v1 += vo1;
+                v2 += vo2;
+            }
+            f |= fo;
+        }
+    }
+    if (lane == 31) {
+        sm.flag[warp] = f;
+        sm.v1[warp] = v1;
+        sm.v2[warp] = v2;
+    }
+    __syncthreads();
+    if (!f) {
+        uint64_t cc1 = 0;
+        uint32_t cc2 = 0;
+        for (int w = 0; w < warp; ++w) {
+            if (sm.flag[w]) {
+                cc1 = sm.v1[w];
+                cc2 = sm.v2[w];
+            } else {
+                cc1 += sm.v1[w];
+                cc2 += sm.v2[w];
+            }
+        }
+        v1 += cc1;
+        v2 += cc2;
+    }
+    c1 = v1;
+    c2 = v2;
+    sm.c1[threadIdx.x] = c1;
+    sm.c2[threadIdx.x] = c2;
+    __syncthreads();
+    cin1 = threadIdx.x ? sm.c1[threadIdx.x - 1] : 0ull;
+    cin2 = threadIdx.x ? sm.c2[threadIdx.x - 1] : 0u;
+}
+
+// ---------------------------------------------------------------------------
+// k_signature: edge-balanced tiles.  Tile t holds arcs [t*2048, (t+1)*2048);
+// thread i of the tile CTA owns the 8 consecutive arcs [8i, 8i+8): two 16-byte
+// loads of heads, one byte of the row-head bitmap (bit j set = arc 8i+j starts
+// a row), 8 gathered head colours.  An exclusive scan of the head counts gives
+// every thread the index of its first row.  Each thread then folds its arcs:
+//   - rows that start and end inside its 8 arcs are written directly,
+//   - the part before its first head belongs to the row continuing from the
+//     previous thread, the part after its last head to the row continuing into
+//     the next thread;
+// a block-wide segmented scan joins the parts of rows that span threads, and
+// the thread in which such a row ends writes it.  A row that crosses a tile
+// edge is added to global memory atomically (its signature was zeroed by the
+// previous pass).  Sums are modulo 2^64 / 2^32, so the split into partial sums
+// does not change the result.  No shared-memory atomics.
+// ---------------------------------------------------------------------------
+template <bool WEIGHTED>
+static __global__ void __launch_bounds__(kTileThreads) k_signature(const uint32_t* __restrict__ rows,
+                                                                   const uint32_t* __restrict__ tile_row,
+                                                                   const uint8_t* __restrict__ head8,
+                                                                   const uint32_t* __restrict__ idx,
+                                                                   const uint64_t* __restrict__ wt, uint64_t m,
+                                                                   const RoundState* __restrict__ st,
+                                                                   const uint32_t* __restrict__ col0,
+                                                                   const uint32_t* __restrict__ col1,
+                                                                   unsigned long long* __restrict__ sig1,
+                                                                   uint32_t* __restrict__ sig2)
+{
+    __shared__ TileScanSmem sm;
     const uint32_t* __restrict__ col = st->parity ? col1 : col0;
-    const uint64_t salt1 = pass_salt1(st->seed, r);
-    const uint32_t salt2 = pass_salt2(st->seed, r);
+    const uint64_t salt = pass_salt1(st->seed, st->round);
 
     const uint64_t tbeg = (uint64_t)blockIdx.x * kTileEdges;
     const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
     const uint64_t tend = tbeg + tlen;
     const uint32_t k0 = tile_row[blockIdx.x];
-    const uint32_t kn = tile_row[blockIdx.x + 1];
-    const uint32_t klast = ((uint64_t)roff[kn] < tend) ? kn : kn - 1u;
-    const uint32_t nrows = klast - k0 + 1u;
-    const bool starts_before = (uint64_t)roff[k0] < tbeg;
-    const bool ends_after = (uint64_t)roff[klast + 1] > tend;
-
-    for (uint32_t j = threadIdx.x; j <= nrows; j += kTileThreads) {
-        uint64_t o = (uint64_t)roff[k0 + j];
-        o = o < tbeg ? tbeg : (o > tend ? tend : o);
-        s_off[j] = (uint32_t)(o - tbeg);
-        if (j < nrows) {
-            s_acc1[j] = 0ull;
-            s_acc2[j] = 0u;
-        }
-    }
-    __syncthreads();
-
+    const uint32_t h0 = head8[tbeg >> 3] & 1u;  // the tile's first arc starts a row
     const uint32_t a = threadIdx.x * kEdgesPerThread;
-    if (a < tlen) {
-        const uint32_t b = min(a + (uint32_t)kEdgesPerThread, tlen);
-        const uint32_t cnt = b - a;
-        uint32_t v[kEdgesPerThread];
-        if (cnt == kEdgesPerThread) {
-            const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
-            const uint4 q0 = __ldg(p), q1 = __ldg(p + 1);
-            v[0] = q0.x; v[1] = q0.y; v[2] = q0.z; v[3] = q0.w;
-            v[4] = q1.x; v[5] = q1.y; v[6] = q1.z; v[7] = q1.w;
-        } else {
-#pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) v[i] = (uint32_t)i < cnt ? __ldg(idx + tbeg + a + i) : 0u;
-        }
-        uint32_t c[kEdgesPerThread];
-#pragma unroll
-        for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? __ldg(col + v[i]) : 0u;
-        uint64_t w[kEdgesPerThread];
-        if (WEIGHTED) {
-#pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldg(wt + tbeg + a + i) : 0ull;
-        }
+    const uint32_t cnt = a < tlen ? min((uint32_t)kEdgesPerThread, tlen - a) : 0u;
 
-        // row containing arc a: largest j with s_off[j] <= a
-        uint32_t lo = 0, hi = nrows - 1u;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi + 1u) >> 1;
-            if (s_off[mid] <= a) lo = mid; else hi = mid - 1u;
-        }
-        uint32_t j = lo;
-        uint64_t acc1 = 0;
-        uint32_t acc2 = 0;
-        auto flush = [&](uint32_t jj) {
-            const bool sb = (jj == 0u) && starts_before;
-            const bool ea = (jj == nrows - 1u) && ends_after;
-            if (!sb && !ea && s_off[jj] >= a && s_off[jj + 1] <= b) {
-                const uint32_t node = rows[k0 + jj];
-                sig1[node] = acc1;
-                sig2[node] = acc2;
-            } else {
-                atomicAdd(&s_acc1[jj], (unsigned long long)acc1);
-                atomicAdd(&s_acc2[jj], acc2);
-            }
-        };
+    uint32_t hb = 0;
+    uint32_t v[kEdgesPerThread];
+    if (cnt == kEdgesPerThread) {
+        hb = head8[(tbeg + a) >> 3];
+        const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
+        const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1);
+        v[0] = q0.x; v[1] = q0.y; v[2] = q0.z; v[3] = q0.w;
+        v[4] = q1.x; v[5] = q1.y; v[6] = q1.z; v[7] = q1.w;
+    } else {
+        if (cnt) hb = head8[(tbeg + a) >> 3] & ((1u << cnt) - 1u);
 #pragma unroll
-        for (int i = 0; i < kEdgesPerThread; ++i) {
-            if ((uint32_t)i < cnt) {
-                const uint32_t e = a + i;
-                while (e >= s_off[j + 1]) {
-                    flush(j);
-                    acc1 = 0;
-                    acc2 = 0;
-                    ++j;
-                }
-                uint64_t t1 = fmix64((uint64_t)c[i] ^ salt1);
-                uint32_t t2 = fmix32(c[i] ^ salt2);
-                if (WEIGHTED) {
-                    t1 *= w[i];
-                    t2 *= (uint32_t)w[i];
-                }
-                acc1 += t1;
-                acc2 += t2;
-            }
-        }
-        flush(j);
+        for (int i = 0; i < kEdgesPerThread; ++i) v[i] = (uint32_t)i < cnt ? __ldcs(idx + tbeg + a + i) : 0u;
     }
-    __syncthreads();
+    uint32_t c[kEdgesPerThread];
+#pragma unroll
+    for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? __ldg(col + v[i]) : 0u;
+    uint64_t w[kEdgesPerThread];
+    if (WEIGHTED) {
+#pragma unroll
+        for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + tbeg + a + i) : 0ull;
+    }
 
-    for (uint32_t jj = threadIdx.x; jj < nrows; jj += kTileThreads) {
-        const bool sb = (jj == 0u) && starts_before;
-        const bool ea = (jj == nrows - 1u) && ends_after;
-        const uint32_t rs = s_off[jj], re = s_off[jj + 1];
-        if (!sb && !ea && rs / kEdgesPerThread == (re - 1u) / kEdgesPerThread) continue;  // written by its thread
-        const uint32_t node = rows[k0 + jj];
-        if (!sb && !ea) {
-            sig1[node] = s_acc1[jj];
-            sig2[node] = s_acc2[jj];
-        } else {
-            atomicAdd(&sig1[node], s_acc1[jj]);
-            atomicAdd(&sig2[node], s_acc2[jj]);
+    // row of arc a-1 (or of arc a when arc a does not start a row):
+    // k0 + (heads in tile arcs [0, a)) - h0
+    const uint32_t kbase = k0 + tile_excl_scan(sm, (uint32_t)__popc(hb)) - h0;
+
+    // fold: `pre` = arcs before this thread's first head, `cur` = the row
+    // opened by the latest head; a row closed inside the thread is written
+    uint64_t pre1 = 0, cur1 = 0;
+    uint32_t pre2 = 0, cur2 = 0;
+    uint32_t nh = 0;
+#pragma unroll
+    for (int i = 0; i < kEdgesPerThread; ++i) {
+        if ((uint32_t)i < cnt) {
+            if ((hb >> i) & 1u) {
+                if (nh > 0) {
+                    const uint32_t node = rows[kbase + nh];
+                    sig1[node] = cur1;
+                    sig2[node] = cur2;
+                }
+                ++nh;
+                cur1 = 0;
+                cur2 = 0;
+            }
+            uint64_t t1;
+            uint32_t t2;
+            arc_terms(c[i], salt, t1, t2);
+            if (WEIGHTED) {
+                t1 *= w[i];
+                t2 *= (uint32_t)w[i];
+            }
+            if (nh == 0) {
+                pre1 += t1;
+                pre2 += t2;
+            } else {
+                cur1 += t1;
+                cur2 += t2;
+            }
         }
+    }
+
+    uint64_t c1, cin1;
+    uint32_t c2, cin2;
+    const bool flag = nh > 0;
+    tile_seg_scan(sm, flag, flag ? cur1 : pre1, flag ? cur2 : pre2, c1, c2, cin1, cin2);
+    if (cnt == 0) return;
+
+    // the row continuing into this thread ends here when this thread has a head
+    if (nh > 0 && (a > 0 || !(hb & 1u))) {
+        const uint32_t node = rows[kbase];
+        const uint64_t tot1 = cin1 + pre1;
+        const uint32_t tot2 = cin2 + pre2;
+        if (kbase == k0 && !h0) {  // began in an earlier tile
+            atomicAdd(&sig1[node], (unsigned long long)tot1);
+            atomicAdd(&sig2[node], tot2);
+        } else {
+            sig1[node] = tot1;
+            sig2[node] = tot2;
+        }
+    }
+    // the last thread of the tile closes the tile's last row
+    if (a + cnt == tlen) {
+        const uint32_t klast = kbase + nh;
+        const bool ends = (tend == m) || (head8[tend >> 3] & 1u);
+        const bool began_before = (klast == k0 && !h0);
+        const uint32_t node = rows[klast];
+        if (ends && !began_before) {
+            sig1[node] = c1;
+            sig2[node] = c2;
+        } else {
+            atomicAdd(&sig1[node], (unsigned long long)c1);
+            atomicAdd(&sig2[node], c2);
+        }
+    }
+}
+
+// Row-head bitmap: bit (e % 8) of byte e / 8 is set iff arc e is the first
+// arc of its row.
+template <typename OffT>
+static __global__ void k_head_bits(uint32_t K, const OffT* __restrict__ roff, uint32_t* __restrict__ head32)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < K) {
+        const uint64_t e = (uint64_t)roff[k];
+        atomicOr(&head32[e >> 5], 1u << (e & 31));
     }
 }
 
