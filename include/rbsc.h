@@ -89,6 +89,8 @@ typedef struct {
     uint64_t d2h_bytes;
     uint32_t round_blocks[64];/* block count before pass 1 and after passes 1..63       */
     uint64_t kernel_launches; /* kernels of this library launched by the call            */
+    double init_ms;           /* device time: initial colours + active-set setup          */
+    double loop_ms;           /* device time: the signature passes (all rounds)          */
 } rbsc_stats;
 
 /* Per-kernel device time of one refinement, measured with CUDA events around

@@ -67,6 +67,8 @@ class Stats(ctypes.Structure):
         ("d2h_bytes", ctypes.c_uint64),
         ("round_blocks", ctypes.c_uint32 * 64),
         ("kernel_launches", ctypes.c_uint64),
+        ("init_ms", ctypes.c_double),
+        ("loop_ms", ctypes.c_double),
     ]
 
 

@@ -14,10 +14,11 @@ constexpr uint32_t kLabelMask = 0x7fffffffu;
 // seen from more than one node (block is not a singleton).
 constexpr uint32_t kJoined = 0x80000000u;
 
-// Edges per signature tile and threads per tile CTA.
+// Signature tiles: one warp per tile of 512 arcs, 16 consecutive arcs per lane;
+// CTAs of 8 warps.
 constexpr int kTileThreads = 256;
-constexpr int kEdgesPerThread = 8;
-constexpr uint32_t kTileEdges = kTileThreads * kEdgesPerThread;  // 2048
+constexpr int kEdgesPerThread = 16;
+constexpr uint32_t kTileEdges = 32 * kEdgesPerThread;  // 512
 
 constexpr int kNodeThreads = 256;
 

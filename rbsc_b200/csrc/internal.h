@@ -6,16 +6,13 @@
 
 #include "../../include/rbsc.h"
 
-namespace rbsc {
-struct RoundState;
-struct Entry;
-}
+#include "refine_kernels.cuh"
 
 struct rbsc_ctx {
     int device = 0;
     rbsc_opts opts{};
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[4] = {};
+    cudaEvent_t ev[6] = {};
     int sm_count = 148;
     std::string err;
 };
@@ -40,7 +37,7 @@ struct rbsc_graph {
 
     // refinement state (allocated on first refine, reused)
     bool bufs = false;
-    uint32_t* d_col[2] = {nullptr, nullptr};
+    uint32_t* d_col[1] = {nullptr};  // colours, updated in place
     uint32_t* d_initlab = nullptr;
     unsigned long long* d_sig1 = nullptr;
     uint32_t* d_sig2 = nullptr;
@@ -56,8 +53,20 @@ struct rbsc_graph {
     void* d_tmp = nullptr;
     size_t tmp_bytes = 0;
 
+    // active set (what the passes still work on)
+    rbsc::ActiveSet* d_as = nullptr;
+    uint2* d_pairs = nullptr;        // (follower, representative)
+    uint32_t* d_grep = nullptr;      // per initial label: smallest arc-less node
+    uint32_t* d_gcnt = nullptr;      // per initial label: arc-less nodes
+    rbsc::CompactBufs cb{};
+    bool compact_arcs = false;
+
     // exact check
     uint32_t* d_vflag = nullptr;
+    uint32_t* d_vrow = nullptr;
+    uint32_t* d_vl8 = nullptr;
+    uint32_t* d_vl32 = nullptr;
+    uint32_t* d_vllong = nullptr;
     uint64_t* d_vdeg = nullptr;
     uint32_t* d_fail = nullptr;
     unsigned long long* d_keys[2] = {nullptr, nullptr};

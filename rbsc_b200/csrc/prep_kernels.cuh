@@ -42,7 +42,7 @@ static __global__ void k_nonempty_flags(uint32_t n, const uint64_t* __restrict__
 }
 
 template <typename OffT>
-static __global__ void k_compact_rows(uint32_t n, uint64_t m, const uint64_t* __restrict__ off, const uint32_t* __restrict__ pos,
+static __global__ void k_prep_rows(uint32_t n, uint64_t m, const uint64_t* __restrict__ off, const uint32_t* __restrict__ pos,
                                uint32_t K, uint32_t* __restrict__ rows, OffT* __restrict__ roff)
 {
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;

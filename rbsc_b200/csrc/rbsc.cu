@@ -173,7 +173,21 @@ static void graph_release_refine(rbsc_graph* g)
     g->loop_exec = nullptr;
     g->loop_graph = nullptr;
     dev_free((void*&)g->d_col[0]);
-    dev_free((void*&)g->d_col[1]);
+    dev_free((void*&)g->d_as);
+    dev_free((void*&)g->d_pairs);
+    dev_free((void*&)g->d_grep);
+    dev_free((void*&)g->d_gcnt);
+    for (int d = 0; d < 2; ++d) {
+        dev_free((void*&)g->cb.rows[d]);
+        dev_free((void*&)g->cb.off[d]);
+        dev_free((void*&)g->cb.src[d]);
+        dev_free((void*&)g->cb.idx[d]);
+        dev_free((void*&)g->cb.wt[d]);
+        dev_free((void*&)g->cb.head8[d]);
+        dev_free((void*&)g->cb.tile_row[d]);
+        dev_free((void*&)g->cb.split[d]);
+        dev_free((void*&)g->cb.nodes[d]);
+    }
     dev_free((void*&)g->d_initlab);
     dev_free((void*&)g->d_sig1);
     dev_free((void*&)g->d_sig2);
@@ -183,6 +197,10 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free((void*&)g->d_out);
     dev_free((void*&)g->d_init);
     dev_free((void*&)g->d_vflag);
+    dev_free((void*&)g->d_vrow);
+    dev_free((void*&)g->d_vl8);
+    dev_free((void*&)g->d_vl32);
+    dev_free((void*&)g->d_vllong);
     dev_free((void*&)g->d_vdeg);
     dev_free((void*&)g->d_fail);
     dev_free((void*&)g->d_keys[0]);
@@ -270,11 +288,11 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, &g->d_roff, (g->off32 ? 4 : 8) * ((size_t)K + 1)));
     if (g->off32) {
         ++rbsc::launch_counter();
-        k_compact_rows<uint32_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint32_t*)g->d_roff);
+        k_prep_rows<uint32_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint32_t*)g->d_roff);
     }
     else {
         ++rbsc::launch_counter();
-        k_compact_rows<uint64_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint64_t*)g->d_roff);
+        k_prep_rows<uint64_t><<<grid_for(n, 256), 256, 0, s>>>(n, m, g->d_off, d_pos, K, g->d_rows, (uint64_t*)g->d_roff);
     }
     CK(cudaGetLastError());
     // tiles
@@ -456,7 +474,6 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     if (g->bufs) return RBSC_OK;
     const size_t n = std::max<uint32_t>(g->n, 1);
     CKS(dev_alloc(ctx, (void**)&g->d_col[0], 4 * n));
-    CKS(dev_alloc(ctx, (void**)&g->d_col[1], 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_initlab, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_sig1, 8 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_sig2, 4 * n));
@@ -467,12 +484,38 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
     CK(cudaMallocHost((void**)&g->h_st, sizeof(RoundState)));
+    // active set: node lists, followers, group representatives, compacted arc sets
+    CKS(dev_alloc(ctx, (void**)&g->d_as, sizeof(ActiveSet)));
+    CKS(dev_alloc(ctx, (void**)&g->d_pairs, 8 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_grep, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_gcnt, 4 * n));
+    g->compact_arcs = g->m > 0 && g->m < (1ull << 32);
+    const size_t K = std::max<uint32_t>(g->K, 1);
+    const size_t tiles = std::max<uint32_t>(g->ntiles, 1);
+    const size_t mpad = tiles * kTileEdges;
+    for (int d = 0; d < 2; ++d) {
+        CKS(dev_alloc(ctx, (void**)&g->cb.nodes[d], 4 * n));
+        if (!g->compact_arcs) continue;
+        CKS(dev_alloc(ctx, (void**)&g->cb.rows[d], 4 * K));
+        CKS(dev_alloc(ctx, (void**)&g->cb.off[d], 4 * (K + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->cb.src[d], 4 * K));
+        CKS(dev_alloc(ctx, (void**)&g->cb.idx[d], 4 * mpad));
+        if (g->weighted) CKS(dev_alloc(ctx, (void**)&g->cb.wt[d], 8 * mpad));
+        CKS(dev_alloc(ctx, (void**)&g->cb.head8[d], mpad / 8 + 16));
+        CKS(dev_alloc(ctx, (void**)&g->cb.tile_row[d], 4 * (tiles + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->cb.split[d], 4 * (tiles + 1)));
+    }
     CK(cudaMemsetAsync(g->d_sig1, 0, 8 * n, ctx->stream));
     CK(cudaMemsetAsync(g->d_sig2, 0, 4 * n, ctx->stream));
     CK(cudaMemsetAsync(g->d_tab, 0, sizeof(Entry) << g->log2tab, ctx->stream));
     g->next_stamp = 1;
     g->bufs = true;
     return RBSC_OK;
+}
+
+static unsigned persistent_grid(rbsc_ctx* ctx, uint64_t work, unsigned per_block)
+{
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(work, per_block), (uint64_t)ctx->sm_count * 16));
 }
 
 // CUDA events around the kernels of one pass (profiling only).
@@ -486,32 +529,51 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
 {
     const uint32_t n = g->n;
     const unsigned clear_grid = (unsigned)std::min<uint64_t>(ctx->sm_count * 8ull, grid_for(1ull << g->log2tab, 256));
+    const unsigned ngrid = persistent_grid(ctx, n, kNodeThreads);
+    const bool hash = ctx->opts.relabel != RBSC_RELABEL_SORT;
     if (t) CK(cudaEventRecord(t->ev[0], s));
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
     if (t) CK(cudaEventRecord(t->ev[1], s));
     if (g->m > 0) {
-        const unsigned tiles = g->ntiles;
+        const unsigned blocks = persistent_grid(ctx, g->ntiles, kTileThreads / 32);
         ++rbsc::launch_counter();
         if (g->weighted)
-            k_signature<true><<<tiles, kTileThreads, 0, s>>>(g->d_rows, g->d_tile_row, g->d_head8, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            k_signature<true><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
         else
-            k_signature<false><<<tiles, kTileThreads, 0, s>>>(g->d_rows, g->d_tile_row, g->d_head8, g->d_idx, g->d_wt, g->m, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2);
+            k_signature<false><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
     }
     if (t) CK(cudaEventRecord(t->ev[2], s));
-    if (ctx->opts.relabel == RBSC_RELABEL_SORT) {
+    if (!hash) {
         CKS(launch_sort_relabel(ctx, g, s));
         if (t) CK(cudaEventRecord(t->ev[3], s));
     } else {
         ++rbsc::launch_counter();
-        k_insert<kModeHash><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, nullptr, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2, g->d_tab, g->log2tab, g->d_slot);
         if (t) CK(cudaEventRecord(t->ev[3], s));
         ++rbsc::launch_counter();
-        k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
+        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_col[0], g->d_tab, g->d_slot, g->d_sig1, g->d_sig2);
     }
+    ++rbsc::launch_counter();
+    k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_pairs, g->d_col[0]);
     if (t) CK(cudaEventRecord(t->ev[4], s));
     ++rbsc::launch_counter();
-    k_fixpoint<kModeHash><<<1, 1, 0, s>>>(g->d_st, h, use_handle);
+    k_fixpoint<kFixHash><<<1, 1, 0, s>>>(g->d_st, g->d_as, hash ? 1 : 0, h, use_handle);
+    // compaction for the next pass
+    ++rbsc::launch_counter();
+    k_compact_nodes<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb);
+    if (g->compact_arcs) {
+        const unsigned kgrid = persistent_grid(ctx, g->K, kNodeThreads);
+        const unsigned agrid = persistent_grid(ctx, ceil_div<uint64_t>(g->m, 16), kNodeThreads);
+        ++rbsc::launch_counter();
+        k_compact_rows<<<kgrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb);
+        ++rbsc::launch_counter();
+        k_compact_decide<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb);
+        ++rbsc::launch_counter();
+        k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig1, g->d_sig2);
+    }
+    ++rbsc::launch_counter();
+    k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb);
     if (t) CK(cudaEventRecord(t->ev[5], s));
     CK(cudaGetLastError());
     return RBSC_OK;
@@ -600,75 +662,149 @@ static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt,
     return RBSC_OK;
 }
 
-// Exact check of the current fixpoint.  Returns the number of failing nodes in
-// *nfail (0 = the partition is the coarsest stable one).
-static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t parity, uint32_t* nfail)
+// Resets the active set to the whole graph and builds the node list and the
+// follower pairs from the current colouring (after the initial or a repair
+// pass).
+static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
 {
     cudaStream_t s = ctx->stream;
     const uint32_t n = g->n;
-    const uint32_t* col = g->d_col[parity];
-    if (!g->d_vflag) {
-        CKS(dev_alloc(ctx, (void**)&g->d_vflag, 4 * ((size_t)n + 1)));
-        CKS(dev_alloc(ctx, (void**)&g->d_vdeg, 8 * ((size_t)n + 1)));
-        CKS(dev_alloc(ctx, (void**)&g->d_fail, 4 * ((size_t)n + 1)));
-    }
-    CKS(ensure_temp(ctx, g, scan_temp_bytes<uint64_t>((uint64_t)n + 1) + 1024));
-    uint64_t* d_tot = (uint64_t*)g->d_small;  // [0] rows (u32 in a u64 slot), [1] keys, [2] nfail
-    CK(cudaMemsetAsync(d_tot, 0, 64, s));
-    ++rbsc::launch_counter();
-    k_verify_mark<<<grid_for(n, 256), 256, 0, s>>>(n, col, g->d_off, g->d_vflag, g->d_vdeg);
-    CK(cudaGetLastError());
-    CK((exclusive_scan<uint32_t, uint32_t>(g->d_vflag, g->d_vflag, n, (uint32_t*)d_tot, g->d_tmp, s)));
-    CK((exclusive_scan<uint64_t, uint64_t>(g->d_vdeg, g->d_vdeg, n, d_tot + 1, g->d_tmp, s)));
-    uint64_t tot[2];
-    CK(cudaMemcpyAsync(tot, d_tot, sizeof tot, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    const uint32_t nrows = (uint32_t)tot[0];
-    const uint64_t nkeys = tot[1];
-    if (nkeys >= (1ull << 32)) return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "exact check: %llu arcs in non-singleton rows (limit 2^32)", (unsigned long long)nkeys);
-    if (nkeys > g->key_cap) {
-        dev_free((void*&)g->d_keys[0]);
-        dev_free((void*&)g->d_keys[1]);
-        dev_free((void*&)g->d_vals[0]);
-        dev_free((void*&)g->d_vals[1]);
-        g->key_cap = 0;
-        CKS(dev_alloc(ctx, (void**)&g->d_keys[0], 8 * nkeys));
-        CKS(dev_alloc(ctx, (void**)&g->d_keys[1], 8 * nkeys));
-        if (g->weighted) {
-            CKS(dev_alloc(ctx, (void**)&g->d_vals[0], 8 * nkeys));
-            CKS(dev_alloc(ctx, (void**)&g->d_vals[1], 8 * nkeys));
-        }
-        g->key_cap = nkeys;
-    }
-    const unsigned long long* keys = g->d_keys[0];
-    const unsigned long long* vals = g->weighted ? g->d_vals[0] : nullptr;
-    if (nkeys > 0) {
+    ActiveSet a;
+    std::memset(&a, 0, sizeof a);
+    a.rows = g->d_rows;
+    a.roff = g->d_roff;
+    a.roff64 = g->off32 ? 0u : 1u;
+    a.tile_row = g->d_tile_row;
+    a.head8 = g->d_head8;
+    a.idx = g->d_idx;
+    a.wt = g->d_wt;
+    a.split = g->d_split;
+    a.m = g->m;
+    a.K = g->K;
+    a.ntiles = g->ntiles;
+    a.nsplit = g->nsplit;
+    a.nodes = g->cb.nodes[0];
+    a.compact_arcs = g->compact_arcs ? 1u : 0u;
+    CK(cudaMemcpyAsync(g->d_as, &a, sizeof a, cudaMemcpyHostToDevice, s));
+    if (g->nsplit) {
         ++rbsc::launch_counter();
-        k_verify_keys<<<grid_for(n, 128), 128, 0, s>>>(n, col, g->d_off, g->d_idx, g->d_wt, g->d_vflag, g->d_vdeg, g->d_keys[0], g->weighted ? g->d_vals[0] : nullptr);
-        CK(cudaGetLastError());
-        CKS(ensure_temp(ctx, g, radix_temp_bytes(nkeys)));
-        const int bits = 31 + (int)log2_ceil(std::max<uint32_t>(nrows, 1));
-        bool in_alt = false;
-        CK(radix_sort<unsigned long long>(g->d_keys[0], g->d_keys[1], g->weighted ? g->d_vals[0] : (unsigned long long*)nullptr,
-                                          g->weighted ? g->d_vals[1] : (unsigned long long*)nullptr, nkeys, 0, bits, g->d_tmp, s, &in_alt));
-        if (in_alt) {
-            keys = g->d_keys[1];
-            vals = g->weighted ? g->d_vals[1] : nullptr;
-        }
+        k_zero_rows<<<grid_for(g->nsplit, 256), 256, 0, s>>>(g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
     }
-    CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
-    const unsigned cgrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 16, grid_for((uint64_t)n * 32, 256));
+    CK(cudaMemsetAsync(g->d_grep, 0xff, 4 * (size_t)n, s));
+    CK(cudaMemsetAsync(g->d_gcnt, 0, 4 * (size_t)n, s));
     ++rbsc::launch_counter();
-    k_verify_compare<<<cgrid, 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->d_vdeg, keys, vals, g->d_fail, (uint32_t*)(d_tot + 2));
+    k_group_reps<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_grep, g->d_gcnt);
+    ++rbsc::launch_counter();
+    k_build_lists<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_col[0], g->d_grep, g->d_gcnt, g->d_as,
+                                                   g->cb.nodes[0], g->d_pairs);
     CK(cudaGetLastError());
-    uint32_t hf = 0;
-    CK(cudaMemcpyAsync(&hf, d_tot + 2, sizeof hf, cudaMemcpyDeviceToHost, s));
+    // node list written into buffer 0: publish it, the next compaction writes buffer 1
+    uint32_t cnt = 0;
+    CK(cudaMemcpyAsync(&cnt, reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nodectr), 4, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    *nfail = hf;
+    const uint32_t zero = 0, one = 1;
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nnodes), &cnt, 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nodectr), &zero, 4, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, dst_nodes), &one, 4, cudaMemcpyHostToDevice, s));
+    CK(cudaStreamSynchronize(s));
     return RBSC_OK;
 }
 
-// Splits the nodes that failed the exact check away from their blocks.
+// Exact check of the current fixpoint.  Returns the number of failing nodes in
+// *nfail (0 = the partition is the coarsest stable one).
+static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail)
+{
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = g->n;
+    const uint32_t* col = g->d_col[0];
+    if (!g->d_vflag) {
+        CKS(dev_alloc(ctx, (void**)&g->d_vflag, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vrow, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vdeg, 8 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_fail, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vl8, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vl32, 4 * ((size_t)n + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->d_vllong, 4 * ((size_t)n + 1)));
+    }
+    uint32_t* counts = reinterpret_cast<uint32_t*>(g->d_small);          // [0..3] list sizes, failures
+    uint64_t* tot = reinterpret_cast<uint64_t*>(g->d_small) + 4;          // [0] rows, [1] keys of the global path
+    CK(cudaMemsetAsync(g->d_small, 0, 64, s));
+    CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), s));
+    CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
+    VerifyLists vl{g->d_vl8, g->d_vl32, g->d_vllong, counts};
+    ++rbsc::launch_counter();
+    k_verify_classify<<<grid_for(n, 256), 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->weighted ? 1 : 0, vl, g->d_vflag,
+                                                      g->d_fail);
+    const unsigned sgrid = persistent_grid(ctx, n, 256);
+    ++rbsc::launch_counter();
+    k_verify_short<8><<<sgrid, 256, 0, s>>>(n, g->d_vl8, counts + 0, col, g->d_off, g->d_idx, g->d_fail, counts + 3);
+    ++rbsc::launch_counter();
+    k_verify_short<32><<<sgrid, 256, 0, s>>>(n, g->d_vl32, counts + 1, col, g->d_off, g->d_idx, g->d_fail, counts + 3);
+    CK(cudaGetLastError());
+    uint32_t hc[4];
+    CK(cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    if (hc[2] > 0) {
+        // global path for long / weighted rows: sort each flagged row's colours
+        CKS(ensure_temp(ctx, g, scan_temp_bytes<uint64_t>((uint64_t)n + 1) + 1024));
+        ++rbsc::launch_counter();
+        k_verify_mark<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, g->d_vflag, g->d_vdeg);
+        CK(cudaGetLastError());
+        CK((exclusive_scan<uint32_t, uint32_t>(g->d_vflag, g->d_vrow, n, (uint32_t*)tot, g->d_tmp, s)));
+        CK((exclusive_scan<uint64_t, uint64_t>(g->d_vdeg, g->d_vdeg, n, tot + 1, g->d_tmp, s)));
+        uint64_t ht[2];
+        CK(cudaMemcpyAsync(ht, tot, sizeof ht, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        const uint32_t nrows = (uint32_t)ht[0];
+        const uint64_t nkeys = ht[1];
+        if (nkeys >= (1ull << 32))
+            return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "exact check: %llu arcs in long rows (limit 2^32)", (unsigned long long)nkeys);
+        if (nkeys > g->key_cap) {
+            dev_free((void*&)g->d_keys[0]);
+            dev_free((void*&)g->d_keys[1]);
+            dev_free((void*&)g->d_vals[0]);
+            dev_free((void*&)g->d_vals[1]);
+            g->key_cap = 0;
+            CKS(dev_alloc(ctx, (void**)&g->d_keys[0], 8 * nkeys));
+            CKS(dev_alloc(ctx, (void**)&g->d_keys[1], 8 * nkeys));
+            if (g->weighted) {
+                CKS(dev_alloc(ctx, (void**)&g->d_vals[0], 8 * nkeys));
+                CKS(dev_alloc(ctx, (void**)&g->d_vals[1], 8 * nkeys));
+            }
+            g->key_cap = nkeys;
+        }
+        const unsigned long long* keys = g->d_keys[0];
+        const unsigned long long* vals = g->weighted ? g->d_vals[0] : nullptr;
+        if (nkeys > 0) {
+            ++rbsc::launch_counter();
+            k_verify_keys<<<grid_for(n, 128), 128, 0, s>>>(n, col, g->d_off, g->d_idx, g->d_wt, g->d_vflag, g->d_vrow, g->d_vdeg,
+                                                          g->d_keys[0], g->weighted ? g->d_vals[0] : nullptr);
+            CK(cudaGetLastError());
+            CKS(ensure_temp(ctx, g, radix_temp_bytes(nkeys)));
+            const int bits = 31 + (int)log2_ceil(std::max<uint32_t>(nrows, 1));
+            bool in_alt = false;
+            CK(radix_sort<unsigned long long>(g->d_keys[0], g->d_keys[1], g->weighted ? g->d_vals[0] : (unsigned long long*)nullptr,
+                                              g->weighted ? g->d_vals[1] : (unsigned long long*)nullptr, nkeys, 0, bits, g->d_tmp, s,
+                                              &in_alt));
+            if (in_alt) {
+                keys = g->d_keys[1];
+                vals = g->weighted ? g->d_vals[1] : nullptr;
+            }
+        }
+        const unsigned cgrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 16, grid_for((uint64_t)hc[2] * 32, 256));
+        ++rbsc::launch_counter();
+        k_verify_compare<<<cgrid, 256, 0, s>>>(g->d_vllong, counts + 2, col, g->d_initlab, g->d_off, g->d_vdeg, keys, vals,
+                                               g->d_fail, counts + 3);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    *nfail = hc[3];
+    return RBSC_OK;
+}
+
+// Splits the nodes that failed the exact check away from their blocks, then
+// restarts the active set from the whole graph.
 static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
 {
     cudaStream_t s = ctx->stream;
@@ -677,13 +813,16 @@ static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
     ++rbsc::launch_counter();
-    k_insert<kModeRepair><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, g->d_fail, g->d_tab, g->log2tab, g->d_slot);
+    k_insert_all<kModeRepair><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_fail, g->d_tab, g->log2tab, g->d_slot);
     ++rbsc::launch_counter();
-    k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, 0, g->d_sig1, g->d_sig2);
+    k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
     ++rbsc::launch_counter();
-    k_fixpoint<kModeRepair><<<1, 1, 0, s>>>(g->d_st, cudaGraphConditionalHandle(), 0);
+    k_fixpoint<kFixRepair><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0, cudaGraphConditionalHandle(), 0);
     CK(cudaGetLastError());
-    return RBSC_OK;
+    // every row signature is recomputed from scratch on the whole graph
+    CK(cudaMemsetAsync(g->d_sig1, 0, 8 * (size_t)n, s));
+    CK(cudaMemsetAsync(g->d_sig2, 0, 4 * (size_t)n, s));
+    return init_active_set(ctx, g);
 }
 
 // The whole refinement of a resident graph, device pointers in and out.
@@ -709,21 +848,17 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     hs.stamp = g->next_stamp;
     hs.clear_pending = 0;
     CK(cudaEventRecord(ctx->ev[0], s));
-    uint32_t parity = 0;
     if (d_init) {
-        hs.parity = 0;
         CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
         CK(cudaMemsetAsync(g->d_col[0], 0, 4 * (size_t)n, s));
         ++rbsc::launch_counter();
-        k_insert<kModeInit><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_sig1, g->d_sig2, d_init, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_all<kModeInit><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], d_init, g->d_tab, g->log2tab, g->d_slot);
         ++rbsc::launch_counter();
-        k_relabel<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], g->d_tab, g->d_slot, g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
+        k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
         ++rbsc::launch_counter();
-        k_fixpoint<kModeInit><<<1, 1, 0, s>>>(g->d_st, cudaGraphConditionalHandle(), 0);
+        k_fixpoint<kFixInit><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0, cudaGraphConditionalHandle(), 0);
         CK(cudaGetLastError());
-        parity = 1;
     } else {
-        hs.parity = 0;
         hs.prev = 1;
         hs.round_blocks[0] = 1;
         CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
@@ -732,21 +867,34 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         CK(cudaGetLastError());
     }
     ++rbsc::launch_counter();
-    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[parity], g->d_initlab);
+    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_initlab);
     CK(cudaGetLastError());
     CKS(read_state(ctx, g));
     const uint32_t initial_blocks = hs.prev;
+    CKS(init_active_set(ctx, g));
+    CK(cudaEventRecord(ctx->ev[4], s));
+    CK(cudaEventSynchronize(ctx->ev[4]));
+    float init_ms = 0.f;
+    cudaEventElapsedTime(&init_ms, ctx->ev[0], ctx->ev[4]);
 
-    float verify_ms = 0.f;
+    float verify_ms = 0.f, loop_ms = 0.f;
     uint32_t repairs = 0;
     for (;;) {
         if (hs.error) break;
+        CK(cudaEventRecord(ctx->ev[4], s));
         CKS(run_loop(ctx, g, kt, &graph_kernels));
+        CK(cudaEventRecord(ctx->ev[5], s));
+        CK(cudaEventSynchronize(ctx->ev[5]));
+        {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+            loop_ms += ms;
+        }
         if (hs.error) break;
         if (!ctx->opts.verify) break;
         CK(cudaEventRecord(ctx->ev[2], s));
         uint32_t nfail = 0;
-        CKS(verify_fixpoint(ctx, g, hs.parity, &nfail));
+        CKS(verify_fixpoint(ctx, g, &nfail));
         CK(cudaEventRecord(ctx->ev[3], s));
         CK(cudaEventSynchronize(ctx->ev[3]));
         float ms = 0.f;
@@ -762,7 +910,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     if (hs.error & kErrRounds) return rbsc_fail(ctx, RBSC_ERR_NOT_CONVERGED, "no fixpoint after %u passes", hs.round);
     uint32_t* out = d_out ? d_out : g->d_out;
     ++rbsc::launch_counter();
-    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[hs.parity], out);
+    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], out);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[1], s));
     CK(cudaEventSynchronize(ctx->ev[1]));
@@ -779,6 +927,8 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         stats->verify_ms = verify_ms;
         for (int i = 0; i < 64 && i < kRoundLog; ++i) stats->round_blocks[i] = hs.round_blocks[i];
         stats->kernel_launches = rbsc::launch_counter() - lc0 + graph_kernels;
+        stats->init_ms = init_ms;
+        stats->loop_ms = loop_ms;
     }
     if (kt) kt->total_ms = total_ms;
     return RBSC_OK;

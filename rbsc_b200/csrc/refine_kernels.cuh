@@ -1,12 +1,25 @@
 // refine_kernels.cuh -- the per-round kernels of the colour-refinement loop.
 //
 // One pass (reference: the body of the round loop, src/rbsc/rbsc.cu:354-425):
-//   k_signature  sig(u) = sum over u's arcs of wt * H(colour(v))      (rbsc.cu:80-87 + ReduceByKey 366-382)
-//   k_insert     (colour(u), sig(u)) -> relabel-table slot             (replaces the sorts + scan of 384-396)
-//   k_relabel    new colour = smallest member of the slot's class      (replaces reorder 396)
-//   k_fixpoint   block count unchanged -> done                          (replaces the D2H + host test of 398-402, 425)
+//   k_signature    sig(u) = sum over u's arcs of wt * H(colour(v))    (rbsc.cu:80-87 + ReduceByKey 366-382)
+//   k_insert_list  (colour(u), sig(u)) -> relabel-table slot           (replaces the sorts + scan of 384-396)
+//   k_relabel_list new colour = smallest member of the slot's class    (replaces reorder 396)
+//   k_follow       arc-less nodes take their representative's colour
+//   k_fixpoint     block count unchanged -> done                        (replaces the D2H + host test of 398-402, 425)
+//   k_compact_*    drop what can no longer change (see below)
 // The reference's injectivity loop (rbsc.cu:404-419) has no counterpart: the
-// per-arc hash here is a bijection of the colour by construction.
+// per-arc term here is a bijection of the colour by construction.
+//
+// Work that cannot change the partition is dropped as the refinement goes:
+//   - a singleton block never splits again, so its node leaves the relabel
+//     list and its row leaves the signature pass (the arc set is compacted on
+//     the device whenever it shrank by a quarter);
+//   - nodes without arcs that share an initial colour have the same
+//     signature (0) in every pass, so they stay together for good: one
+//     representative per such group goes through the relabel, the others
+//     copy its colour.
+// The colour array is updated in place: every pass reads the colours of the
+// previous pass in k_signature / k_insert before k_relabel overwrites them.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -20,7 +33,7 @@ constexpr int kRoundLog = 64;
 // k_fixpoint (one thread) advances it.
 struct RoundState {
     uint32_t round;          // completed signature passes
-    uint32_t parity;         // colour buffer holding the current colouring
+    uint32_t parity;         // unused (colours are updated in place)
     uint32_t count;          // blocks counted by the running pass
     uint32_t prev;           // blocks after the last completed pass
     uint32_t done;           // fixpoint reached
@@ -36,10 +49,58 @@ struct RoundState {
 constexpr uint32_t kErrProbe = 1u;   // relabel table full (cannot happen at load <= 1/2)
 constexpr uint32_t kErrRounds = 2u;  // max_rounds reached
 
-// Pass modes of k_insert / k_fixpoint.
-constexpr int kModeHash = 0;    // key = (label, signature)
-constexpr int kModeInit = 1;    // key = initial colour (exact)
-constexpr int kModeRepair = 2;  // key = (label, failed-exact-check flag) (exact)
+// What the pass kernels work on; the compaction kernels shrink it.
+struct ActiveSet {
+    // arc set of k_signature: non-empty rows, their arcs, the tiling
+    const uint32_t* rows;      // node of each row (K)
+    const void* roff;          // first arc of each row (K+1; uint64 when roff64, else uint32)
+    const uint32_t* tile_row;  // row holding the first arc of each tile (ntiles+1)
+    const uint8_t* head8;      // row-head bitmap
+    const uint32_t* idx;       // arc heads
+    const uint64_t* wt;        // arc weights or null
+    const uint32_t* split;     // rows crossing a tile edge
+    uint64_t m;
+    uint32_t K;
+    uint32_t ntiles;
+    uint32_t nsplit;
+    uint32_t roff64;
+    // node list of the hash relabel: entries node | kRepFlag
+    const uint32_t* nodes;
+    uint32_t nnodes;
+    uint32_t retired;          // singleton blocks dropped from the node list
+    // compaction bookkeeping
+    unsigned long long rowctr; // (rows << 32) | arcs reserved in the destination arc set
+    uint32_t nodectr;          // entries written to the destination node list
+    uint32_t splitctr;         // rows appended to the destination split list
+    uint32_t do_copy;          // the arc set is rebuilt in this pass
+    uint32_t new_K;
+    uint32_t new_m;
+    uint32_t dst_arcs;         // which compacted arc buffer the next rebuild writes
+    uint32_t dst_nodes;        // which node-list buffer the next compaction writes
+    uint32_t compact_arcs;     // arc-set compaction allowed (M < 2^32)
+    uint32_t nfollow;          // follower list length
+};
+
+// Node-list flag: the node represents a group of arc-less nodes with the same
+// initial colour, so its block is never a singleton.
+constexpr uint32_t kRepFlag = 0x80000000u;
+
+// Static pointers of the ping-pong compaction buffers.
+struct CompactBufs {
+    uint32_t* rows[2];
+    uint32_t* off[2];      // uint32 offsets (K+1)
+    uint32_t* src[2];      // where each row's arcs start in the source arc set
+    uint32_t* idx[2];
+    uint64_t* wt[2];
+    uint8_t* head8[2];
+    uint32_t* tile_row[2];
+    uint32_t* split[2];
+    uint32_t* nodes[2];
+};
+
+// Pass modes of the exact (non-hashed) relabels over all nodes.
+constexpr int kModeInit = 1;    // key = initial colour
+constexpr int kModeRepair = 2;  // key = (label, failed-exact-check flag)
 
 // ---------------------------------------------------------------------------
 // relabel table: 16-byte entries {k1 (64), k2 (32: 24 hash bits | 8-bit stamp),
@@ -72,8 +133,8 @@ __device__ __forceinline__ void cas_entry(Entry* p, uint64_t clo, uint64_t chi, 
 }
 
 // Finds or claims the slot of key (k1, k2) for node u.  `multi`: u stands for
-// several nodes with this key (warp-aggregated), so the class is not a
-// singleton.  Returns the slot; *claimed = this call created the class.
+// several nodes with this key, so the class is not a singleton.  Returns the
+// slot; *claimed = this call created the class.
 __device__ __forceinline__ uint32_t table_insert(Entry* tab, uint32_t log2size, uint64_t k1, uint32_t k2, uint32_t stamp,
                                                  uint32_t u, bool multi, bool* claimed, uint32_t* err)
 {
@@ -111,14 +172,14 @@ __device__ __forceinline__ uint32_t table_insert(Entry* tab, uint32_t log2size, 
 }
 
 // ---------------------------------------------------------------------------
-// Per-arc term of the signature: an injective function of the head colour c
+// Per-arc term of the signature: an injective function of the head's label
 // (the multiply by an odd constant, the xor-shift and the second multiply are
 // all bijections of uint64), salted per pass.  t1 feeds the 64-bit sum, t2 a
 // second, independent-looking 32-bit sum.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void arc_terms(uint32_t c, uint64_t salt, uint64_t& t1, uint32_t& t2)
 {
-    uint64_t y = (uint64_t)(c ^ (uint32_t)salt) * 0x9e3779b97f4a7c15ull;
+    uint64_t y = (uint64_t)((c & kLabelMask) ^ (uint32_t)salt) * 0x9e3779b97f4a7c15ull;
     y ^= y >> 32;
     y *= 0xd6e8feb86659fd93ull;
     y ^= y >> 32;
@@ -126,216 +187,169 @@ __device__ __forceinline__ void arc_terms(uint32_t c, uint64_t salt, uint64_t& t
     t2 = (uint32_t)(y >> 32) * 0x2545f491u + (uint32_t)y * ((uint32_t)y | 1u);
 }
 
-// Block-wide scans over the 256 threads of a tile CTA.
-struct TileScanSmem {
-    uint32_t heads[kTileThreads / 32];
-    uint32_t flag[kTileThreads / 32];
-    unsigned long long v1[kTileThreads / 32];
-    uint32_t v2[kTileThreads / 32];
-    unsigned long long c1[kTileThreads];
-    uint32_t c2[kTileThreads];
-};
-
-// exclusive prefix over the block of n (per thread)
-__device__ __forceinline__ uint32_t tile_excl_scan(TileScanSmem& sm, uint32_t n)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t h = n;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t o = __shfl_up_sync(0xffffffffu, h, d);
-        if (lane >= d) h += o;
-    }
-    if (lane == 31) sm.heads[warp] = h;
-    __syncthreads();
-    uint32_t base = 0;
-    for (int w = 0; w < warp; ++w) base += sm.heads[w];
-    return base + h - n;
-}
-
-// inclusive segmented prefix of (v1, v2) over the block, a segment starting at
-// every thread whose flag is set; also returns the previous thread's result
-// (cin), i.e. what arrives at this thread's first arc
-__device__ __forceinline__ void tile_seg_scan(TileScanSmem& sm, bool flag, uint64_t v1, uint32_t v2, uint64_t& c1,
-                                              uint32_t& c2, uint64_t& cin1, uint32_t& cin2)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t f = flag ? 1u : 0u;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t fo = __shfl_up_sync(0xffffffffu, f, d);
-        const uint64_t vo1 = __shfl_up_sync(0xffffffffu, v1, d);
-        const uint32_t vo2 = __shfl_up_sync(0xffffffffu, v2, d);
-        if (lane >= d) {
-            if (!f) {
-                v1 += vo1;
-                v2 += vo2;
-            }
-            f |= fo;
-        }
-    }
-    if (lane == 31) {
-        sm.flag[warp] = f;
-        sm.v1[warp] = v1;
-        sm.v2[warp] = v2;
-    }
-    __syncthreads();
-    if (!f) {
-        uint64_t cc1 = 0;
-        uint32_t cc2 = 0;
-        for (int w = 0; w < warp; ++w) {
-            if (sm.flag[w]) {
-                cc1 = sm.v1[w];
-                cc2 = sm.v2[w];
-            } else {
-                cc1 += sm.v1[w];
-                cc2 += sm.v2[w];
-            }
-        }
-        v1 += cc1;
-        v2 += cc2;
-    }
-    c1 = v1;
-    c2 = v2;
-    sm.c1[threadIdx.x] = c1;
-    sm.c2[threadIdx.x] = c2;
-    __syncthreads();
-    cin1 = threadIdx.x ? sm.c1[threadIdx.x - 1] : 0ull;
-    cin2 = threadIdx.x ? sm.c2[threadIdx.x - 1] : 0u;
-}
-
 // ---------------------------------------------------------------------------
-// k_signature: edge-balanced tiles.  Tile t holds arcs [t*2048, (t+1)*2048);
-// thread i of the tile CTA owns the 8 consecutive arcs [8i, 8i+8): two 16-byte
-// loads of heads, one byte of the row-head bitmap (bit j set = arc 8i+j starts
-// a row), 8 gathered head colours.  An exclusive scan of the head counts gives
-// every thread the index of its first row.  Each thread then folds its arcs:
-//   - rows that start and end inside its 8 arcs are written directly,
+// k_signature: edge-balanced tiles of 512 arcs, one tile at a time per warp
+// (persistent warps).  Lane l owns the 16 consecutive arcs [16l, 16l+16) of
+// the tile: four 16-byte loads of heads, two bytes of the row-head bitmap (bit
+// j set = arc 16l+j starts a row), 16 gathered head colours.  A warp exclusive
+// scan of the head counts gives every lane the index of its first row.  Each
+// lane folds its arcs:
+//   - rows that start and end inside its 16 arcs are written directly,
 //   - the part before its first head belongs to the row continuing from the
-//     previous thread, the part after its last head to the row continuing into
-//     the next thread;
-// a block-wide segmented scan joins the parts of rows that span threads, and
-// the thread in which such a row ends writes it.  A row that crosses a tile
-// edge is added to global memory atomically (its signature was zeroed by the
-// previous pass).  Sums are modulo 2^64 / 2^32, so the split into partial sums
-// does not change the result.  No shared-memory atomics.
+//     previous lane, the part after its last head to the row continuing into
+//     the next lane;
+// a warp segmented scan joins the parts of rows that span lanes, and the lane
+// in which such a row ends writes it.  A row that crosses a tile edge is added
+// to global memory atomically (its signature was zeroed beforehand).  Sums
+// are modulo 2^64 / 2^32, so the split into partial sums does not change the
+// result.  Warps are independent: no shared memory, no block barrier.
 // ---------------------------------------------------------------------------
 template <bool WEIGHTED>
-static __global__ void __launch_bounds__(kTileThreads) k_signature(const uint32_t* __restrict__ rows,
-                                                                   const uint32_t* __restrict__ tile_row,
-                                                                   const uint8_t* __restrict__ head8,
-                                                                   const uint32_t* __restrict__ idx,
-                                                                   const uint64_t* __restrict__ wt, uint64_t m,
+static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveSet* __restrict__ as,
                                                                    const RoundState* __restrict__ st,
-                                                                   const uint32_t* __restrict__ col0,
-                                                                   const uint32_t* __restrict__ col1,
+                                                                   const uint32_t* __restrict__ col,
                                                                    unsigned long long* __restrict__ sig1,
                                                                    uint32_t* __restrict__ sig2)
 {
-    __shared__ TileScanSmem sm;
-    const uint32_t* __restrict__ col = st->parity ? col1 : col0;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t ntiles = as->ntiles;
+    const uint64_t m = as->m;
+    const uint32_t* __restrict__ rows = as->rows;
+    const uint32_t* __restrict__ tile_row = as->tile_row;
+    const uint8_t* __restrict__ head8 = as->head8;
+    const uint32_t* __restrict__ idx = as->idx;
+    const uint64_t* __restrict__ wt = as->wt;
     const uint64_t salt = pass_salt1(st->seed, st->round);
+    const uint32_t warps = gridDim.x * (kTileThreads / 32);
 
-    const uint64_t tbeg = (uint64_t)blockIdx.x * kTileEdges;
-    const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
-    const uint64_t tend = tbeg + tlen;
-    const uint32_t k0 = tile_row[blockIdx.x];
-    const uint32_t h0 = head8[tbeg >> 3] & 1u;  // the tile's first arc starts a row
-    const uint32_t a = threadIdx.x * kEdgesPerThread;
-    const uint32_t cnt = a < tlen ? min((uint32_t)kEdgesPerThread, tlen - a) : 0u;
+    for (uint32_t tile = blockIdx.x * (kTileThreads / 32) + (threadIdx.x >> 5); tile < ntiles; tile += warps) {
+        const uint64_t tbeg = (uint64_t)tile * kTileEdges;
+        const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
+        const uint64_t tend = tbeg + tlen;
+        const uint32_t k0 = tile_row[tile];
+        const uint32_t h0 = head8[tbeg >> 3] & 1u;  // the tile's first arc starts a row
+        const uint32_t a = lane * kEdgesPerThread;
+        const uint32_t cnt = a < tlen ? min((uint32_t)kEdgesPerThread, tlen - a) : 0u;
 
-    uint32_t hb = 0;
-    uint32_t v[kEdgesPerThread];
-    if (cnt == kEdgesPerThread) {
-        hb = head8[(tbeg + a) >> 3];
-        const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
-        const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1);
-        v[0] = q0.x; v[1] = q0.y; v[2] = q0.z; v[3] = q0.w;
-        v[4] = q1.x; v[5] = q1.y; v[6] = q1.z; v[7] = q1.w;
-    } else {
-        if (cnt) hb = head8[(tbeg + a) >> 3] & ((1u << cnt) - 1u);
+        uint32_t hb = 0;
+        uint32_t c[kEdgesPerThread];
+        uint64_t w[kEdgesPerThread];
+        if (cnt == kEdgesPerThread) {
+            hb = *reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3));
+            const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
+            const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1), q2 = __ldcs(p + 2), q3 = __ldcs(p + 3);
+            c[0] = __ldg(col + q0.x); c[1] = __ldg(col + q0.y); c[2] = __ldg(col + q0.z); c[3] = __ldg(col + q0.w);
+            c[4] = __ldg(col + q1.x); c[5] = __ldg(col + q1.y); c[6] = __ldg(col + q1.z); c[7] = __ldg(col + q1.w);
+            c[8] = __ldg(col + q2.x); c[9] = __ldg(col + q2.y); c[10] = __ldg(col + q2.z); c[11] = __ldg(col + q2.w);
+            c[12] = __ldg(col + q3.x); c[13] = __ldg(col + q3.y); c[14] = __ldg(col + q3.z); c[15] = __ldg(col + q3.w);
+        } else {
+            if (cnt) hb = (uint32_t)(*reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3))) & ((1u << cnt) - 1u);
 #pragma unroll
-        for (int i = 0; i < kEdgesPerThread; ++i) v[i] = (uint32_t)i < cnt ? __ldcs(idx + tbeg + a + i) : 0u;
-    }
-    uint32_t c[kEdgesPerThread];
+            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? __ldg(col + __ldcs(idx + tbeg + a + i)) : 0u;
+        }
+        if (WEIGHTED) {
 #pragma unroll
-    for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? __ldg(col + v[i]) : 0u;
-    uint64_t w[kEdgesPerThread];
-    if (WEIGHTED) {
-#pragma unroll
-        for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + tbeg + a + i) : 0ull;
-    }
+            for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + tbeg + a + i) : 0ull;
+        }
 
-    // row of arc a-1 (or of arc a when arc a does not start a row):
-    // k0 + (heads in tile arcs [0, a)) - h0
-    const uint32_t kbase = k0 + tile_excl_scan(sm, (uint32_t)__popc(hb)) - h0;
-
-    // fold: `pre` = arcs before this thread's first head, `cur` = the row
-    // opened by the latest head; a row closed inside the thread is written
-    uint64_t pre1 = 0, cur1 = 0;
-    uint32_t pre2 = 0, cur2 = 0;
-    uint32_t nh = 0;
+        // row of arc a-1 (or of arc a when arc a does not start a row):
+        // k0 + (heads in tile arcs [0, a)) - h0
+        const uint32_t nheads = (uint32_t)__popc(hb);
+        uint32_t hs = nheads;
 #pragma unroll
-    for (int i = 0; i < kEdgesPerThread; ++i) {
-        if ((uint32_t)i < cnt) {
-            if ((hb >> i) & 1u) {
-                if (nh > 0) {
-                    const uint32_t node = rows[kbase + nh];
-                    sig1[node] = cur1;
-                    sig2[node] = cur2;
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xffffffffu, hs, d);
+            if (lane >= (uint32_t)d) hs += o;
+        }
+        const uint32_t kbase = k0 + hs - nheads - h0;
+
+        // fold: `pre` = arcs before this lane's first head, `cur` = the row
+        // opened by the latest head; a row closed inside the lane is written
+        uint64_t pre1 = 0, cur1 = 0;
+        uint32_t pre2 = 0, cur2 = 0;
+        uint32_t nh = 0;
+#pragma unroll
+        for (int i = 0; i < kEdgesPerThread; ++i) {
+            if ((uint32_t)i < cnt) {
+                if ((hb >> i) & 1u) {
+                    if (nh > 0) {
+                        const uint32_t node = rows[kbase + nh];
+                        sig1[node] = cur1;
+                        sig2[node] = cur2;
+                    }
+                    ++nh;
+                    cur1 = 0;
+                    cur2 = 0;
                 }
-                ++nh;
-                cur1 = 0;
-                cur2 = 0;
+                uint64_t t1;
+                uint32_t t2;
+                arc_terms(c[i], salt, t1, t2);
+                if (WEIGHTED) {
+                    t1 *= w[i];
+                    t2 *= (uint32_t)w[i];
+                }
+                if (nh == 0) {
+                    pre1 += t1;
+                    pre2 += t2;
+                } else {
+                    cur1 += t1;
+                    cur2 += t2;
+                }
             }
-            uint64_t t1;
-            uint32_t t2;
-            arc_terms(c[i], salt, t1, t2);
-            if (WEIGHTED) {
-                t1 *= w[i];
-                t2 *= (uint32_t)w[i];
+        }
+
+        // warp inclusive segmented scan of the lanes' trailing parts (a
+        // segment starts at every lane with a head)
+        uint32_t f = nh > 0 ? 1u : 0u;
+        uint64_t c1 = f ? cur1 : pre1;
+        uint32_t c2 = f ? cur2 : pre2;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t fo = __shfl_up_sync(0xffffffffu, f, d);
+            const uint64_t vo1 = __shfl_up_sync(0xffffffffu, c1, d);
+            const uint32_t vo2 = __shfl_up_sync(0xffffffffu, c2, d);
+            if (lane >= (uint32_t)d) {
+                if (!f) {
+                    c1 += vo1;
+                    c2 += vo2;
+                }
+                f |= fo;
             }
-            if (nh == 0) {
-                pre1 += t1;
-                pre2 += t2;
+        }
+        uint64_t cin1 = __shfl_up_sync(0xffffffffu, c1, 1);
+        uint32_t cin2 = __shfl_up_sync(0xffffffffu, c2, 1);
+        if (lane == 0) {
+            cin1 = 0;
+            cin2 = 0;
+        }
+        if (cnt == 0) continue;
+
+        // the row continuing into this lane ends here when this lane has a head
+        if (nh > 0 && (a > 0 || !(hb & 1u))) {
+            const uint32_t node = rows[kbase];
+            const uint64_t tot1 = cin1 + pre1;
+            const uint32_t tot2 = cin2 + pre2;
+            if (kbase == k0 && !h0) {  // began in an earlier tile
+                atomicAdd(&sig1[node], (unsigned long long)tot1);
+                atomicAdd(&sig2[node], tot2);
             } else {
-                cur1 += t1;
-                cur2 += t2;
+                sig1[node] = tot1;
+                sig2[node] = tot2;
             }
         }
-    }
-
-    uint64_t c1, cin1;
-    uint32_t c2, cin2;
-    const bool flag = nh > 0;
-    tile_seg_scan(sm, flag, flag ? cur1 : pre1, flag ? cur2 : pre2, c1, c2, cin1, cin2);
-    if (cnt == 0) return;
-
-    // the row continuing into this thread ends here when this thread has a head
-    if (nh > 0 && (a > 0 || !(hb & 1u))) {
-        const uint32_t node = rows[kbase];
-        const uint64_t tot1 = cin1 + pre1;
-        const uint32_t tot2 = cin2 + pre2;
-        if (kbase == k0 && !h0) {  // began in an earlier tile
-            atomicAdd(&sig1[node], (unsigned long long)tot1);
-            atomicAdd(&sig2[node], tot2);
-        } else {
-            sig1[node] = tot1;
-            sig2[node] = tot2;
-        }
-    }
-    // the last thread of the tile closes the tile's last row
-    if (a + cnt == tlen) {
-        const uint32_t klast = kbase + nh;
-        const bool ends = (tend == m) || (head8[tend >> 3] & 1u);
-        const bool began_before = (klast == k0 && !h0);
-        const uint32_t node = rows[klast];
-        if (ends && !began_before) {
-            sig1[node] = c1;
-            sig2[node] = c2;
-        } else {
-            atomicAdd(&sig1[node], (unsigned long long)c1);
-            atomicAdd(&sig2[node], c2);
+        // the last lane of the tile closes the tile's last row
+        if (a + cnt == tlen) {
+            const uint32_t klast = kbase + nh;
+            const bool ends = (tend == m) || (head8[tend >> 3] & 1u);
+            const bool began_before = (klast == k0 && !h0);
+            const uint32_t node = rows[klast];
+            if (ends && !began_before) {
+                sig1[node] = c1;
+                sig2[node] = c2;
+            } else {
+                atomicAdd(&sig1[node], (unsigned long long)c1);
+                atomicAdd(&sig2[node], c2);
+            }
         }
     }
 }
@@ -353,117 +367,457 @@ static __global__ void k_head_bits(uint32_t K, const OffT* __restrict__ roff, ui
 }
 
 // ---------------------------------------------------------------------------
-// k_insert: one thread per node.  Singleton nodes keep their colour.  The
-// others build their key, group with equal keys of their warp
-// (__match_any_sync), and the group's smallest node probes the table once for
-// the group.  Counts the blocks of the new partition.
+// Relabel through the table.  Each node of a warp builds its key, groups with
+// equal keys of the warp (__match_any_sync), and one lane probes the table
+// once for the group, offering the group's smallest node as the class label.
+// Counts the classes it creates.
 // ---------------------------------------------------------------------------
-template <int MODE>
-static __global__ void __launch_bounds__(kNodeThreads) k_insert(uint32_t n, RoundState* __restrict__ st,
-                                                         const uint32_t* __restrict__ col0, const uint32_t* __restrict__ col1,
-                                                         const unsigned long long* __restrict__ sig1,
-                                                         const uint32_t* __restrict__ sig2,
-                                                         const uint32_t* __restrict__ aux, Entry* __restrict__ tab,
-                                                         uint32_t log2size, uint32_t* __restrict__ slot)
+__device__ __forceinline__ void insert_warp(bool need, uint32_t u, bool rep, uint64_t k1, uint32_t k2, uint32_t stamp,
+                                            Entry* tab, uint32_t log2size, uint32_t* slot, uint32_t* err,
+                                            bool& new_block)
 {
-    const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
     const int lane = threadIdx.x & 31;
-    const bool active = u < n;
-    const uint32_t* __restrict__ col = st->parity ? col1 : col0;
-    const uint32_t stamp = st->stamp;
-    const uint32_t c = active ? col[u] : kSingleton;
-    const bool need = active && (MODE == kModeInit || !(c & kSingleton));
-
-    uint64_t k1 = 0;
-    uint32_t k2 = stamp;
-    if (need) {
-        const uint32_t lab = c & kLabelMask;
-        if (MODE == kModeHash) {
-            uint64_t s1 = sig1[u];
-            uint32_t s2 = sig2[u];
-            const uint32_t hb = st->hash_bits;
-            if (hb) {
-                s1 &= (hb >= 64) ? ~0ull : ((1ull << hb) - 1ull);
-                s2 = 0;
-            }
-            const uint64_t seed = st->seed;
-            k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
-            k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
-        } else if (MODE == kModeInit) {
-            k1 = aux[u];
-        } else {
-            k1 = (uint64_t)lab | ((uint64_t)(aux[u] != 0u) << 32);
-        }
-    }
     const unsigned need_mask = __ballot_sync(0xffffffffu, need);
-    bool new_block = active && !need;
+    const unsigned rep_mask = __ballot_sync(0xffffffffu, need && rep);
     if (need) {
         const unsigned peers = __match_any_sync(need_mask, k1) & __match_any_sync(need_mask, k2);
         const int leader = __ffs(peers) - 1;
+        // the list is not in node order: the group's label candidate is its minimum
+        const uint32_t umin = __reduce_min_sync(peers, u);
         uint32_t s = 0;
         bool claimed = false;
-        if (lane == leader) s = table_insert(tab, log2size, k1, k2, stamp, u, __popc(peers) > 1, &claimed, &st->error);
+        if (lane == leader)
+            s = table_insert(tab, log2size, k1, k2, stamp, umin, __popc(peers) > 1 || (rep_mask & peers), &claimed, err);
         s = __shfl_sync(peers, s, leader);
         slot[u] = s;
         new_block = (lane == leader) && claimed;
     }
-    const unsigned nb = __ballot_sync(0xffffffffu, new_block);
-    if (lane == 0 && nb) atomicAdd(&st->count, (uint32_t)__popc(nb));
 }
 
-// k_relabel: new colour of every node; also zeroes the signatures of the rows
-// that cross a tile edge (the next pass adds into them atomically).
-static __global__ void __launch_bounds__(kNodeThreads) k_relabel(uint32_t n, const RoundState* __restrict__ st, uint32_t* __restrict__ col0,
-                                                          uint32_t* __restrict__ col1, const Entry* __restrict__ tab,
-                                                          const uint32_t* __restrict__ slot,
-                                                          const uint32_t* __restrict__ split_rows, uint32_t nsplit,
-                                                          unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
+__device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
+{
+    const unsigned nb = __ballot_sync(0xffffffffu, new_block);
+    if ((threadIdx.x & 31) == 0 && nb) atomicAdd(counter, (uint32_t)__popc(nb));
+}
+
+// Hashed pass over the node list (persistent, grid-stride by warps).
+static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
+                                                                     const uint32_t* __restrict__ col,
+                                                                     const unsigned long long* __restrict__ sig1,
+                                                                     const uint32_t* __restrict__ sig2,
+                                                                     Entry* __restrict__ tab, uint32_t log2size,
+                                                                     uint32_t* __restrict__ slot)
+{
+    const uint32_t nn = as->nnodes;
+    const uint32_t* __restrict__ nodes = as->nodes;
+    const uint32_t stamp = st->stamp;
+    const uint32_t hb = st->hash_bits;
+    const uint64_t seed = st->seed;
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    uint32_t made = 0;
+    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
+        const uint32_t i = base + (threadIdx.x & 31);
+        const bool active = i < nn;
+        const uint32_t e = active ? nodes[i] : 0u;
+        const uint32_t u = e & ~kRepFlag;
+        const uint32_t c = active ? col[u] : kSingleton;
+        const bool need = active && !(c & kSingleton);
+        uint64_t k1 = 0;
+        uint32_t k2 = stamp;
+        if (need) {
+            const uint32_t lab = c & kLabelMask;
+            uint64_t s1 = sig1[u];
+            uint32_t s2 = sig2[u];
+            if (hb) {
+                s1 &= (hb >= 64) ? ~0ull : ((1ull << hb) - 1ull);
+                s2 = 0;
+            }
+            k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
+            k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
+        }
+        bool nb = active && !need;
+        insert_warp(need, u, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2size, slot, &st->error, nb);
+        made += nb ? 1u : 0u;
+    }
+    // one atomic per warp
+    made = __reduce_add_sync(0xffffffffu, made);
+    if ((threadIdx.x & 31) == 0 && made) atomicAdd(&st->count, made);
+}
+
+// Exact pass over all nodes: initial colours (MODE kModeInit, aux = colours)
+// or the repair of a failed exact check (kModeRepair, aux = failure flags).
+template <int MODE>
+static __global__ void __launch_bounds__(kNodeThreads) k_insert_all(uint32_t n, RoundState* __restrict__ st,
+                                                                    const uint32_t* __restrict__ col,
+                                                                    const uint32_t* __restrict__ aux, Entry* __restrict__ tab,
+                                                                    uint32_t log2size, uint32_t* __restrict__ slot)
 {
     const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
-    const uint32_t* __restrict__ cur = st->parity ? col1 : col0;
-    uint32_t* __restrict__ nxt = st->parity ? col0 : col1;
-    if (u < n) {
-        const uint32_t c = cur[u];
-        uint32_t out = c;
-        if (!(c & kSingleton)) {
-            const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(tab + slot[u]) + 3);
-            out = (v & kLabelMask) | ((v & kJoined) ? 0u : kSingleton);
-        }
-        nxt[u] = out;
+    const bool active = u < n;
+    const uint32_t stamp = st->stamp;
+    const uint32_t c = active ? col[u] : kSingleton;
+    const bool need = active && (MODE == kModeInit || !(c & kSingleton));
+    uint64_t k1 = 0;
+    if (need) k1 = (MODE == kModeInit) ? (uint64_t)aux[u] : ((uint64_t)(c & kLabelMask) | ((uint64_t)(aux[u] != 0u) << 32));
+    bool nb = active && !need;
+    insert_warp(need, u, false, k1, stamp, stamp, tab, log2size, slot, &st->error, nb);
+    count_blocks(nb, &st->count);
+}
+
+__device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, const uint32_t* slot, uint32_t u)
+{
+    if (c & kSingleton) return c;
+    const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(tab + slot[u]) + 3);
+    return (v & kLabelMask) | ((v & kJoined) ? 0u : kSingleton);
+}
+
+// New colours of the node list, in place; also zeroes the signatures of the
+// rows that cross a tile edge (the next pass adds into them atomically).
+static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
+                                                                      const Entry* __restrict__ tab,
+                                                                      const uint32_t* __restrict__ slot,
+                                                                      unsigned long long* __restrict__ sig1,
+                                                                      uint32_t* __restrict__ sig2)
+{
+    const uint32_t nn = as->nnodes;
+    const uint32_t* __restrict__ nodes = as->nodes;
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < nn; i += stride) {
+        const uint32_t u = nodes[i] & ~kRepFlag;
+        col[u] = relabel_one(col[u], tab, slot, u);
     }
-    for (uint32_t i = u; i < nsplit; i += gridDim.x * kNodeThreads) {
-        const uint32_t node = split_rows[i];
+    const uint32_t ns = as->nsplit;
+    const uint32_t* __restrict__ split = as->split;
+    for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < ns; i += stride) {
+        const uint32_t node = split[i];
         sig1[node] = 0ull;
         sig2[node] = 0u;
     }
 }
 
+// New colours of all nodes (after k_insert_all), in place.
+static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n, uint32_t* __restrict__ col,
+                                                                     const Entry* __restrict__ tab,
+                                                                     const uint32_t* __restrict__ slot)
+{
+    const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
+    if (u < n) col[u] = relabel_one(col[u], tab, slot, u);
+}
+
+// Followers (arc-less nodes that are not their group's representative) take
+// the representative's colour.  pairs[i] = (follower, representative).
+static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
+                                                                uint32_t* __restrict__ col)
+{
+    const uint32_t nf = as->nfollow;
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < nf; i += stride) {
+        const uint2 p = pairs[i];
+        col[p.x] = col[p.y];
+    }
+}
+
 // k_fixpoint: one thread.  Closes the running pass and decides whether the
 // device-side while loop runs another one.
+//   hashed pass: blocks = classes found in the node list + retired singletons
+//   (add_retired) or the count written by the sort-based relabel
+//   init / repair pass: blocks = classes found over all nodes
+constexpr int kFixHash = 0;
+constexpr int kFixInit = 1;
+constexpr int kFixRepair = 2;
 template <int MODE>
-static __global__ void k_fixpoint(RoundState* st, cudaGraphConditionalHandle handle, int use_handle)
+static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_retired, cudaGraphConditionalHandle handle,
+                                  int use_handle)
 {
-    const uint32_t cnt = st->count;
+    uint32_t cnt = st->count;
     st->count = 0;
-    if (MODE == kModeHash) {
+    if (MODE == kFixHash) {
+        if (add_retired) cnt += as->retired;
         const uint32_t r = st->round + 1u;
         st->round = r;
         if (r < kRoundLog) st->round_blocks[r] = cnt;
         if (cnt == st->prev) st->done = 1u;
-    } else if (MODE == kModeInit) {
+    } else if (MODE == kFixInit) {
         st->round_blocks[0] = cnt;
         st->done = 0u;
     } else {
         st->done = 0u;
     }
     st->prev = cnt;
-    st->parity ^= 1u;
     const uint32_t stamp = st->stamp % 255u + 1u;
     st->stamp = stamp;
     st->clear_pending = stamp == 1u;
     if (!st->done && st->round >= st->max_rounds) st->error |= kErrRounds;
     const bool more = !st->done && !st->error;
     if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+// ---------------------------------------------------------------------------
+// Compaction (runs after k_fixpoint while the loop goes on).
+// ---------------------------------------------------------------------------
+
+// Keeps the non-singleton entries of the node list (order is not kept: the
+// relabel does not depend on it); dropped nodes are singleton blocks for good.
+static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
+                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
+{
+    if (st->done || st->error) return;
+    const uint32_t nn = as->nnodes;
+    const uint32_t* __restrict__ src = as->nodes;
+    uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    const int lane = threadIdx.x & 31;
+    uint32_t dropped = 0;
+    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
+        const uint32_t i = base + lane;
+        const bool valid = i < nn;
+        const uint32_t e = valid ? src[i] : 0u;
+        const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        uint32_t pos0 = 0;
+        if (lane == 0 && km) pos0 = atomicAdd(&as->nodectr, (uint32_t)__popc(km));
+        pos0 = __shfl_sync(0xffffffffu, pos0, 0);
+        if (keep) dst[pos0 + __popc(km & ((1u << lane) - 1u))] = e;
+        dropped += (valid && !keep) ? 1u : 0u;
+    }
+    dropped = __reduce_add_sync(0xffffffffu, dropped);
+    if (lane == 0 && dropped) atomicAdd(&as->retired, dropped);
+}
+
+// Counts and places the rows of non-singleton nodes of the current arc set in
+// the destination arc set.  One 64-bit atomic per warp reserves (rows, arcs)
+// together, so row order and arc order agree in the destination.
+static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
+                                                                      const uint32_t* __restrict__ col, CompactBufs bufs)
+{
+    if (st->done || st->error || !as->compact_arcs) return;
+    const uint32_t K = as->K;
+    const uint32_t* __restrict__ rows = as->rows;
+    const bool r64 = as->roff64 != 0;
+    const uint64_t* __restrict__ roff64 = reinterpret_cast<const uint64_t*>(as->roff);
+    const uint32_t* __restrict__ roff32 = reinterpret_cast<const uint32_t*>(as->roff);
+    const uint32_t d = as->dst_arcs;
+    uint32_t* __restrict__ drows = bufs.rows[d];
+    uint32_t* __restrict__ doff = bufs.off[d];
+    uint32_t* __restrict__ dsrc = bufs.src[d];
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    const int lane = threadIdx.x & 31;
+    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < K; base += stride) {
+        const uint32_t k = base + lane;
+        const bool valid = k < K;
+        uint32_t node = 0, deg = 0, start = 0;
+        bool keep = false;
+        if (valid) {
+            node = rows[k];
+            keep = !(col[node] & kSingleton);
+            if (keep) {
+                const uint64_t b = r64 ? roff64[k] : roff32[k];
+                const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
+                start = (uint32_t)b;
+                deg = (uint32_t)(e - b);
+            }
+        }
+        const unsigned km = __ballot_sync(0xffffffffu, keep);
+        uint32_t dsum = deg;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, dsum, o);
+            if (lane >= o) dsum += t;
+        }
+        const uint32_t wtot = __shfl_sync(0xffffffffu, dsum, 31);
+        unsigned long long old = 0;
+        if (lane == 0 && km) old = atomicAdd(&as->rowctr, ((unsigned long long)__popc(km) << 32) | wtot);
+        old = __shfl_sync(0xffffffffu, old, 0);
+        if (keep) {
+            const uint32_t kn = (uint32_t)(old >> 32) + __popc(km & ((1u << lane) - 1u));
+            drows[kn] = node;
+            doff[kn] = (uint32_t)old + dsum - deg;
+            dsrc[kn] = start;
+        }
+    }
+}
+
+// Decides whether the arc set is rebuilt: when its arcs dropped to 3/4 or less.
+static __global__ void k_compact_decide(ActiveSet* as, const RoundState* st, CompactBufs bufs)
+{
+    if (st->done || st->error || !as->compact_arcs) {
+        as->do_copy = 0;
+        return;
+    }
+    const uint32_t nk = (uint32_t)(as->rowctr >> 32);
+    const uint32_t nm = (uint32_t)(as->rowctr & 0xffffffffull);
+    const bool copy = nk > 0 && (uint64_t)nm * 4ull <= as->m * 3ull;
+    as->do_copy = copy ? 1u : 0u;
+    as->new_K = nk;
+    as->new_m = nm;
+    if (copy) {
+        const uint32_t d = as->dst_arcs;
+        bufs.off[d][nk] = nm;
+        bufs.tile_row[d][(nm + kTileEdges - 1) / kTileEdges] = nk;
+    }
+}
+
+// Copies the arcs of the kept rows (16 destination arcs per thread), and
+// builds the destination's row-head bitmap, tile rows and split list.  A row
+// entering the split list gets its signatures zeroed here.
+static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet* __restrict__ as, CompactBufs bufs,
+                                                                      unsigned long long* __restrict__ sig1,
+                                                                      uint32_t* __restrict__ sig2)
+{
+    if (!as->do_copy) return;
+    const uint32_t nk = as->new_K;
+    const uint32_t nm = as->new_m;
+    const uint32_t d = as->dst_arcs;
+    const uint32_t* __restrict__ doff = bufs.off[d];
+    const uint32_t* __restrict__ dsrc = bufs.src[d];
+    const uint32_t* __restrict__ drows = bufs.rows[d];
+    uint32_t* __restrict__ didx = bufs.idx[d];
+    uint64_t* __restrict__ dwt = bufs.wt[d];
+    const uint32_t* __restrict__ sidx = as->idx;
+    const uint64_t* __restrict__ swt = as->wt;
+    const uint32_t chunks = (nm + 15u) / 16u;
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    for (uint32_t ch = blockIdx.x * kNodeThreads + threadIdx.x; ch < chunks; ch += stride) {
+        const uint32_t e0 = ch * 16u;
+        // row holding arc e0: largest k with doff[k] <= e0
+        uint32_t lo = 0, hi = nk - 1u;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo + 1u) >> 1);
+            if (doff[mid] <= e0) lo = mid; else hi = mid - 1u;
+        }
+        const uint32_t k0 = lo;
+        uint32_t k = k0;
+        uint32_t rb = doff[k], re = doff[k + 1], src = dsrc[k];
+        uint32_t bits = 0;
+        for (uint32_t i = 0; i < 16u; ++i) {
+            const uint32_t e = e0 + i;
+            if (e >= nm) break;
+            while (e >= re) {
+                ++k;
+                rb = re;
+                re = doff[k + 1];
+                src = dsrc[k];
+            }
+            if (e == rb) bits |= 1u << i;
+            didx[e] = sidx[src + (e - rb)];
+            if (swt) dwt[e] = swt[src + (e - rb)];
+        }
+        *reinterpret_cast<uint16_t*>(bufs.head8[d] + (e0 >> 3)) = (uint16_t)bits;
+        if ((e0 & (kTileEdges - 1u)) == 0u) {
+            bufs.tile_row[d][e0 / kTileEdges] = k0;
+            if (e0 > 0 && doff[k0] < e0) {  // row k0 crosses this tile edge
+                const uint32_t node = drows[k0];
+                const uint32_t p = atomicAdd(&as->splitctr, 1u);
+                bufs.split[d][p] = node;
+                sig1[node] = 0ull;
+                sig2[node] = 0u;
+            }
+        }
+    }
+}
+
+// Switches the pass kernels to the compacted node list / arc set.
+static __global__ void k_compact_finalize(ActiveSet* as, const RoundState* st, CompactBufs bufs)
+{
+    if (st->done || st->error) return;
+    const uint32_t dn = as->dst_nodes;
+    as->nodes = bufs.nodes[dn];
+    as->nnodes = as->nodectr;
+    as->nodectr = 0;
+    as->dst_nodes = dn ^ 1u;
+    if (as->do_copy) {
+        const uint32_t d = as->dst_arcs;
+        as->rows = bufs.rows[d];
+        as->roff = bufs.off[d];
+        as->roff64 = 0;
+        as->tile_row = bufs.tile_row[d];
+        as->head8 = bufs.head8[d];
+        as->idx = bufs.idx[d];
+        as->wt = as->wt ? bufs.wt[d] : nullptr;
+        as->split = bufs.split[d];
+        as->nsplit = as->splitctr;
+        as->m = as->new_m;
+        as->K = as->new_K;
+        as->ntiles = (as->new_m + kTileEdges - 1) / kTileEdges;
+        as->dst_arcs = d ^ 1u;
+        as->do_copy = 0;
+    }
+    as->rowctr = 0;
+    as->splitctr = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Node list and followers, built once per refinement after the initial pass.
+// ---------------------------------------------------------------------------
+
+// For every group of arc-less nodes with the same initial label: its smallest
+// node (grep) and whether it has more than one member (gcnt, saturating at 2).
+// Most such nodes share a handful of labels, so the lanes of a warp with the
+// same label are combined first, and the global words are read before any
+// atomic: once a label's minimum and count are settled, later warps only read.
+static __global__ void k_group_reps(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ initlab,
+                                    uint32_t* __restrict__ grep, uint32_t* __restrict__ gcnt)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool dangling = u < n && off[u + 1] == off[u];
+    const unsigned dm = __ballot_sync(0xffffffffu, dangling);
+    if (!dangling) return;
+    const uint32_t g = initlab[u];
+    const unsigned peers = __match_any_sync(dm, g);
+    const uint32_t umin = __reduce_min_sync(peers, u);
+    if ((threadIdx.x & 31) != (uint32_t)(__ffs(peers) - 1)) return;
+    if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
+    if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
+}
+
+// Node list = non-singleton nodes that are not followers (representatives
+// flagged); follower pairs; singleton count.
+static __global__ void k_build_lists(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ initlab,
+                                     const uint32_t* __restrict__ col, const uint32_t* __restrict__ grep,
+                                     const uint32_t* __restrict__ gcnt, ActiveSet* __restrict__ as,
+                                     uint32_t* __restrict__ nodes, uint2* __restrict__ pairs)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const bool valid = u < n;
+    bool follower = false, rep = false, listed = false, single = false;
+    uint32_t r = 0;
+    if (valid) {
+        single = (col[u] & kSingleton) != 0;
+        if (!single && off[u + 1] == off[u]) {
+            const uint32_t g = initlab[u];
+            if (gcnt[g] >= 2u) {
+                r = grep[g];
+                follower = r != u;
+                rep = r == u;
+            }
+        }
+        listed = !single && !follower;
+    }
+    const unsigned lm = __ballot_sync(0xffffffffu, listed);
+    uint32_t p = 0;
+    if (lane == 0 && lm) p = atomicAdd(&as->nodectr, (uint32_t)__popc(lm));
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (listed) nodes[p + __popc(lm & ((1u << lane) - 1u))] = u | (rep ? kRepFlag : 0u);
+    const unsigned fm = __ballot_sync(0xffffffffu, follower);
+    uint32_t q = 0;
+    if (lane == 0 && fm) q = atomicAdd(&as->nfollow, (uint32_t)__popc(fm));
+    q = __shfl_sync(0xffffffffu, q, 0);
+    if (follower) pairs[q + __popc(fm & ((1u << lane) - 1u))] = make_uint2(u, r);
+    const unsigned sm = __ballot_sync(0xffffffffu, single);
+    if (lane == 0 && sm) atomicAdd(&as->retired, (uint32_t)__popc(sm));
+}
+
+// Zeroes the signatures of the given rows (the split rows of the whole-graph
+// tiling, before a refinement starts on it: an earlier refinement may have
+// left values there that the first pass would add to).
+static __global__ void k_zero_rows(const uint32_t* __restrict__ list, uint32_t count, unsigned long long* __restrict__ sig1,
+                                   uint32_t* __restrict__ sig2)
+{
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        sig1[list[i]] = 0ull;
+        sig2[list[i]] = 0u;
+    }
 }
 
 // k_clear_table: clears the table when the stamp wrapped.

@@ -10,6 +10,7 @@
 // smallest node id of the group as its label -- the first node of each group,
 // because every sort is stable and the node ids start in increasing order.
 // The labels are therefore identical to those of the hash-table relabel.
+// The sort covers every node (singletons included, as the reference does).
 #include <algorithm>
 #include <cuda_runtime.h>
 
@@ -48,23 +49,19 @@ __global__ void k_sr_gather_sig1(uint32_t n, const RoundState* __restrict__ st, 
     if (i < n) keys[i] = masked_sig1(st, sig1[perm[i]]);
 }
 
-__global__ void k_sr_gather_label(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ col0,
-                                  const uint32_t* __restrict__ col1, const uint32_t* __restrict__ perm,
+__global__ void k_sr_gather_label(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ perm,
                                   unsigned long long* __restrict__ keys)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t* col = st->parity ? col1 : col0;
     if (i < n) keys[i] = col[perm[i]] & kLabelMask;
 }
 
 // head[i] = position i starts a new (label, signature) group
-__global__ void k_sr_heads(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ col0,
-                           const uint32_t* __restrict__ col1, const uint32_t* __restrict__ perm,
-                           const unsigned long long* __restrict__ sig1, const uint32_t* __restrict__ sig2,
-                           uint32_t* __restrict__ head)
+__global__ void k_sr_heads(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ col,
+                           const uint32_t* __restrict__ perm, const unsigned long long* __restrict__ sig1,
+                           const uint32_t* __restrict__ sig2, uint32_t* __restrict__ head)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const uint32_t* col = st->parity ? col1 : col0;
     if (i >= n) return;
     uint32_t h = 1;
     if (i > 0) {
@@ -82,19 +79,22 @@ __global__ void k_sr_gstart(uint32_t n, const uint32_t* __restrict__ head, const
     if (i < n && head[i]) gstart[gid[i]] = i;
 }
 
-__global__ void k_sr_assign(uint32_t n, const RoundState* __restrict__ st, uint32_t* __restrict__ col0,
-                            uint32_t* __restrict__ col1, const uint32_t* __restrict__ perm, const uint32_t* __restrict__ head,
+// New colours in place (the sorts and group flags were computed from the old
+// ones in the previous kernels); also zeroes the signatures of the rows that
+// cross a tile edge of the current arc set.
+__global__ void k_sr_assign(uint32_t n, const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
+                            const uint32_t* __restrict__ perm, const uint32_t* __restrict__ head,
                             const uint32_t* __restrict__ gid, const uint32_t* __restrict__ gstart,
-                            const uint32_t* __restrict__ split_rows, uint32_t nsplit, unsigned long long* __restrict__ sig1,
-                            uint32_t* __restrict__ sig2)
+                            unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    uint32_t* nxt = st->parity ? col0 : col1;
     if (i < n) {
         const uint32_t grp = head[i] ? gid[i] : gid[i] - 1u;
         const bool single = head[i] && (i + 1 == n || head[i + 1]);
-        nxt[perm[i]] = perm[gstart[grp]] | (single ? kSingleton : 0u);
+        col[perm[i]] = perm[gstart[grp]] | (single ? kSingleton : 0u);
     }
+    const uint32_t nsplit = as->nsplit;
+    const uint32_t* __restrict__ split_rows = as->split;
     for (uint32_t k = i; k < nsplit; k += gridDim.x * blockDim.x) {
         const uint32_t node = split_rows[k];
         sig1[node] = 0ull;
@@ -160,21 +160,20 @@ rbsc_status launch_sort_relabel(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
         return rbsc_cuda_fail(ctx, e, "radix_sort (sig1)", __LINE__);
     if (alt) { std::swap(k0, k1); std::swap(p0, p1); }
     ++rbsc::launch_counter();
-    k_sr_gather_label<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], p0, k0);
+    k_sr_gather_label<<<grid, 256, 0, s>>>(n, g->d_col[0], p0, k0);
     if ((e = radix_sort<uint32_t>(k0, k1, p0, p1, n, 0, 31, g->d_sr_tmp, s, &alt)) != cudaSuccess)
         return rbsc_cuda_fail(ctx, e, "radix_sort (label)", __LINE__);
     if (alt) { std::swap(k0, k1); std::swap(p0, p1); }
     // p0 = sorted node order; p1 is free: use it for the group ids
     ++rbsc::launch_counter();
-    k_sr_heads<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], p0, g->d_sig1, g->d_sig2, g->d_sr_head);
+    k_sr_heads<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], p0, g->d_sig1, g->d_sig2, g->d_sr_head);
     uint32_t* count = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(g->d_st) + offsetof(RoundState, count));
     if ((e = exclusive_scan<uint32_t, uint32_t>(g->d_sr_head, p1, n, count, g->d_sr_tmp, s)) != cudaSuccess)
         return rbsc_cuda_fail(ctx, e, "exclusive_scan (heads)", __LINE__);
     ++rbsc::launch_counter();
     k_sr_gstart<<<grid, 256, 0, s>>>(n, g->d_sr_head, p1, g->d_sr_gstart);
     ++rbsc::launch_counter();
-    k_sr_assign<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], g->d_col[1], p0, g->d_sr_head, p1, g->d_sr_gstart, g->d_split,
-                                     g->nsplit, g->d_sig1, g->d_sig2);
+    k_sr_assign<<<grid, 256, 0, s>>>(n, g->d_as, g->d_col[0], p0, g->d_sr_head, p1, g->d_sr_gstart, g->d_sig1, g->d_sig2);
     if ((e = cudaGetLastError()) != cudaSuccess) return rbsc_cuda_fail(ctx, e, "sort relabel launch", __LINE__);
     return RBSC_OK;
 }

@@ -9,10 +9,13 @@
 //   for every node u of a non-singleton block with representative r (the
 //   block's smallest node): initial colour(u) == initial colour(r), and the
 //   multiset {(colour(v), summed weight)} over u's arcs equals r's.
-// The rows of all nodes in non-singleton blocks are turned into keys
-// (row << 31 | head colour), radix-sorted (which sorts every row's colours),
-// and u's sorted row is compared with r's.  Nodes that fail are split from
-// their block by an exact repair pass, and refinement resumes.
+// Short rows (at most 32 arcs, unit weights) are compared in registers: a
+// group of 8 or 32 lanes loads u's and r's head colours and bitonic-sorts
+// both.  Longer rows and weighted rows go through a global path: their rows
+// are turned into keys (row << 31 | head colour), radix-sorted (which sorts
+// every row's colours), and u's sorted row is compared with r's.  Nodes that
+// fail are split from their block by an exact repair pass, and refinement
+// resumes.
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
@@ -20,28 +23,138 @@
 
 namespace rbsc {
 
-// vflag[u] = u's row is needed by the check; vdeg[u] = its length if needed.
-static __global__ void k_verify_mark(uint32_t n, const uint32_t* __restrict__ col, const uint64_t* __restrict__ off,
-                              uint32_t* __restrict__ vflag, uint64_t* __restrict__ vdeg)
+struct VerifyLists {
+    uint32_t* l8;     // nodes whose row has 1..8 arcs
+    uint32_t* l32;    // 9..32 arcs
+    uint32_t* llong;  // longer or weighted rows
+    uint32_t* counts; // [0] = |l8|, [1] = |l32|, [2] = |llong|, [3] = failures
+};
+
+__device__ __forceinline__ void append(uint32_t* list, uint32_t* counter, bool take, uint32_t v)
+{
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    const int lane = threadIdx.x & 31;
+    uint32_t p = 0;
+    if (lane == 0 && m) p = atomicAdd(counter, (uint32_t)__popc(m));
+    p = __shfl_sync(0xffffffffu, p, 0);
+    if (take) list[p + __popc(m & ((1u << lane) - 1u))] = v;
+}
+
+// Classifies every node against its block's representative r (the block's
+// smallest node): quick failures (initial colour, row length), empty rows
+// (equal), short rows (lists l8 / l32), long or weighted rows (list llong;
+// their and r's rows are flagged for the global path in vflag).
+static __global__ void k_verify_classify(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ initlab,
+                                         const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
+                                         uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    bool t8 = false, t32 = false, tl = false, bad = false;
+    if (u < n) {
+        const uint32_t c = col[u];
+        const uint32_t r = c & kLabelMask;
+        if (!(c & kSingleton) && r != u) {
+            const uint64_t du = off[u + 1] - off[u], dr = off[r + 1] - off[r];
+            if (initlab[u] != initlab[r]) bad = true;
+            else if (weighted) tl = du > 0 || dr > 0;
+            else if (du != dr) bad = true;
+            else if (du == 0) {}
+            else if (du <= 8) t8 = true;
+            else if (du <= 32) t32 = true;
+            else tl = true;
+            if (tl) {
+                vflag[u] = 1u;
+                vflag[r] = 1u;
+            }
+            if (bad) fail[u] = 1u;
+        }
+    }
+    append(vl.l8, &vl.counts[0], t8, u);
+    append(vl.l32, &vl.counts[1], t32, u);
+    append(vl.llong, &vl.counts[2], tl, u);
+    const unsigned bm = __ballot_sync(0xffffffffu, bad);
+    if ((threadIdx.x & 31) == 0 && bm) atomicAdd(&vl.counts[3], (uint32_t)__popc(bm));
+}
+
+// Bitonic sort of one value per lane across aligned groups of G lanes.
+template <int G> __device__ __forceinline__ uint32_t group_sort(uint32_t v)
+{
+    const int gl = threadIdx.x & (G - 1);
+#pragma unroll
+    for (int k = 2; k <= G; k <<= 1) {
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            const uint32_t o = __shfl_xor_sync(0xffffffffu, v, j);
+            const bool up = (gl & k) == 0;
+            const bool lower = (gl & j) == 0;
+            v = (lower == up) ? min(v, o) : max(v, o);
+        }
+    }
+    return v;
+}
+
+// Groups of G lanes compare the sorted head colours of u and its block's
+// representative (rows of equal length <= G, unit weights).
+template <int G>
+static __global__ void k_verify_short(uint32_t n, const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                      const uint32_t* __restrict__ col, const uint64_t* __restrict__ off,
+                                      const uint32_t* __restrict__ idx, uint32_t* __restrict__ fail,
+                                      uint32_t* __restrict__ nfail)
+{
+    const uint32_t cnt = *count;
+    const int gl = threadIdx.x & (G - 1);
+    const unsigned gmask = (G == 32) ? 0xffffffffu : (((1u << G) - 1u) << ((threadIdx.x & 31) & ~(G - 1)));
+    constexpr uint32_t kGroupsPerWarp = 32 / G;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t nwarps = (gridDim.x * blockDim.x) >> 5;
+    const uint32_t gw = (threadIdx.x & 31) / G;
+    // the loop runs the same number of times on every lane of a warp (the
+    // shuffles need all 32); groups past the end carry no work
+    for (uint32_t wb = warp * kGroupsPerWarp; wb < cnt; wb += nwarps * kGroupsPerWarp) {
+        const uint32_t gi = wb + gw;
+        const bool valid = gi < cnt;
+        uint32_t a = 0xffffffffu, b = 0xffffffffu;
+        uint32_t u = 0;
+        if (valid) {
+            u = list[gi];
+            const uint32_t r = col[u] & kLabelMask;
+            const uint64_t ou = off[u], orr = off[r];
+            const uint32_t d = (uint32_t)(off[u + 1] - ou);
+            if ((uint32_t)gl < d) {
+                a = col[idx[ou + gl]] & kLabelMask;
+                b = col[idx[orr + gl]] & kLabelMask;
+            }
+        }
+        a = group_sort<G>(a);
+        b = group_sort<G>(b);
+        const unsigned diff = __ballot_sync(0xffffffffu, a != b) & gmask;
+        if (valid && gl == 0 && diff) {
+            fail[u] = 1u;
+            atomicAdd(nfail, 1u);
+        }
+    }
+}
+
+// vflag[u] = u's row is needed by the global path; vdeg[u] = its length.
+static __global__ void k_verify_mark(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ vflag,
+                              uint64_t* __restrict__ vdeg)
 {
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
-    const uint64_t d = off[u + 1] - off[u];
-    const bool need = !(col[u] & kSingleton) && d > 0;
-    vflag[u] = need ? 1u : 0u;
-    vdeg[u] = need ? d : 0ull;
+    vdeg[u] = vflag[u] ? off[u + 1] - off[u] : 0ull;
 }
 
 // Keys of the needed rows: (row index << 31) | colour of the head.
 static __global__ void k_verify_keys(uint32_t n, const uint32_t* __restrict__ col, const uint64_t* __restrict__ off,
                               const uint32_t* __restrict__ idx, const uint64_t* __restrict__ wt,
-                              const uint32_t* __restrict__ vrow, const uint64_t* __restrict__ voff,
-                              unsigned long long* __restrict__ keys, unsigned long long* __restrict__ vals)
+                              const uint32_t* __restrict__ vflag, const uint32_t* __restrict__ vrow,
+                              const uint64_t* __restrict__ voff, unsigned long long* __restrict__ keys,
+                              unsigned long long* __restrict__ vals)
 {
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
     const uint64_t b = off[u], e = off[u + 1];
-    if (e == b || (col[u] & kSingleton)) return;
+    if (e == b || !vflag[u]) return;
     const uint64_t row = vrow[u];
     const uint64_t base = voff[u];
     for (uint64_t k = b; k < e; ++k) {
@@ -68,17 +181,19 @@ __device__ __forceinline__ bool next_run(const unsigned long long* keys, const u
     return false;
 }
 
-// One warp per node (grid-stride).  fail[u] = 1 when u's row differs from its
-// representative's.
-static __global__ void k_verify_compare(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ initlab,
+// One warp per node of the long list (grid-stride).  fail[u] = 1 when u's
+// row differs from its representative's.
+static __global__ void k_verify_compare(const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
+                                 const uint32_t* __restrict__ col, const uint32_t* __restrict__ initlab,
                                  const uint64_t* __restrict__ off, const uint64_t* __restrict__ voff,
                                  const unsigned long long* __restrict__ keys, const unsigned long long* __restrict__ vals,
                                  uint32_t* __restrict__ fail, uint32_t* __restrict__ nfail)
 {
     const int lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < n; w += warps) {
-        const uint32_t u = (uint32_t)w;
+    const uint32_t cnt = *count;
+    for (uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; w < cnt; w += warps) {
+        const uint32_t u = list[w];
         const uint32_t c = col[u];
         const uint32_t r = c & kLabelMask;
         if ((c & kSingleton) || r == u) continue;

@@ -72,6 +72,11 @@ def _random_cases():
     yield "weighted", off, idx, wt, None
     off, idx = G.er_undirected(400, 4.0, seed=8)
     yield "labels", off, idx, None, np.random.default_rng(8).integers(1, 9, size=400).astype(np.uint32)
+    # rows longer than 32 arcs in non-singleton blocks (global path of the exact check)
+    off, idx = G.complete_bipartite(40, 45)
+    yield "bipartite40x45", off, idx, None, None
+    off, idx = G.random_lift(48, 48 * 40, 4, seed=9)
+    yield "dense_lift", off, idx, None, None
     # multi-arcs and self-loops count with multiplicity
     s = np.array([0, 0, 0, 1, 1, 2, 2, 2, 3, 3, 3, 4])
     d = np.array([1, 1, 2, 2, 1, 0, 0, 2, 4, 4, 3, 4])
@@ -111,6 +116,11 @@ def test_forced_collisions_are_repaired(bits, relabel):
         ex = oracle.refine_exact(off, idx, wt)
         r = c.refine(off, idx, wt)
         assert np.array_equal(r.labels, ex.labels)
+        # long rows: the collisions must be caught by the sort-based comparison
+        off, idx = G.random_lift(40, 40 * 36, 3, seed=2)
+        ex = oracle.refine_exact(off, idx)
+        r = c.refine(off, idx)
+        assert np.array_equal(r.labels, ex.labels) and r.blocks == ex.blocks
 
 
 def test_edge_cases(ctx):
@@ -146,14 +156,23 @@ def test_long_path_wraps_table_stamp(ctx):
     assert r.rounds == 700
 
 
-def test_resident_graph_repeatable(ctx):
-    off, idx = G.rmat(12, 8, seed=4)
+@pytest.mark.parametrize("scale", [12, 16])
+def test_resident_graph_repeatable(ctx, scale):
+    """Refinements of one resident graph are independent of each other (state
+    left by an earlier call -- compacted arc sets, table stamps, signatures --
+    must not leak into the next)."""
+    off, idx = G.rmat(scale, 8, seed=4)
     g = ctx.upload(off, idx)
     init = R.degree_bucket_colors(off)
     ex = oracle.refine_exact(off, idx, init=init)
     for _ in range(3):
         r = g.refine(init)
         _check_against(r, ex.labels, ex.blocks, ex.rounds)
+        assert r.repairs == 0
+        u = g.refine()
+        assert u.repairs == 0 and u.verified == 1
+    ex_u = oracle.refine_exact(off, idx)
+    assert np.array_equal(u.labels, ex_u.labels) and u.rounds == ex_u.rounds
     g.free()
 
 
