@@ -99,10 +99,15 @@ typedef struct {
 typedef struct {
     uint32_t passes;          /* hashed passes timed                                     */
     double signature_ms;      /* total over the passes: k_signature                     */
-    double insert_ms;         /* k_insert (or the sort-based relabel's sorts)            */
-    double relabel_ms;        /* k_relabel                                               */
-    double other_ms;          /* table clear + fixpoint kernels                          */
+    double insert_ms;         /* table inserts (or the sort-based relabel's sorts)       */
+    double relabel_ms;        /* relabel + follower copy                                 */
+    double other_ms;          /* table clear, fixpoint test, compaction                  */
     double total_ms;          /* whole refinement, including the exact check             */
+    double init_ms;           /* initial-colour pass                                     */
+    double setup_ms;          /* node list / follower construction                       */
+    float pass_ms[32][4];     /* per pass (first 32): signature, insert, relabel, other  */
+    uint64_t pass_arcs[32];   /* arcs in the signature pass                              */
+    uint32_t pass_nodes[32];  /* nodes in the relabel list                               */
 } rbsc_kernel_times;
 
 /* A CSR graph.  `offsets` has n+1 entries of `offset_bytes` (4 or 8) bytes;

@@ -222,7 +222,12 @@ class Graph:
         st = _lib.Stats()
         _check(lib, lib.rbsc_graph_profile(self.ctx._h, self._h, d_init, ctypes.byref(kt), ctypes.byref(st)),
                self.ctx._h)
-        times = {k: getattr(kt, k) for k, _ in _lib.KernelTimes._fields_}
+        times = {k: getattr(kt, k) for k, _ in _lib.KernelTimes._fields_
+                 if k not in ("pass_ms", "pass_arcs", "pass_nodes")}
+        np_ = min(32, kt.passes)
+        times["per_pass"] = [dict(signature_ms=kt.pass_ms[i][0], insert_ms=kt.pass_ms[i][1],
+                                  relabel_ms=kt.pass_ms[i][2], other_ms=kt.pass_ms[i][3],
+                                  arcs=int(kt.pass_arcs[i]), nodes=int(kt.pass_nodes[i])) for i in range(np_)]
         return times, _result(st, None)
 
     def degree_colors_device(self, d_out: int):

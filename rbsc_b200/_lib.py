@@ -80,6 +80,11 @@ class KernelTimes(ctypes.Structure):
         ("relabel_ms", ctypes.c_double),
         ("other_ms", ctypes.c_double),
         ("total_ms", ctypes.c_double),
+        ("init_ms", ctypes.c_double),
+        ("setup_ms", ctypes.c_double),
+        ("pass_ms", (ctypes.c_float * 4) * 32),
+        ("pass_arcs", ctypes.c_uint64 * 32),
+        ("pass_nodes", ctypes.c_uint32 * 32),
     ]
 
 

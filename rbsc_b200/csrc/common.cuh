@@ -60,6 +60,54 @@ __host__ __device__ __forceinline__ uint32_t pass_salt2(uint64_t seed, uint32_t 
 
 template <typename T> __host__ __device__ __forceinline__ T ceil_div(T a, T b) { return (a + b - 1) / b; }
 
+// Block-wide reservation in an output list: every thread with `take` gets a
+// distinct position; the block makes one atomicAdd on `counter` (a global
+// counter shared by all blocks), instead of one per warp.  Must be called by
+// all threads of the block (it synchronises twice).  BLOCK = threads per block.
+template <int BLOCK> struct BlockReserveSmem {
+    uint32_t warp_pre[BLOCK / 32];
+    unsigned long long base;
+};
+
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_reserve(bool take, uint32_t* counter, BlockReserveSmem<BLOCK>& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (lane == 0) sm.warp_pre[warp] = (uint32_t)__popc(m);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            const uint32_t c = sm.warp_pre[w];
+            sm.warp_pre[w] = run;
+            run += c;
+        }
+        sm.base = run ? atomicAdd(counter, run) : 0u;
+    }
+    __syncthreads();
+    const uint32_t pos = (uint32_t)sm.base + sm.warp_pre[warp] + (uint32_t)__popc(m & ((1u << lane) - 1u));
+    __syncthreads();
+    return pos;
+}
+
+// Sum over the block of a per-thread count, added to `counter` with one
+// atomic per block.  Called by all threads of the block.
+template <int BLOCK>
+__device__ __forceinline__ void block_count(uint32_t v, uint32_t* counter, BlockReserveSmem<BLOCK>& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    v = __reduce_add_sync(0xffffffffu, v);
+    if (lane == 0) sm.warp_pre[warp] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) run += sm.warp_pre[w];
+        if (run) atomicAdd(counter, run);
+    }
+    __syncthreads();
+}
+
 // Kernels enqueued by the calling host thread (reported in rbsc_stats).
 inline uint64_t& launch_counter()
 {

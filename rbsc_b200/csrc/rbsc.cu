@@ -640,11 +640,25 @@ static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt,
         if (kt)
             for (auto& e : t.ev) CK(cudaEventCreate(&e));
         for (;;) {
+            ActiveSet before;
+            if (kt) {
+                CK(cudaMemcpyAsync(&before, g->d_as, sizeof before, cudaMemcpyDeviceToHost, ctx->stream));
+                CK(cudaStreamSynchronize(ctx->stream));
+            }
             rbsc_status st = launch_pass(ctx, g, ctx->stream, cudaGraphConditionalHandle(), 0, kt ? &t : nullptr);
             if (st == RBSC_OK) st = read_state(ctx, g);
             if (st == RBSC_OK && kt) {
                 float ms[5];
                 for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], t.ev[i], t.ev[i + 1]);
+                if (kt->passes < 32) {
+                    float* pm = kt->pass_ms[kt->passes];
+                    pm[0] = ms[1];
+                    pm[1] = ms[2];
+                    pm[2] = ms[3];
+                    pm[3] = ms[0] + ms[4];
+                    kt->pass_arcs[kt->passes] = before.m;
+                    kt->pass_nodes[kt->passes] = before.nnodes;
+                }
                 kt->passes += 1;
                 kt->other_ms += ms[0] + ms[4];
                 kt->signature_ms += ms[1];
@@ -871,7 +885,21 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     CK(cudaGetLastError());
     CKS(read_state(ctx, g));
     const uint32_t initial_blocks = hs.prev;
+    if (kt) {
+        CK(cudaEventRecord(ctx->ev[4], s));
+        CK(cudaEventSynchronize(ctx->ev[4]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]);
+        kt->init_ms = ms;
+    }
     CKS(init_active_set(ctx, g));
+    if (kt) {
+        CK(cudaEventRecord(ctx->ev[5], s));
+        CK(cudaEventSynchronize(ctx->ev[5]));
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
+        kt->setup_ms = ms;
+    }
     CK(cudaEventRecord(ctx->ev[4], s));
     CK(cudaEventSynchronize(ctx->ev[4]));
     float init_ms = 0.f;

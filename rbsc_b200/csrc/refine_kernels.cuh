@@ -372,8 +372,16 @@ static __global__ void k_head_bits(uint32_t K, const OffT* __restrict__ roff, ui
 // once for the group, offering the group's smallest node as the class label.
 // Counts the classes it creates.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ void insert_warp(bool need, uint32_t u, bool rep, uint64_t k1, uint32_t k2, uint32_t stamp,
-                                            Entry* tab, uint32_t log2size, uint32_t* slot, uint32_t* err,
+// log2 of the table window used for a list of `count` keys (load <= 1/2).
+__device__ __forceinline__ uint32_t table_window(uint32_t count, uint32_t log2size)
+{
+    uint32_t w = 10;
+    while (w < log2size && (1ull << w) < 2ull * count) ++w;
+    return w;
+}
+
+__device__ __forceinline__ void insert_warp(bool need, uint32_t u, uint32_t slot_index, bool rep, uint64_t k1, uint32_t k2,
+                                            uint32_t stamp, Entry* tab, uint32_t log2size, uint32_t* slot, uint32_t* err,
                                             bool& new_block)
 {
     const int lane = threadIdx.x & 31;
@@ -389,7 +397,7 @@ __device__ __forceinline__ void insert_warp(bool need, uint32_t u, bool rep, uin
         if (lane == leader)
             s = table_insert(tab, log2size, k1, k2, stamp, umin, __popc(peers) > 1 || (rep_mask & peers), &claimed, err);
         s = __shfl_sync(peers, s, leader);
-        slot[u] = s;
+        slot[slot_index] = s;
         new_block = (lane == leader) && claimed;
     }
 }
@@ -400,7 +408,7 @@ __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
     if ((threadIdx.x & 31) == 0 && nb) atomicAdd(counter, (uint32_t)__popc(nb));
 }
 
-// Hashed pass over the node list (persistent, grid-stride by warps).
+// Hashed pass over the node list (persistent, grid-stride by blocks).
 static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                                      const uint32_t* __restrict__ col,
                                                                      const unsigned long long* __restrict__ sig1,
@@ -408,12 +416,16 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
                                                                      Entry* __restrict__ tab, uint32_t log2size,
                                                                      uint32_t* __restrict__ slot)
 {
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
     const uint32_t stamp = st->stamp;
     const uint32_t hb = st->hash_bits;
     const uint64_t seed = st->seed;
     const uint32_t stride = gridDim.x * kNodeThreads;
+    // probe only the first 2^k entries, 2^k >= 2 * list length: the table of
+    // a late pass with few active nodes stays in L2
+    const uint32_t log2win = table_window(nn, log2size);
     uint32_t made = 0;
     for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
         const uint32_t i = base + (threadIdx.x & 31);
@@ -436,12 +448,10 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
             k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
         }
         bool nb = active && !need;
-        insert_warp(need, u, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2size, slot, &st->error, nb);
+        insert_warp(need, u, i, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
         made += nb ? 1u : 0u;
     }
-    // one atomic per warp
-    made = __reduce_add_sync(0xffffffffu, made);
-    if ((threadIdx.x & 31) == 0 && made) atomicAdd(&st->count, made);
+    block_count<kNodeThreads>(made, &st->count, sm);
 }
 
 // Exact pass over all nodes: initial colours (MODE kModeInit, aux = colours)
@@ -460,19 +470,22 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_all(uint32_t n, 
     uint64_t k1 = 0;
     if (need) k1 = (MODE == kModeInit) ? (uint64_t)aux[u] : ((uint64_t)(c & kLabelMask) | ((uint64_t)(aux[u] != 0u) << 32));
     bool nb = active && !need;
-    insert_warp(need, u, false, k1, stamp, stamp, tab, log2size, slot, &st->error, nb);
-    count_blocks(nb, &st->count);
+    insert_warp(need, u, u, false, k1, stamp, stamp, tab, log2size, slot, &st->error, nb);
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
+    block_count<kNodeThreads>(nb ? 1u : 0u, &st->count, sm);
 }
 
-__device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, const uint32_t* slot, uint32_t u)
+__device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, uint32_t s)
 {
     if (c & kSingleton) return c;
-    const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(tab + slot[u]) + 3);
+    const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(tab + s) + 3);
     return (v & kLabelMask) | ((v & kJoined) ? 0u : kSingleton);
 }
 
-// New colours of the node list, in place; also zeroes the signatures of the
-// rows that cross a tile edge (the next pass adds into them atomically).
+// New colours of the node list, in place (slots are indexed by list
+// position); also zeroes the signatures of the rows that cross a tile edge
+// (the next pass adds into them atomically).  Four list entries per thread
+// and iteration, so their dependent loads overlap.
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
                                                                       const Entry* __restrict__ tab,
                                                                       const uint32_t* __restrict__ slot,
@@ -482,9 +495,20 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const Acti
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
     const uint32_t stride = gridDim.x * kNodeThreads;
-    for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < nn; i += stride) {
-        const uint32_t u = nodes[i] & ~kRepFlag;
-        col[u] = relabel_one(col[u], tab, slot, u);
+    constexpr int U = 4;
+    for (uint32_t i0 = blockIdx.x * kNodeThreads + threadIdx.x; i0 < nn; i0 += U * stride) {
+        uint32_t u[U], s[U], c[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t i = i0 + j * stride;
+            u[j] = i < nn ? (nodes[i] & ~kRepFlag) : 0xffffffffu;
+            s[j] = i < nn ? slot[i] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) c[j] = u[j] != 0xffffffffu ? col[u[j]] : kSingleton;
+#pragma unroll
+        for (int j = 0; j < U; ++j)
+            if (u[j] != 0xffffffffu) col[u[j]] = relabel_one(c[j], tab, s[j]);
     }
     const uint32_t ns = as->nsplit;
     const uint32_t* __restrict__ split = as->split;
@@ -501,7 +525,10 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n,
                                                                      const uint32_t* __restrict__ slot)
 {
     const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
-    if (u < n) col[u] = relabel_one(col[u], tab, slot, u);
+    if (u < n) {
+        const uint32_t c = col[u];
+        if (!(c & kSingleton)) col[u] = relabel_one(c, tab, slot[u]);
+    }
 }
 
 // Followers (arc-less nodes that are not their group's representative) take
@@ -561,35 +588,33 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                        const uint32_t* __restrict__ col, CompactBufs bufs)
 {
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
     if (st->done || st->error) return;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ src = as->nodes;
     uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
     const uint32_t stride = gridDim.x * kNodeThreads;
-    const int lane = threadIdx.x & 31;
     uint32_t dropped = 0;
-    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
-        const uint32_t i = base + lane;
+    for (uint32_t base = blockIdx.x * kNodeThreads; base < nn; base += stride) {
+        const uint32_t i = base + threadIdx.x;
         const bool valid = i < nn;
         const uint32_t e = valid ? src[i] : 0u;
         const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
-        const unsigned km = __ballot_sync(0xffffffffu, keep);
-        uint32_t pos0 = 0;
-        if (lane == 0 && km) pos0 = atomicAdd(&as->nodectr, (uint32_t)__popc(km));
-        pos0 = __shfl_sync(0xffffffffu, pos0, 0);
-        if (keep) dst[pos0 + __popc(km & ((1u << lane) - 1u))] = e;
+        const uint32_t pos = block_reserve<kNodeThreads>(keep, &as->nodectr, sm);
+        if (keep) dst[pos] = e;
         dropped += (valid && !keep) ? 1u : 0u;
     }
-    dropped = __reduce_add_sync(0xffffffffu, dropped);
-    if (lane == 0 && dropped) atomicAdd(&as->retired, dropped);
+    block_count<kNodeThreads>(dropped, &as->retired, sm);
 }
 
 // Counts and places the rows of non-singleton nodes of the current arc set in
-// the destination arc set.  One 64-bit atomic per warp reserves (rows, arcs)
+// the destination arc set.  One 64-bit atomic per block reserves (rows, arcs)
 // together, so row order and arc order agree in the destination.
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
+    __shared__ unsigned long long s_warp[kNodeThreads / 32];
+    __shared__ unsigned long long s_base;
     if (st->done || st->error || !as->compact_arcs) return;
     const uint32_t K = as->K;
     const uint32_t* __restrict__ rows = as->rows;
@@ -601,13 +626,12 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
     uint32_t* __restrict__ doff = bufs.off[d];
     uint32_t* __restrict__ dsrc = bufs.src[d];
     const uint32_t stride = gridDim.x * kNodeThreads;
-    const int lane = threadIdx.x & 31;
-    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < K; base += stride) {
-        const uint32_t k = base + lane;
-        const bool valid = k < K;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t base = blockIdx.x * kNodeThreads; base < K; base += stride) {
+        const uint32_t k = base + threadIdx.x;
         uint32_t node = 0, deg = 0, start = 0;
         bool keep = false;
-        if (valid) {
+        if (k < K) {
             node = rows[k];
             keep = !(col[node] & kSingleton);
             if (keep) {
@@ -617,23 +641,34 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
                 deg = (uint32_t)(e - b);
             }
         }
-        const unsigned km = __ballot_sync(0xffffffffu, keep);
-        uint32_t dsum = deg;
+        // per-thread (rows, arcs) packed: rows in the high half
+        unsigned long long v = keep ? ((1ull << 32) | deg) : 0ull;
+        unsigned long long incl = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t t = __shfl_up_sync(0xffffffffu, dsum, o);
-            if (lane >= o) dsum += t;
+            const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += t;
         }
-        const uint32_t wtot = __shfl_sync(0xffffffffu, dsum, 31);
-        unsigned long long old = 0;
-        if (lane == 0 && km) old = atomicAdd(&as->rowctr, ((unsigned long long)__popc(km) << 32) | wtot);
-        old = __shfl_sync(0xffffffffu, old, 0);
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned long long run = 0;
+            for (int w = 0; w < kNodeThreads / 32; ++w) {
+                const unsigned long long c = s_warp[w];
+                s_warp[w] = run;
+                run += c;
+            }
+            s_base = run ? atomicAdd(&as->rowctr, run) : 0ull;
+        }
+        __syncthreads();
         if (keep) {
-            const uint32_t kn = (uint32_t)(old >> 32) + __popc(km & ((1u << lane) - 1u));
+            const unsigned long long pos = s_base + s_warp[warp] + incl - v;
+            const uint32_t kn = (uint32_t)(pos >> 32);
             drows[kn] = node;
-            doff[kn] = (uint32_t)old + dsum - deg;
+            doff[kn] = (uint32_t)pos;
             dsrc[kn] = start;
         }
+        __syncthreads();
     }
 }
 
@@ -752,22 +787,55 @@ static __global__ void k_compact_finalize(ActiveSet* as, const RoundState* st, C
 
 // For every group of arc-less nodes with the same initial label: its smallest
 // node (grep) and whether it has more than one member (gcnt, saturating at 2).
-// Most such nodes share a handful of labels, so the lanes of a warp with the
-// same label are combined first, and the global words are read before any
-// atomic: once a label's minimum and count are settled, later warps only read.
-static __global__ void k_group_reps(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ initlab,
-                                    uint32_t* __restrict__ grep, uint32_t* __restrict__ gcnt)
+// Most such nodes share a handful of labels, so they are combined per warp
+// (__match_any_sync), then per block in a small shared-memory table, and
+// only then in global memory, where the words are read before any atomic:
+// once a label's minimum and count are settled, later blocks only read.
+constexpr int kRepSlots = 64;
+static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uint64_t* __restrict__ off,
+                                                           const uint32_t* __restrict__ initlab,
+                                                           uint32_t* __restrict__ grep, uint32_t* __restrict__ gcnt)
 {
+    __shared__ uint32_t s_lab[kRepSlots], s_min[kRepSlots], s_cnt[kRepSlots];
+    for (int i = threadIdx.x; i < kRepSlots; i += blockDim.x) {
+        s_lab[i] = 0xffffffffu;
+        s_min[i] = 0xffffffffu;
+        s_cnt[i] = 0u;
+    }
+    __syncthreads();
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     const bool dangling = u < n && off[u + 1] == off[u];
     const unsigned dm = __ballot_sync(0xffffffffu, dangling);
-    if (!dangling) return;
-    const uint32_t g = initlab[u];
-    const unsigned peers = __match_any_sync(dm, g);
-    const uint32_t umin = __reduce_min_sync(peers, u);
-    if ((threadIdx.x & 31) != (uint32_t)(__ffs(peers) - 1)) return;
-    if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
-    if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
+    if (dangling) {
+        const uint32_t g = initlab[u];
+        const unsigned peers = __match_any_sync(dm, g);
+        const uint32_t umin = __reduce_min_sync(peers, u);
+        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) {
+            // open-addressed shared table keyed by label; a full table falls
+            // back to the global words directly
+            uint32_t h = (g * 0x9e3779b1u) >> 26;
+            bool placed = false;
+            for (int p = 0; p < kRepSlots && !placed; ++p, h = (h + 1) & (kRepSlots - 1)) {
+                const uint32_t prev = atomicCAS(&s_lab[h], 0xffffffffu, g);
+                if (prev == 0xffffffffu || prev == g) {
+                    atomicMin(&s_min[h], umin);
+                    atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
+                    placed = true;
+                }
+            }
+            if (!placed) {
+                if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
+                if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kRepSlots; i += blockDim.x) {
+        const uint32_t g = s_lab[i];
+        if (g == 0xffffffffu) continue;
+        if (*(volatile uint32_t*)&grep[g] > s_min[i]) atomicMin(&grep[g], s_min[i]);
+        if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], s_cnt[i]);
+    }
 }
 
 // Node list = non-singleton nodes that are not followers (representatives
@@ -777,8 +845,8 @@ static __global__ void k_build_lists(uint32_t n, const uint64_t* __restrict__ of
                                      const uint32_t* __restrict__ gcnt, ActiveSet* __restrict__ as,
                                      uint32_t* __restrict__ nodes, uint2* __restrict__ pairs)
 {
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
     const bool valid = u < n;
     bool follower = false, rep = false, listed = false, single = false;
     uint32_t r = 0;
@@ -794,18 +862,11 @@ static __global__ void k_build_lists(uint32_t n, const uint64_t* __restrict__ of
         }
         listed = !single && !follower;
     }
-    const unsigned lm = __ballot_sync(0xffffffffu, listed);
-    uint32_t p = 0;
-    if (lane == 0 && lm) p = atomicAdd(&as->nodectr, (uint32_t)__popc(lm));
-    p = __shfl_sync(0xffffffffu, p, 0);
-    if (listed) nodes[p + __popc(lm & ((1u << lane) - 1u))] = u | (rep ? kRepFlag : 0u);
-    const unsigned fm = __ballot_sync(0xffffffffu, follower);
-    uint32_t q = 0;
-    if (lane == 0 && fm) q = atomicAdd(&as->nfollow, (uint32_t)__popc(fm));
-    q = __shfl_sync(0xffffffffu, q, 0);
-    if (follower) pairs[q + __popc(fm & ((1u << lane) - 1u))] = make_uint2(u, r);
-    const unsigned sm = __ballot_sync(0xffffffffu, single);
-    if (lane == 0 && sm) atomicAdd(&as->retired, (uint32_t)__popc(sm));
+    const uint32_t p = block_reserve<kNodeThreads>(listed, &as->nodectr, sm);
+    if (listed) nodes[p] = u | (rep ? kRepFlag : 0u);
+    const uint32_t q = block_reserve<kNodeThreads>(follower, &as->nfollow, sm);
+    if (follower) pairs[q] = make_uint2(u, r);
+    block_count<kNodeThreads>(single ? 1u : 0u, &as->retired, sm);
 }
 
 // Zeroes the signatures of the given rows (the split rows of the whole-graph

@@ -30,16 +30,6 @@ struct VerifyLists {
     uint32_t* counts; // [0] = |l8|, [1] = |l32|, [2] = |llong|, [3] = failures
 };
 
-__device__ __forceinline__ void append(uint32_t* list, uint32_t* counter, bool take, uint32_t v)
-{
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    const int lane = threadIdx.x & 31;
-    uint32_t p = 0;
-    if (lane == 0 && m) p = atomicAdd(counter, (uint32_t)__popc(m));
-    p = __shfl_sync(0xffffffffu, p, 0);
-    if (take) list[p + __popc(m & ((1u << lane) - 1u))] = v;
-}
-
 // Classifies every node against its block's representative r (the block's
 // smallest node): quick failures (initial colour, row length), empty rows
 // (equal), short rows (lists l8 / l32), long or weighted rows (list llong;
@@ -69,11 +59,14 @@ static __global__ void k_verify_classify(uint32_t n, const uint32_t* __restrict_
             if (bad) fail[u] = 1u;
         }
     }
-    append(vl.l8, &vl.counts[0], t8, u);
-    append(vl.l32, &vl.counts[1], t32, u);
-    append(vl.llong, &vl.counts[2], tl, u);
-    const unsigned bm = __ballot_sync(0xffffffffu, bad);
-    if ((threadIdx.x & 31) == 0 && bm) atomicAdd(&vl.counts[3], (uint32_t)__popc(bm));
+    __shared__ BlockReserveSmem<256> sm;
+    uint32_t p = block_reserve<256>(t8, &vl.counts[0], sm);
+    if (t8) vl.l8[p] = u;
+    p = block_reserve<256>(t32, &vl.counts[1], sm);
+    if (t32) vl.l32[p] = u;
+    p = block_reserve<256>(tl, &vl.counts[2], sm);
+    if (tl) vl.llong[p] = u;
+    block_count<256>(bad ? 1u : 0u, &vl.counts[3], sm);
 }
 
 // Bitonic sort of one value per lane across aligned groups of G lanes.
