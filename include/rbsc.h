@@ -66,8 +66,10 @@ typedef struct {
                                  device-side while node; 0 = host-driven loop           */
     uint64_t seed;            /* hash salt seed                                          */
     int32_t test_hash_bits;   /* TEST HOOK: keep only the low k bits of every signature
-                                 (0 = off).  Forces hash collisions so the exact check
-                                 and repair path can be exercised.                      */
+                                 (0 = off; k < 0 or k >= 64: drop signatures entirely, so
+                                 the hashed rounds never split and every split comes
+                                 from the exact check and repair).  Forces collisions so
+                                 the exact check and repair path can be exercised.      */
     int32_t reserved[7];
 } rbsc_opts;
 

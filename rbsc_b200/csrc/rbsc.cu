@@ -858,7 +858,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     std::memset(&hs, 0, sizeof hs);
     hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);
     hs.seed = ctx->opts.seed;
-    hs.hash_bits = (uint32_t)std::max(0, ctx->opts.test_hash_bits);
+    hs.hash_bits = ctx->opts.test_hash_bits < 0 ? 64u : (uint32_t)ctx->opts.test_hash_bits;
     hs.stamp = g->next_stamp;
     hs.clear_pending = 0;
     CK(cudaEventRecord(ctx->ev[0], s));

@@ -440,8 +440,8 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
             const uint32_t lab = c & kLabelMask;
             uint64_t s1 = sig1[u];
             uint32_t s2 = sig2[u];
-            if (hb) {
-                s1 &= (hb >= 64) ? ~0ull : ((1ull << hb) - 1ull);
+            if (hb) {  // test hook: truncated (or, from 64 bits on, no) signatures
+                s1 = (hb >= 64) ? 0ull : (s1 & ((1ull << hb) - 1ull));
                 s2 = 0;
             }
             k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);

@@ -27,7 +27,7 @@ namespace {
 __device__ __forceinline__ uint64_t masked_sig1(const RoundState* st, uint64_t s)
 {
     const uint32_t hb = st->hash_bits;
-    if (hb) s &= (hb >= 64) ? ~0ull : ((1ull << hb) - 1ull);
+    if (hb) s = (hb >= 64) ? 0ull : (s & ((1ull << hb) - 1ull));
     return s;
 }
 __device__ __forceinline__ uint32_t masked_sig2(const RoundState* st, uint32_t s) { return st->hash_bits ? 0u : s; }

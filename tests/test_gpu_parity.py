@@ -98,11 +98,12 @@ def test_random_vs_oracle(ctx, case, use_graph):
     assert r.initial_blocks == ex.round_blocks[0]
 
 
-@pytest.mark.parametrize("bits", [1, 3])
+@pytest.mark.parametrize("bits", [1, 3, -1])
 @pytest.mark.parametrize("relabel", [R.RELABEL_HASH, R.RELABEL_SORT], ids=["hash", "sort"])
 def test_forced_collisions_are_repaired(bits, relabel):
-    """Signatures truncated to `bits` bits collide all the time; the exact
-    check must split every wrong merge, so the partition is still exact."""
+    """Signatures truncated to `bits` bits collide all the time (bits = -1:
+    no signatures at all, the hashed rounds never split); the exact check
+    must split every wrong merge, so the partition is still exact."""
     with R.Context(0, test_hash_bits=bits, relabel=relabel) as c:
         for seed in range(3):
             off, idx = G.er_directed(150, 500, seed=seed)
@@ -111,6 +112,8 @@ def test_forced_collisions_are_repaired(bits, relabel):
             assert r.verified == 1
             assert np.array_equal(r.labels, ex.labels)
             assert r.blocks == ex.blocks
+            if bits < 0:
+                assert r.repairs > 0
         off, idx = G.random_lift(16, 48, 4, seed=1)
         wt = np.random.default_rng(1).integers(1, 3, size=len(idx)).astype(np.uint64)
         ex = oracle.refine_exact(off, idx, wt)
