@@ -204,6 +204,44 @@ rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_fa
 rbsc_status rbsc_gen_rmat_host(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
                                uint64_t seed, int32_t threads, rbsc_host_graph* out);
 
+/* ---- refinement without device allocation -------------------------------- */
+
+/* No counterpart in the reference (which allocates everything it uses,
+ * rbsc.cu:234-270).  For callers that cannot allocate device memory -- code
+ * running while another framework owns the device memory pool, real-time paths
+ * that must avoid the device synchronisation an allocation can cause, hosts
+ * that only hand out pointers into memory they manage themselves.
+ *
+ * Refines a small graph held in the caller's device memory in one kernel
+ * launch on `stream` (a cudaStream_t, or NULL for the default stream) of the
+ * current device.  Limits: N <= RBSC_NOALLOC_MAX_NODES, M <=
+ * RBSC_NOALLOC_MAX_ARCS; larger graphs are rejected with RBSC_ERR_TOO_LARGE.
+ * d_init_colors (may be NULL), d_out_labels (N uint32, canonical labels) and
+ * d_result are device pointers; d_result is written when the kernel ends
+ * (status RBSC_OK, RBSC_ERR_NOT_CONVERGED or RBSC_ERR_DEVICE).  opts may be
+ * NULL (defaults; relabel, verify and use_graph are ignored: the kernel always
+ * hashes and checks exactly).  The return value reports argument errors and
+ * launch failures only; synchronise the stream before reading d_result.
+ *
+ * Nothing is allocated: all scratch (about 5 MB) is one static device array of
+ * the library, held by every GPU that loads it until the process exits, and
+ * shared by all calls -- calls whose kernels overlap on the GPU race on it.
+ * The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress); make that first call before any stream capture. */
+#define RBSC_NOALLOC_MAX_NODES 16384u
+#define RBSC_NOALLOC_MAX_ARCS (1u << 24)
+
+typedef struct {
+    uint32_t blocks;
+    uint32_t rounds;
+    uint32_t repairs;
+    int32_t status;
+} rbsc_noalloc_result;
+
+rbsc_status rbsc_refine_noalloc(const rbsc_csr* device_graph, const uint32_t* d_init_colors,
+                                uint32_t* d_out_labels, rbsc_noalloc_result* d_result,
+                                const rbsc_opts* opts, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

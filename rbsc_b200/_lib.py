@@ -34,8 +34,11 @@ EXPORTED = [
     "rbsc_ctx_set_opts", "rbsc_refine", "rbsc_graph_upload", "rbsc_graph_from_device", "rbsc_graph_free",
     "rbsc_graph_info", "rbsc_graph_device_csr", "rbsc_graph_refine", "rbsc_graph_refine_device",
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
-    "rbsc_gen_rmat_host", "rbsc_graph_profile",
+    "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc",
 ]
+
+NOALLOC_MAX_NODES = 16384
+NOALLOC_MAX_ARCS = 1 << 24
 
 
 class Opts(ctypes.Structure):
@@ -99,6 +102,15 @@ class Csr(ctypes.Structure):
     ]
 
 
+class NoallocResult(ctypes.Structure):
+    _fields_ = [
+        ("blocks", ctypes.c_uint32),
+        ("rounds", ctypes.c_uint32),
+        ("repairs", ctypes.c_uint32),
+        ("status", ctypes.c_int32),
+    ]
+
+
 class HostGraph(ctypes.Structure):
     _fields_ = [
         ("n", ctypes.c_uint32),
@@ -140,6 +152,7 @@ def load():
     lib.rbsc_graph_refine_device.argtypes = [vp, vp, vp, vp, P(Stats)]
     lib.rbsc_graph_degree_colors.argtypes = [vp, vp, vp]
     lib.rbsc_graph_profile.argtypes = [vp, vp, vp, P(KernelTimes), P(Stats)]
+    lib.rbsc_refine_noalloc.argtypes = [P(Csr), vp, vp, vp, P(Opts), vp]
     lib.rbsc_parse_arcs.argtypes = [ctypes.c_char_p, ctypes.c_size_t, P(HostGraph)]
     lib.rbsc_host_graph_free.argtypes = [P(HostGraph)]
     lib.rbsc_gen_rmat_device.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
