@@ -70,7 +70,9 @@ typedef struct {
                                  the hashed rounds never split and every split comes
                                  from the exact check and repair).  Forces collisions so
                                  the exact check and repair path can be exercised.      */
-    int32_t reserved[7];
+    int32_t no_persist;       /* 1: never hand small active sets to the persistent
+                                 kernel (every pass stays one launch per phase)         */
+    int32_t reserved[6];
 } rbsc_opts;
 
 typedef struct {
@@ -110,6 +112,8 @@ typedef struct {
     float pass_ms[32][4];     /* per pass (first 32): signature, insert, relabel, other  */
     uint64_t pass_arcs[32];   /* arcs in the signature pass                              */
     uint32_t pass_nodes[32];  /* nodes in the relabel list                               */
+    double persist_ms;        /* the persistent kernel (small active sets), all its passes */
+    uint32_t persist_passes;
 } rbsc_kernel_times;
 
 /* A CSR graph.  `offsets` has n+1 entries of `offset_bytes` (4 or 8) bytes;

@@ -95,7 +95,8 @@ class Context:
     ``rbsc_opts`` of include/rbsc.h."""
 
     def __init__(self, device: int = 0, relabel: int = RELABEL_HASH, verify: bool = True, max_rounds: int = 0,
-                 use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0):
+                 use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0,
+                 persistent: bool = True):
         self._lib = _lib.load()
         o = _lib.Opts()
         self._lib.rbsc_opts_default(ctypes.byref(o))
@@ -105,6 +106,7 @@ class Context:
         o.use_graph = 1 if use_graph else 0
         o.seed = seed
         o.test_hash_bits = test_hash_bits
+        o.no_persist = 0 if persistent else 1
         self._opts = o
         h = self._lib.rbsc_ctx_create(device, ctypes.byref(o))
         if not h:
@@ -133,6 +135,8 @@ class Context:
         for k, v in kw.items():
             if k == "verify" or k == "use_graph":
                 v = 1 if v else 0
+            if k == "persistent":
+                k, v = "no_persist", 0 if v else 1
             setattr(self._opts, k, v)
         _check(self._lib, self._lib.rbsc_ctx_set_opts(self._h, ctypes.byref(self._opts)), self._h)
 

@@ -49,7 +49,8 @@ class Opts(ctypes.Structure):
         ("use_graph", ctypes.c_int32),
         ("seed", ctypes.c_uint64),
         ("test_hash_bits", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("no_persist", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 
@@ -88,6 +89,8 @@ class KernelTimes(ctypes.Structure):
         ("pass_ms", (ctypes.c_float * 4) * 32),
         ("pass_arcs", ctypes.c_uint64 * 32),
         ("pass_nodes", ctypes.c_uint32 * 32),
+        ("persist_ms", ctypes.c_double),
+        ("persist_passes", ctypes.c_uint32),
     ]
 
 

@@ -75,18 +75,21 @@ __global__ void k_rmat_keep(uint64_t m0, uint32_t scale, const unsigned long lon
     keep[i] = ((i == 0 || keys[i - 1] != k) && ((k >> scale) != (k & mask))) ? 1u : 0u;
 }
 
+// Writes the heads of the kept arcs and the CSR offsets, from the sorted keys:
+// the first kept arc of source u sits at pos[i] for the first i with src >= u,
+// so the thread of key i writes off[x] for every x in (src(i-1), src(i)].
 __global__ void k_rmat_emit(uint64_t m0, uint32_t scale, const unsigned long long* __restrict__ keys,
                             const uint32_t* __restrict__ keep, const uint32_t* __restrict__ pos, uint32_t* __restrict__ idx,
-                            unsigned long long* __restrict__ deg)
+                            uint64_t* __restrict__ off)
 {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m0) return;
-    const uint64_t k = keys[i];
+    if (i > m0) return;
     const uint64_t mask = (1ull << scale) - 1ull;
-    if ((i == 0 || keys[i - 1] != k) && ((k >> scale) != (k & mask))) {
-        idx[pos[i]] = (uint32_t)(k & mask);
-        atomicAdd(&deg[k >> scale], 1ull);
-    }
+    const uint64_t n = 1ull << scale;
+    const uint64_t u = i < m0 ? (keys[i] >> scale) : n;   // i == m0: sentinel past the last source
+    const int64_t prev = i == 0 ? -1 : (int64_t)(keys[i - 1] >> scale);
+    for (int64_t x = prev + 1; x <= (int64_t)u && x <= (int64_t)n; ++x) off[x] = pos[i];
+    if (i < m0 && keep[i]) idx[pos[i]] = (uint32_t)(keys[i] & mask);
 }
 
 }  // namespace
@@ -113,7 +116,7 @@ extern "C" rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint3
     if (m0 >= (1ull << 32)) return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "device R-MAT generator: edge_factor * 2^scale must be < 2^32");
     rbsc_status st = RBSC_OK;
     cudaStream_t s = ctx->stream;
-    unsigned long long *keys0 = nullptr, *keys1 = nullptr, *deg = nullptr;
+    unsigned long long *keys0 = nullptr, *keys1 = nullptr;
     uint32_t *keep = nullptr, *pos = nullptr;
     void* tmp = nullptr;
     rbsc_graph* g = nullptr;
@@ -144,13 +147,9 @@ extern "C" rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint3
     g->n = (uint32_t)n;
     g->m = mu;
     CKGS(graph_alloc_csr(ctx, g, false));
-    // degrees into d_off[0..n), then exclusive scan -> offsets
-    deg = (unsigned long long*)g->d_off;
-    CKG(cudaMemsetAsync(deg, 0, 8 * (n + 1), s));
     ++rbsc::launch_counter();
-    k_rmat_emit<<<(unsigned)ceil_div<uint64_t>(m0, 256), 256, 0, s>>>(m0, scale, sorted, keep, pos, g->d_idx, deg);
+    k_rmat_emit<<<(unsigned)ceil_div<uint64_t>(m0 + 1, 256), 256, 0, s>>>(m0, scale, sorted, keep, pos, g->d_idx, g->d_off);
     CKG(cudaGetLastError());
-    CKG((exclusive_scan<uint64_t, uint64_t>(g->d_off, g->d_off, n + 1, (uint64_t*)nullptr, tmp, s)));
     CKG(cudaStreamSynchronize(s));
     cudaFree(keys0); keys0 = nullptr;
     cudaFree(keys1); keys1 = nullptr;

@@ -43,6 +43,7 @@ struct rbsc_graph {
     uint32_t* d_sig2 = nullptr;
     uint32_t* d_slot = nullptr;
     uint32_t* d_out = nullptr;
+    void* d_rank = nullptr;          // first pass: dense class ranks (uint8 / uint16)
     uint32_t* d_init = nullptr;
     rbsc::Entry* d_tab = nullptr;
     uint32_t log2tab = 0;
@@ -55,6 +56,7 @@ struct rbsc_graph {
 
     // active set (what the passes still work on)
     rbsc::ActiveSet* d_as = nullptr;
+    rbsc::GridSync* d_gsync = nullptr;
     uint2* d_pairs = nullptr;        // (follower, representative)
     uint32_t* d_grep = nullptr;      // per initial label: smallest arc-less node
     uint32_t* d_gcnt = nullptr;      // per initial label: arc-less nodes
@@ -86,6 +88,7 @@ struct rbsc_graph {
     cudaGraph_t loop_graph = nullptr;
     cudaGraphExec_t loop_exec = nullptr;
     int loop_relabel = -1;
+    int loop_no_persist = -1;
     uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop
 };
 

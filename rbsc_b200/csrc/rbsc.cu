@@ -174,6 +174,7 @@ static void graph_release_refine(rbsc_graph* g)
     g->loop_graph = nullptr;
     dev_free((void*&)g->d_col[0]);
     dev_free((void*&)g->d_as);
+    dev_free((void*&)g->d_gsync);
     dev_free((void*&)g->d_pairs);
     dev_free((void*&)g->d_grep);
     dev_free((void*&)g->d_gcnt);
@@ -195,6 +196,7 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free((void*&)g->d_tab);
     dev_free((void*&)g->d_st);
     dev_free((void*&)g->d_out);
+    dev_free((void*&)g->d_rank);
     dev_free((void*&)g->d_init);
     dev_free((void*&)g->d_vflag);
     dev_free((void*&)g->d_vrow);
@@ -479,6 +481,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_sig2, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_slot, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_out, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_rank, 2 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_small, 256));
     g->log2tab = std::max<uint32_t>(10, log2_ceil(2ull * n));
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
@@ -486,6 +489,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CK(cudaMallocHost((void**)&g->h_st, sizeof(RoundState)));
     // active set: node lists, followers, group representatives, compacted arc sets
     CKS(dev_alloc(ctx, (void**)&g->d_as, sizeof(ActiveSet)));
+    CKS(dev_alloc(ctx, (void**)&g->d_gsync, sizeof(GridSync)));
     CKS(dev_alloc(ctx, (void**)&g->d_pairs, 8 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_grep, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_gcnt, 4 * n));
@@ -513,6 +517,11 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     return RBSC_OK;
 }
 
+// The persistent kernel takes over once both the active arcs and the listed
+// nodes are at most these.
+constexpr uint64_t kPersistArcs = 1ull << 22;
+constexpr uint32_t kPersistNodes = 1u << 22;
+
 static unsigned persistent_grid(rbsc_ctx* ctx, uint64_t work, unsigned per_block)
 {
     return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(work, per_block), (uint64_t)ctx->sm_count * 16));
@@ -524,8 +533,11 @@ struct PassTimer {
 };
 
 // Launches the kernels of one hashed pass on stream s (also used for capture).
+// First-pass gather variants (see k_signature / k_signature_uniform).
+enum FirstPass { kPassFull = 0, kPassUniform = 1, kPassRank8 = 2, kPassRank16 = 3 };
+
 static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle,
-                               PassTimer* t = nullptr)
+                               PassTimer* t = nullptr, int first = kPassFull, uint32_t c0 = 0)
 {
     const uint32_t n = g->n;
     const unsigned clear_grid = (unsigned)std::min<uint64_t>(ctx->sm_count * 8ull, grid_for(1ull << g->log2tab, 256));
@@ -538,10 +550,29 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (g->m > 0) {
         const unsigned blocks = persistent_grid(ctx, g->ntiles, kTileThreads / 32);
         ++rbsc::launch_counter();
-        if (g->weighted)
-            k_signature<true><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
-        else
-            k_signature<false><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
+        if (first == kPassUniform) {
+            const unsigned ugrid = persistent_grid(ctx, g->K, kNodeThreads);
+            if (g->weighted)
+                k_signature_uniform<true><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig1, g->d_sig2);
+            else
+                k_signature_uniform<false><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig1, g->d_sig2);
+        } else if (first == kPassRank8) {
+            const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
+            if (g->weighted)
+                k_signature<true, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+            else
+                k_signature<false, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+        } else if (first == kPassRank16) {
+            const uint16_t* cr = reinterpret_cast<const uint16_t*>(g->d_rank);
+            if (g->weighted)
+                k_signature<true, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+            else
+                k_signature<false, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+        } else if (g->weighted) {
+            k_signature<true, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
+        } else {
+            k_signature<false, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
+        }
     }
     if (t) CK(cudaEventRecord(t->ev[2], s));
     if (!hash) {
@@ -558,7 +589,7 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_pairs, g->d_col[0]);
     if (t) CK(cudaEventRecord(t->ev[4], s));
     ++rbsc::launch_counter();
-    k_fixpoint<kFixHash><<<1, 1, 0, s>>>(g->d_st, g->d_as, hash ? 1 : 0, h, use_handle);
+    k_fixpoint<kFixHash><<<1, 1, 0, s>>>(g->d_st, g->d_as, hash ? 1 : 0);
     // compaction for the next pass
     ++rbsc::launch_counter();
     k_compact_nodes<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb);
@@ -573,7 +604,8 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig1, g->d_sig2);
     }
     ++rbsc::launch_counter();
-    k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb);
+    const bool persist = hash && !ctx->opts.no_persist;
+    k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb, persist ? kPersistArcs : 0ull, kPersistNodes, h, use_handle);
     if (t) CK(cudaEventRecord(t->ev[5], s));
     CK(cudaGetLastError());
     return RBSC_OK;
@@ -581,7 +613,7 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
 
 static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
 {
-    if (g->loop_exec && g->loop_relabel == ctx->opts.relabel) return RBSC_OK;
+    if (g->loop_exec && g->loop_relabel == ctx->opts.relabel && g->loop_no_persist == ctx->opts.no_persist) return RBSC_OK;
     if (g->loop_exec) cudaGraphExecDestroy(g->loop_exec);
     if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
     g->loop_exec = nullptr;
@@ -616,6 +648,7 @@ static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
     if (e != cudaSuccess) return rbsc_cuda_fail(ctx, e, "cudaStreamEndCapture", __LINE__);
     CK(cudaGraphInstantiate(&g->loop_exec, g->loop_graph, 0));
     g->loop_relabel = ctx->opts.relabel;
+    g->loop_no_persist = ctx->opts.no_persist;
     return RBSC_OK;
 }
 
@@ -626,7 +659,99 @@ static rbsc_status read_state(rbsc_ctx* ctx, rbsc_graph* g)
     return RBSC_OK;
 }
 
-static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels)
+static rbsc_status run_passes(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels);
+static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt);
+
+static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels,
+                            int first = kPassFull, uint32_t c0 = 0)
+{
+    bool handoff = false;
+    if (first != kPassFull) {
+        // the first pass with its narrow gather, launched from the host; the
+        // remaining passes below
+        PassTimer t;
+        if (kt)
+            for (auto& e : t.ev) CK(cudaEventCreate(&e));
+        ActiveSet before;
+        if (kt) {
+            CK(cudaMemcpyAsync(&before, g->d_as, sizeof before, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+        }
+        CKS(ensure_sort_relabel_bufs(ctx, g));
+        rbsc_status st = launch_pass(ctx, g, ctx->stream, cudaGraphConditionalHandle(), 0, kt ? &t : nullptr, first, c0);
+        if (st == RBSC_OK) st = read_state(ctx, g);
+        if (st == RBSC_OK && kt) {
+            float ms[5];
+            for (int i = 0; i < 5; ++i) cudaEventElapsedTime(&ms[i], t.ev[i], t.ev[i + 1]);
+            float* pm = kt->pass_ms[0];
+            pm[0] = ms[1];
+            pm[1] = ms[2];
+            pm[2] = ms[3];
+            pm[3] = ms[0] + ms[4];
+            kt->pass_arcs[0] = first == kPassUniform ? 0 : before.m;
+            kt->pass_nodes[0] = before.nnodes;
+            kt->passes = 1;
+            kt->other_ms += ms[0] + ms[4];
+            kt->signature_ms += ms[1];
+            kt->insert_ms += ms[2];
+            kt->relabel_ms += ms[3];
+        }
+        if (kt)
+            for (auto& e : t.ev) cudaEventDestroy(e);
+        if (st != RBSC_OK) return st;
+        if (g->h_st->done || g->h_st->error) return RBSC_OK;
+        handoff = g->h_st->handoff != 0;
+    }
+    if (!handoff) {
+        CKS(run_passes(ctx, g, kt, graph_kernels));
+        handoff = g->h_st->handoff != 0;
+    }
+    if (handoff && !g->h_st->done && !g->h_st->error) CKS(run_persistent(ctx, g, kt));
+    return RBSC_OK;
+}
+
+// The small-set tail of the refinement: one cooperative launch of
+// k_refine_persistent (all blocks resident, bounded grid barriers).
+static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt)
+{
+    cudaStream_t s = ctx->stream;
+    int bps = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_refine_persistent, kNodeThreads, 0));
+    const unsigned grid = (unsigned)std::max(1, bps) * (unsigned)ctx->sm_count;
+    CK(cudaMemsetAsync(g->d_gsync, 0, sizeof(GridSync), s));
+    PersistArgs a;
+    a.as = g->d_as;
+    a.st = g->d_st;
+    a.col = g->d_col[0];
+    a.sig1 = g->d_sig1;
+    a.sig2 = g->d_sig2;
+    a.tab = g->d_tab;
+    a.log2tab = g->log2tab;
+    a.tab_entries = 1ull << g->log2tab;
+    a.slot = g->d_slot;
+    a.pairs = g->d_pairs;
+    a.gs = g->d_gsync;
+    a.weighted = g->weighted ? 1 : 0;
+    void* args[] = {&a};
+    const uint32_t r0 = g->h_st->round;
+    if (kt) CK(cudaEventRecord(ctx->ev[2], s));
+    ++rbsc::launch_counter();
+    CK(cudaLaunchCooperativeKernel((const void*)k_refine_persistent, dim3(grid), dim3(kNodeThreads), args, 0, s));
+    if (kt) CK(cudaEventRecord(ctx->ev[3], s));
+    CKS(read_state(ctx, g));
+    if (kt) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, ctx->ev[2], ctx->ev[3]);
+        kt->persist_ms += ms;
+        kt->persist_passes += g->h_st->round - r0;
+    }
+    if (g->h_st->error & kErrBarrier) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "persistent kernel: a grid barrier timed out");
+    return RBSC_OK;
+}
+
+// Passes with the active set still large: the CUDA-graph loop (or the
+// host-driven loop), until the fixpoint, an error or the hand-off.
+static rbsc_status run_passes(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels)
 {
     if (ctx->opts.use_graph && !kt) {
         CKS(build_loop_graph(ctx, g));
@@ -665,7 +790,7 @@ static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt,
                 kt->insert_ms += ms[2];
                 kt->relabel_ms += ms[3];
             }
-            if (st != RBSC_OK || g->h_st->done || g->h_st->error) {
+            if (st != RBSC_OK || g->h_st->done || g->h_st->error || g->h_st->handoff) {
                 if (kt)
                     for (auto& e : t.ev) cudaEventDestroy(e);
                 if (st != RBSC_OK) return st;
@@ -831,7 +956,7 @@ static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
     ++rbsc::launch_counter();
     k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
     ++rbsc::launch_counter();
-    k_fixpoint<kFixRepair><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0, cudaGraphConditionalHandle(), 0);
+    k_fixpoint<kFixRepair><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0);
     CK(cudaGetLastError());
     // every row signature is recomputed from scratch on the whole graph
     CK(cudaMemsetAsync(g->d_sig1, 0, 8 * (size_t)n, s));
@@ -870,7 +995,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         ++rbsc::launch_counter();
         k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
         ++rbsc::launch_counter();
-        k_fixpoint<kFixInit><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0, cudaGraphConditionalHandle(), 0);
+        k_fixpoint<kFixInit><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0);
         CK(cudaGetLastError());
     } else {
         hs.prev = 1;
@@ -905,12 +1030,37 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     float init_ms = 0.f;
     cudaEventElapsedTime(&init_ms, ctx->ev[0], ctx->ev[4]);
 
+    // first pass: few initial classes -> gather their dense ranks (1 or 2
+    // bytes per node); one class -> no gather at all
+    int first = kPassFull;
+    uint32_t c0 = 0;
+    if (g->m > 0 && ctx->opts.relabel != RBSC_RELABEL_SORT) {
+        if (initial_blocks == 1) {
+            first = kPassUniform;
+            CK(cudaMemcpyAsync(&c0, g->d_col[0], 4, cudaMemcpyDeviceToHost, s));
+            CK(cudaStreamSynchronize(s));
+        } else if (initial_blocks <= 65536) {
+            first = initial_blocks <= 256 ? kPassRank8 : kPassRank16;
+            CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)n + 1) + 1024));
+            ++rbsc::launch_counter();
+            k_class_heads<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_slot);
+            CK((exclusive_scan<uint32_t, uint32_t>(g->d_slot, g->d_slot, n, (uint32_t*)nullptr, g->d_tmp, s)));
+            ++rbsc::launch_counter();
+            if (first == kPassRank8)
+                k_class_ranks<uint8_t><<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_slot, (uint8_t*)g->d_rank);
+            else
+                k_class_ranks<uint16_t><<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_slot, (uint16_t*)g->d_rank);
+            CK(cudaGetLastError());
+        }
+    }
+
     float verify_ms = 0.f, loop_ms = 0.f;
     uint32_t repairs = 0;
     for (;;) {
         if (hs.error) break;
         CK(cudaEventRecord(ctx->ev[4], s));
-        CKS(run_loop(ctx, g, kt, &graph_kernels));
+        CKS(run_loop(ctx, g, kt, &graph_kernels, first, c0));
+        first = kPassFull;
         CK(cudaEventRecord(ctx->ev[5], s));
         CK(cudaEventSynchronize(ctx->ev[5]));
         {

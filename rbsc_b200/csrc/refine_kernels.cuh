@@ -42,12 +42,15 @@ struct RoundState {
     uint32_t stamp;          // relabel-table stamp of the running pass, 1..255
     uint32_t clear_pending;  // table must be cleared before the running pass
     uint32_t hash_bits;      // test hook: signatures truncated to this many bits (0 = off)
+    uint32_t handoff;        // the active set is small: the persistent kernel takes over
+    uint32_t pad;
     uint64_t seed;
     uint32_t round_blocks[kRoundLog];
 };
 
 constexpr uint32_t kErrProbe = 1u;   // relabel table full (cannot happen at load <= 1/2)
 constexpr uint32_t kErrRounds = 2u;  // max_rounds reached
+constexpr uint32_t kErrBarrier = 4u; // a grid barrier of the persistent kernel timed out
 
 // What the pass kernels work on; the compaction kernels shrink it.
 struct ActiveSet {
@@ -204,12 +207,25 @@ __device__ __forceinline__ void arc_terms(uint32_t c, uint64_t salt, uint64_t& t
 // are modulo 2^64 / 2^32, so the split into partial sums does not change the
 // result.  Warps are independent: no shared memory, no block barrier.
 // ---------------------------------------------------------------------------
-template <bool WEIGHTED>
-static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveSet* __restrict__ as,
-                                                                   const RoundState* __restrict__ st,
-                                                                   const uint32_t* __restrict__ col,
-                                                                   unsigned long long* __restrict__ sig1,
-                                                                   uint32_t* __restrict__ sig2)
+// ColT: the gathered colour.  uint32_t = the colour word (label); the first
+// pass may instead gather the dense rank of the initial class as uint8_t /
+// uint16_t when there are few initial classes (a narrower array, mostly L1/L2
+// resident).  Any injective relabelling of the colours gives the same
+// partition.
+// Colour gathers go through the read-only path (ld.global.nc) in the pass
+// kernels, where the colours do not change during the launch; the persistent
+// kernel rewrites them between its phases, so it reads them at L2 (NC false).
+template <bool NC, typename ColT>
+__device__ __forceinline__ uint32_t gather_col(const ColT* p)
+{
+    if constexpr (NC) return (uint32_t)__ldg(p);
+    else return (uint32_t)__ldcg(p);
+}
+
+template <bool WEIGHTED, typename ColT, bool NC = true>
+__device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
+                                               const ColT* __restrict__ col, unsigned long long* __restrict__ sig1,
+                                               uint32_t* __restrict__ sig2)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t ntiles = as->ntiles;
@@ -234,18 +250,23 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveS
         uint32_t hb = 0;
         uint32_t c[kEdgesPerThread];
         uint64_t w[kEdgesPerThread];
+        static_assert(sizeof(ColT) <= 4, "colour type");
         if (cnt == kEdgesPerThread) {
             hb = *reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3));
             const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
             const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1), q2 = __ldcs(p + 2), q3 = __ldcs(p + 3);
-            c[0] = __ldg(col + q0.x); c[1] = __ldg(col + q0.y); c[2] = __ldg(col + q0.z); c[3] = __ldg(col + q0.w);
-            c[4] = __ldg(col + q1.x); c[5] = __ldg(col + q1.y); c[6] = __ldg(col + q1.z); c[7] = __ldg(col + q1.w);
-            c[8] = __ldg(col + q2.x); c[9] = __ldg(col + q2.y); c[10] = __ldg(col + q2.z); c[11] = __ldg(col + q2.w);
-            c[12] = __ldg(col + q3.x); c[13] = __ldg(col + q3.y); c[14] = __ldg(col + q3.z); c[15] = __ldg(col + q3.w);
+            c[0] = gather_col<NC>(col + q0.x); c[1] = gather_col<NC>(col + q0.y);
+            c[2] = gather_col<NC>(col + q0.z); c[3] = gather_col<NC>(col + q0.w);
+            c[4] = gather_col<NC>(col + q1.x); c[5] = gather_col<NC>(col + q1.y);
+            c[6] = gather_col<NC>(col + q1.z); c[7] = gather_col<NC>(col + q1.w);
+            c[8] = gather_col<NC>(col + q2.x); c[9] = gather_col<NC>(col + q2.y);
+            c[10] = gather_col<NC>(col + q2.z); c[11] = gather_col<NC>(col + q2.w);
+            c[12] = gather_col<NC>(col + q3.x); c[13] = gather_col<NC>(col + q3.y);
+            c[14] = gather_col<NC>(col + q3.z); c[15] = gather_col<NC>(col + q3.w);
         } else {
             if (cnt) hb = (uint32_t)(*reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3))) & ((1u << cnt) - 1u);
 #pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? __ldg(col + __ldcs(idx + tbeg + a + i)) : 0u;
+            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? gather_col<NC>(col + __ldcs(idx + tbeg + a + i)) : 0u;
         }
         if (WEIGHTED) {
 #pragma unroll
@@ -354,6 +375,66 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveS
     }
 }
 
+template <bool WEIGHTED, typename ColT>
+static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveSet* __restrict__ as,
+                                                                   const RoundState* __restrict__ st,
+                                                                   const ColT* __restrict__ col,
+                                                                   unsigned long long* __restrict__ sig1,
+                                                                   uint32_t* __restrict__ sig2)
+{
+    signature_body<WEIGHTED, ColT>(as, st, col, sig1, sig2);
+}
+
+// First pass when every node starts in one block (the reference's default):
+// every arc's term is the same, so a row's signature is its length (or its
+// total weight) times that term, and no arc needs to be read.
+template <bool WEIGHTED>
+static __global__ void __launch_bounds__(kNodeThreads) k_signature_uniform(const ActiveSet* __restrict__ as,
+                                                                           const RoundState* __restrict__ st,
+                                                                           const uint64_t* __restrict__ off,
+                                                                           const uint64_t* __restrict__ wt, uint32_t c0,
+                                                                           unsigned long long* __restrict__ sig1,
+                                                                           uint32_t* __restrict__ sig2)
+{
+    const uint32_t K = as->K;
+    const uint32_t* __restrict__ rows = as->rows;
+    uint64_t t1;
+    uint32_t t2;
+    arc_terms(c0, pass_salt1(st->seed, st->round), t1, t2);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) {
+        const uint32_t u = rows[k];
+        const uint64_t b = off[u], e = off[u + 1];
+        uint64_t w = e - b;
+        uint32_t w2 = (uint32_t)w;
+        if (WEIGHTED) {
+            w = 0;
+            w2 = 0;
+            for (uint64_t j = b; j < e; ++j) {
+                w += wt[j];
+                w2 += (uint32_t)wt[j];
+            }
+        }
+        sig1[u] = w * t1;
+        sig2[u] = w2 * t2;
+    }
+}
+
+// Dense ranks of the classes (labels in increasing order): flag[u] = u is the
+// smallest node of its class.
+static __global__ void k_class_heads(uint32_t n, const uint32_t* __restrict__ col, uint32_t* __restrict__ flag)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < n) flag[u] = (col[u] & kLabelMask) == u ? 1u : 0u;
+}
+
+template <typename ColT>
+static __global__ void k_class_ranks(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ rank,
+                                     ColT* __restrict__ out)
+{
+    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
+    if (u < n) out[u] = (ColT)rank[col[u] & kLabelMask];
+}
+
 // Row-head bitmap: bit (e % 8) of byte e / 8 is set iff arc e is the first
 // arc of its row.
 template <typename OffT>
@@ -408,15 +489,14 @@ __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
     if ((threadIdx.x & 31) == 0 && nb) atomicAdd(counter, (uint32_t)__popc(nb));
 }
 
-// Hashed pass over the node list (persistent, grid-stride by blocks).
-static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
-                                                                     const uint32_t* __restrict__ col,
-                                                                     const unsigned long long* __restrict__ sig1,
-                                                                     const uint32_t* __restrict__ sig2,
-                                                                     Entry* __restrict__ tab, uint32_t log2size,
-                                                                     uint32_t* __restrict__ slot)
+// Hashed pass over the node list (grid-stride by blocks); returns this
+// thread's count of new blocks.
+__device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
+                                                     const uint32_t* __restrict__ col,
+                                                     const unsigned long long* __restrict__ sig1,
+                                                     const uint32_t* __restrict__ sig2, Entry* __restrict__ tab,
+                                                     uint32_t log2size, uint32_t* __restrict__ slot)
 {
-    __shared__ BlockReserveSmem<kNodeThreads> sm;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
     const uint32_t stamp = st->stamp;
@@ -451,6 +531,18 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
         insert_warp(need, u, i, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
         made += nb ? 1u : 0u;
     }
+    return made;
+}
+
+static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
+                                                                     const uint32_t* __restrict__ col,
+                                                                     const unsigned long long* __restrict__ sig1,
+                                                                     const uint32_t* __restrict__ sig2,
+                                                                     Entry* __restrict__ tab, uint32_t log2size,
+                                                                     uint32_t* __restrict__ slot)
+{
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
+    const uint32_t made = insert_list_body(as, st, col, sig1, sig2, tab, log2size, slot);
     block_count<kNodeThreads>(made, &st->count, sm);
 }
 
@@ -486,11 +578,9 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 // position); also zeroes the signatures of the rows that cross a tile edge
 // (the next pass adds into them atomically).  Four list entries per thread
 // and iteration, so their dependent loads overlap.
-static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
-                                                                      const Entry* __restrict__ tab,
-                                                                      const uint32_t* __restrict__ slot,
-                                                                      unsigned long long* __restrict__ sig1,
-                                                                      uint32_t* __restrict__ sig2)
+__device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
+                                                  const Entry* __restrict__ tab, const uint32_t* __restrict__ slot,
+                                                  unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
@@ -519,6 +609,15 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const Acti
     }
 }
 
+static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
+                                                                      const Entry* __restrict__ tab,
+                                                                      const uint32_t* __restrict__ slot,
+                                                                      unsigned long long* __restrict__ sig1,
+                                                                      uint32_t* __restrict__ sig2)
+{
+    relabel_list_body(as, col, tab, slot, sig1, sig2);
+}
+
 // New colours of all nodes (after k_insert_all), in place.
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n, uint32_t* __restrict__ col,
                                                                      const Entry* __restrict__ tab,
@@ -533,8 +632,8 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n,
 
 // Followers (arc-less nodes that are not their group's representative) take
 // the representative's colour.  pairs[i] = (follower, representative).
-static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
-                                                                uint32_t* __restrict__ col)
+__device__ __forceinline__ void follow_body(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
+                                            uint32_t* __restrict__ col)
 {
     const uint32_t nf = as->nfollow;
     const uint32_t stride = gridDim.x * kNodeThreads;
@@ -542,6 +641,12 @@ static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet*
         const uint2 p = pairs[i];
         col[p.x] = col[p.y];
     }
+}
+
+static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
+                                                                uint32_t* __restrict__ col)
+{
+    follow_body(as, pairs, col);
 }
 
 // k_fixpoint: one thread.  Closes the running pass and decides whether the
@@ -553,8 +658,7 @@ constexpr int kFixHash = 0;
 constexpr int kFixInit = 1;
 constexpr int kFixRepair = 2;
 template <int MODE>
-static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_retired, cudaGraphConditionalHandle handle,
-                                  int use_handle)
+__device__ __forceinline__ void fixpoint_body(RoundState* st, const ActiveSet* as, int add_retired)
 {
     uint32_t cnt = st->count;
     st->count = 0;
@@ -567,16 +671,22 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
     } else if (MODE == kFixInit) {
         st->round_blocks[0] = cnt;
         st->done = 0u;
+        st->handoff = 0u;
     } else {
         st->done = 0u;
+        st->handoff = 0u;
     }
     st->prev = cnt;
     const uint32_t stamp = st->stamp % 255u + 1u;
     st->stamp = stamp;
     st->clear_pending = stamp == 1u;
     if (!st->done && st->round >= st->max_rounds) st->error |= kErrRounds;
-    const bool more = !st->done && !st->error;
-    if (use_handle) cudaGraphSetConditional(handle, more ? 1u : 0u);
+}
+
+template <int MODE>
+static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_retired)
+{
+    fixpoint_body<MODE>(st, as, add_retired);
 }
 
 // ---------------------------------------------------------------------------
@@ -751,10 +861,17 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
     }
 }
 
-// Switches the pass kernels to the compacted node list / arc set.
-static __global__ void k_compact_finalize(ActiveSet* as, const RoundState* st, CompactBufs bufs)
+// Switches the pass kernels to the compacted node list / arc set, and
+// decides whether the device-side while loop runs another pass: not when the
+// fixpoint is reached, an error was raised, or (handoff_arcs > 0) the active
+// set became small enough for the persistent kernel, which then takes over.
+static __global__ void k_compact_finalize(ActiveSet* as, RoundState* st, CompactBufs bufs, uint64_t handoff_arcs,
+                                          uint32_t handoff_nodes, cudaGraphConditionalHandle handle, int use_handle)
 {
-    if (st->done || st->error) return;
+    if (st->done || st->error) {
+        if (use_handle) cudaGraphSetConditional(handle, 0u);
+        return;
+    }
     const uint32_t dn = as->dst_nodes;
     as->nodes = bufs.nodes[dn];
     as->nnodes = as->nodectr;
@@ -779,6 +896,9 @@ static __global__ void k_compact_finalize(ActiveSet* as, const RoundState* st, C
     }
     as->rowctr = 0;
     as->splitctr = 0;
+    const bool small = handoff_arcs > 0 && as->m <= handoff_arcs && as->nnodes <= handoff_nodes;
+    st->handoff = small ? 1u : 0u;
+    if (use_handle) cudaGraphSetConditional(handle, small ? 0u : 1u);
 }
 
 // ---------------------------------------------------------------------------
@@ -881,13 +1001,98 @@ static __global__ void k_zero_rows(const uint32_t* __restrict__ list, uint32_t c
     }
 }
 
-// k_clear_table: clears the table when the stamp wrapped.
-static __global__ void k_clear_table(const RoundState* __restrict__ st, Entry* __restrict__ tab, uint64_t entries)
+// Clears the table when the stamp wrapped.
+__device__ __forceinline__ void clear_table_body(const RoundState* __restrict__ st, Entry* __restrict__ tab, uint64_t entries)
 {
     if (!st->clear_pending) return;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < entries; i += (uint64_t)gridDim.x * blockDim.x) {
         tab[i].k1 = 0ull;
         tab[i].hi = 0ull;
+    }
+}
+
+static __global__ void k_clear_table(const RoundState* __restrict__ st, Entry* __restrict__ tab, uint64_t entries)
+{
+    clear_table_body(st, tab, entries);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent pass kernel: once the active set is small, one cooperative
+// launch runs the remaining passes (the same phases as the kernels above,
+// separated by grid barriers) instead of a dozen small launches per pass.
+// The barrier is a counter + generation word; every wait is bounded: after
+// kBarrierSpin polls the kernel raises kErrBarrier and every block returns.
+// ---------------------------------------------------------------------------
+struct GridSync {
+    unsigned count;
+    unsigned gen;
+};
+
+constexpr uint32_t kBarrierSpin = 1u << 24;  // polls of ~64 ns: more than a second
+
+__device__ __forceinline__ bool grid_barrier(GridSync* gs, RoundState* st)
+{
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile unsigned* vgen = &gs->gen;
+        volatile uint32_t* verr = &st->error;
+        const unsigned g = *vgen;
+        __threadfence();
+        if (atomicAdd(&gs->count, 1u) == gridDim.x - 1u) {
+            gs->count = 0;  // nobody else touches the counter until the generation moves
+            __threadfence();
+            atomicAdd(&gs->gen, 1u);
+        } else {
+            uint32_t it = 0;
+            while (*vgen == g) {
+                if (++it > kBarrierSpin || (*verr & kErrBarrier)) {
+                    atomicOr(&st->error, kErrBarrier);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return !(*(volatile uint32_t*)&st->error & kErrBarrier);
+}
+
+struct PersistArgs {
+    ActiveSet* as;
+    RoundState* st;
+    uint32_t* col;
+    unsigned long long* sig1;
+    uint32_t* sig2;
+    Entry* tab;
+    uint32_t log2tab;
+    uint64_t tab_entries;
+    uint32_t* slot;
+    const uint2* pairs;
+    GridSync* gs;
+    int weighted;
+};
+
+static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
+{
+    static_assert(kNodeThreads == kTileThreads, "the signature phase runs one tile per warp");
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
+    for (;;) {
+        clear_table_body(a.st, a.tab, a.tab_entries);
+        if (!grid_barrier(a.gs, a.st)) return;
+        if (a.weighted) signature_body<true, uint32_t, false>(a.as, a.st, a.col, a.sig1, a.sig2);
+        else signature_body<false, uint32_t, false>(a.as, a.st, a.col, a.sig1, a.sig2);
+        if (!grid_barrier(a.gs, a.st)) return;
+        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig1, a.sig2, a.tab, a.log2tab, a.slot);
+        block_count<kNodeThreads>(made, &a.st->count, sm);
+        if (!grid_barrier(a.gs, a.st)) return;
+        relabel_list_body(a.as, a.col, a.tab, a.slot, a.sig1, a.sig2);
+        if (!grid_barrier(a.gs, a.st)) return;
+        follow_body(a.as, a.pairs, a.col);
+        if (!grid_barrier(a.gs, a.st)) return;
+        if (blockIdx.x == 0 && threadIdx.x == 0) fixpoint_body<kFixHash>(a.st, a.as, 1);
+        if (!grid_barrier(a.gs, a.st)) return;
+        if (*(volatile uint32_t*)&a.st->done || *(volatile uint32_t*)&a.st->error) return;
     }
 }
 

@@ -85,15 +85,19 @@ def _random_cases():
 
 
 @pytest.mark.parametrize("case", list(_random_cases()), ids=lambda c: c[0])
-@pytest.mark.parametrize("use_graph", [True, False], ids=["graph", "hostloop"])
-def test_random_vs_oracle(ctx, case, use_graph):
+@pytest.mark.parametrize("use_graph,persistent", [(True, True), (False, True), (True, False)],
+                         ids=["graph", "hostloop", "graph_nopersist"])
+def test_random_vs_oracle(ctx, case, use_graph, persistent):
+    """persistent: small active sets go to the persistent kernel (the default,
+    which every graph here reaches after its first pass); off: every pass is
+    a sequence of launches."""
     _, off, idx, wt, init = case
     ex = oracle.refine_exact(off, idx, wt, init)
-    ctx.set_opts(use_graph=use_graph)
+    ctx.set_opts(use_graph=use_graph, persistent=persistent)
     try:
         r = ctx.refine(off, idx, wt, init)
     finally:
-        ctx.set_opts(use_graph=True)
+        ctx.set_opts(use_graph=True, persistent=True)
     _check_against(r, ex.labels, ex.blocks, ex.rounds)
     assert r.initial_blocks == ex.round_blocks[0]
 
@@ -150,11 +154,17 @@ def test_invalid_graphs_rejected(ctx):
         ctx.refine(np.array([0, 2, 1], dtype=np.uint64), np.array([0, 1], dtype=np.uint32))
 
 
-def test_long_path_wraps_table_stamp(ctx):
-    """A 700-node path needs 700 passes; the 8-bit table stamp wraps twice."""
+@pytest.mark.parametrize("persistent", [True, False], ids=["persist", "nopersist"])
+def test_long_path_wraps_table_stamp(ctx, persistent):
+    """A 700-node path needs 700 passes; the 8-bit table stamp wraps twice
+    (inside the persistent kernel, or across launched passes)."""
     off, idx = G.path(700)
     ex = oracle.refine_exact(off, idx)
-    r = ctx.refine(off, idx)
+    ctx.set_opts(persistent=persistent)
+    try:
+        r = ctx.refine(off, idx)
+    finally:
+        ctx.set_opts(persistent=True)
     _check_against(r, ex.labels, ex.blocks, ex.rounds)
     assert r.rounds == 700
 
@@ -252,7 +262,16 @@ def test_large_rmat_properties():
         c.set_opts(relabel=R.RELABEL_SORT)
         b = g.refine(init)
         assert np.array_equal(a.labels, b.labels) and a.rounds == b.rounds
-        c.set_opts(relabel=R.RELABEL_HASH)
+        c.set_opts(relabel=R.RELABEL_HASH, persistent=False)
+        p = g.refine(init)
+        assert np.array_equal(a.labels, p.labels) and a.rounds == p.rounds
+        c.set_opts(persistent=True)
+        import torch
+        d_init = torch.from_numpy(init.astype(np.int32)).cuda()
+        times, q = g.profile(d_init.data_ptr())
+        assert q.blocks == a.blocks and q.rounds == a.rounds
+        assert times["persist_passes"] >= 1
+        assert times["passes"] + times["persist_passes"] == a.rounds
         z = g.refine(a.labels)
         assert np.array_equal(z.labels, a.labels) and z.rounds == 1
         # every block refines the degree classes
