@@ -108,6 +108,67 @@ __device__ __forceinline__ void block_count(uint32_t v, uint32_t* counter, Block
     __syncthreads();
 }
 
+// Buffered append to a global list: the flagged values of each block
+// iteration go to a shared-memory buffer, and the block reserves space in the
+// global list (one atomicAdd on the shared counter) only when the buffer is
+// full and at the end.  A counter that every block of a large grid hits once
+// per iteration serialises in L2 (one atomic after another on one address);
+// this makes it one per CAP values.  All calls are block-collective.
+template <typename T, int CAP, int BLOCK> struct BlockAppend {
+    static_assert(CAP >= BLOCK, "a block iteration must fit in an empty buffer");
+    T buf[CAP];
+    uint32_t warp_cnt[BLOCK / 32];
+    uint32_t count;
+    uint32_t base;
+};
+
+template <typename T, int CAP, int BLOCK>
+__device__ __forceinline__ void block_append_begin(BlockAppend<T, CAP, BLOCK>& s)
+{
+    if (threadIdx.x == 0) s.count = 0;
+    __syncthreads();
+}
+
+// Writes the buffered values out (block-collective).
+template <typename T, int CAP, int BLOCK>
+__device__ __forceinline__ void block_append_flush(BlockAppend<T, CAP, BLOCK>& s, uint32_t* counter, T* out)
+{
+    __syncthreads();
+    const uint32_t cnt = s.count;
+    if (cnt == 0) return;
+    if (threadIdx.x == 0) s.base = atomicAdd(counter, cnt);
+    __syncthreads();
+    const uint32_t base = s.base;
+    for (uint32_t i = threadIdx.x; i < cnt; i += BLOCK) out[base + i] = s.buf[i];
+    __syncthreads();
+    if (threadIdx.x == 0) s.count = 0;
+    __syncthreads();
+}
+
+template <typename T, int CAP, int BLOCK>
+__device__ __forceinline__ void block_append(BlockAppend<T, CAP, BLOCK>& s, bool take, const T& v, uint32_t* counter, T* out)
+{
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (lane == 0) s.warp_cnt[warp] = (uint32_t)__popc(m);
+    __syncthreads();
+    uint32_t before = 0, total = 0;
+#pragma unroll
+    for (int w = 0; w < BLOCK / 32; ++w) {
+        const uint32_t c = s.warp_cnt[w];
+        before += (w < (int)warp) ? c : 0u;
+        total += c;
+    }
+    uint32_t cnt = s.count;
+    if (cnt + total > (uint32_t)CAP) {  // block-uniform
+        block_append_flush(s, counter, out);
+        cnt = 0;
+    }
+    if (take) s.buf[cnt + before + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) s.count = cnt + total;
+}
+
 // Kernels enqueued by the calling host thread (reported in rbsc_stats).
 inline uint64_t& launch_counter()
 {

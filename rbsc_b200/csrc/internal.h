@@ -39,8 +39,7 @@ struct rbsc_graph {
     bool bufs = false;
     uint32_t* d_col[1] = {nullptr};  // colours, updated in place
     uint32_t* d_initlab = nullptr;
-    unsigned long long* d_sig1 = nullptr;
-    uint32_t* d_sig2 = nullptr;
+    rbsc::Sig* d_sig = nullptr;  // per-node signature (16 B)
     uint32_t* d_slot = nullptr;
     uint32_t* d_out = nullptr;
     void* d_rank = nullptr;          // first pass: dense class ranks (uint8 / uint16)
@@ -57,6 +56,7 @@ struct rbsc_graph {
     // active set (what the passes still work on)
     rbsc::ActiveSet* d_as = nullptr;
     rbsc::GridSync* d_gsync = nullptr;
+    rbsc::ActiveSet* h_as = nullptr;  // pinned staging of the initial active set
     uint2* d_pairs = nullptr;        // (follower, representative)
     uint32_t* d_grep = nullptr;      // per initial label: smallest arc-less node
     uint32_t* d_gcnt = nullptr;      // per initial label: arc-less nodes

@@ -107,7 +107,7 @@ __device__ uint32_t na_table_pass(int mode, uint32_t n, uint32_t* col, const uin
     __syncthreads();
     for (uint32_t u = threadIdx.x; u < n; u += kNaThreads) {
         const uint32_t c = mode == 1 ? 0u : col[u];
-        if (!(c & kSingleton)) col[u] = relabel_one(c, tab, slot[u]);
+        if (!(c & kSingleton)) col[u] = relabel_one<false>(c, tab, slot[u]);
     }
     __syncthreads();
     return *(volatile uint32_t*)s_count;

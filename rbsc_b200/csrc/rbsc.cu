@@ -190,8 +190,7 @@ static void graph_release_refine(rbsc_graph* g)
         dev_free((void*&)g->cb.nodes[d]);
     }
     dev_free((void*&)g->d_initlab);
-    dev_free((void*&)g->d_sig1);
-    dev_free((void*&)g->d_sig2);
+    dev_free((void*&)g->d_sig);
     dev_free((void*&)g->d_slot);
     dev_free((void*&)g->d_tab);
     dev_free((void*&)g->d_st);
@@ -215,6 +214,8 @@ static void graph_release_refine(rbsc_graph* g)
     g->key_cap = 0;
     if (g->h_st) cudaFreeHost(g->h_st);
     g->h_st = nullptr;
+    if (g->h_as) cudaFreeHost(g->h_as);
+    g->h_as = nullptr;
     g->bufs = false;
     sortrelabel_release(g);
 }
@@ -477,8 +478,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     const size_t n = std::max<uint32_t>(g->n, 1);
     CKS(dev_alloc(ctx, (void**)&g->d_col[0], 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_initlab, 4 * n));
-    CKS(dev_alloc(ctx, (void**)&g->d_sig1, 8 * n));
-    CKS(dev_alloc(ctx, (void**)&g->d_sig2, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_sig, sizeof(Sig) * n));
     CKS(dev_alloc(ctx, (void**)&g->d_slot, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_out, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_rank, 2 * n));
@@ -487,6 +487,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
     CK(cudaMallocHost((void**)&g->h_st, sizeof(RoundState)));
+    CK(cudaMallocHost((void**)&g->h_as, sizeof(ActiveSet)));
     // active set: node lists, followers, group representatives, compacted arc sets
     CKS(dev_alloc(ctx, (void**)&g->d_as, sizeof(ActiveSet)));
     CKS(dev_alloc(ctx, (void**)&g->d_gsync, sizeof(GridSync)));
@@ -509,8 +510,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
         CKS(dev_alloc(ctx, (void**)&g->cb.tile_row[d], 4 * (tiles + 1)));
         CKS(dev_alloc(ctx, (void**)&g->cb.split[d], 4 * (tiles + 1)));
     }
-    CK(cudaMemsetAsync(g->d_sig1, 0, 8 * n, ctx->stream));
-    CK(cudaMemsetAsync(g->d_sig2, 0, 4 * n, ctx->stream));
+    CK(cudaMemsetAsync(g->d_sig, 0, sizeof(Sig) * n, ctx->stream));
     CK(cudaMemsetAsync(g->d_tab, 0, sizeof(Entry) << g->log2tab, ctx->stream));
     g->next_stamp = 1;
     g->bufs = true;
@@ -553,25 +553,25 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         if (first == kPassUniform) {
             const unsigned ugrid = persistent_grid(ctx, g->K, kNodeThreads);
             if (g->weighted)
-                k_signature_uniform<true><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig1, g->d_sig2);
+                k_signature_uniform<true><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig);
             else
-                k_signature_uniform<false><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig1, g->d_sig2);
+                k_signature_uniform<false><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig);
         } else if (first == kPassRank8) {
             const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
             if (g->weighted)
-                k_signature<true, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+                k_signature<true, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig);
             else
-                k_signature<false, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+                k_signature<false, uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig);
         } else if (first == kPassRank16) {
             const uint16_t* cr = reinterpret_cast<const uint16_t*>(g->d_rank);
             if (g->weighted)
-                k_signature<true, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+                k_signature<true, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig);
             else
-                k_signature<false, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig1, g->d_sig2);
+                k_signature<false, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig);
         } else if (g->weighted) {
-            k_signature<true, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
+            k_signature<true, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
         } else {
-            k_signature<false, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2);
+            k_signature<false, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
         }
     }
     if (t) CK(cudaEventRecord(t->ev[2], s));
@@ -580,10 +580,10 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         if (t) CK(cudaEventRecord(t->ev[3], s));
     } else {
         ++rbsc::launch_counter();
-        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig1, g->d_sig2, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab, g->log2tab, g->d_slot);
         if (t) CK(cudaEventRecord(t->ev[3], s));
         ++rbsc::launch_counter();
-        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_col[0], g->d_tab, g->d_slot, g->d_sig1, g->d_sig2);
+        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_col[0], g->d_tab, g->d_slot, g->d_sig);
     }
     ++rbsc::launch_counter();
     k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_pairs, g->d_col[0]);
@@ -601,7 +601,7 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         ++rbsc::launch_counter();
         k_compact_decide<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb);
         ++rbsc::launch_counter();
-        k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig1, g->d_sig2);
+        k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig);
     }
     ++rbsc::launch_counter();
     const bool persist = hash && !ctx->opts.no_persist;
@@ -723,8 +723,7 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     a.as = g->d_as;
     a.st = g->d_st;
     a.col = g->d_col[0];
-    a.sig1 = g->d_sig1;
-    a.sig2 = g->d_sig2;
+    a.sig = g->d_sig;
     a.tab = g->d_tab;
     a.log2tab = g->log2tab;
     a.tab_entries = 1ull << g->log2tab;
@@ -824,28 +823,23 @@ static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
     a.nsplit = g->nsplit;
     a.nodes = g->cb.nodes[0];
     a.compact_arcs = g->compact_arcs ? 1u : 0u;
-    CK(cudaMemcpyAsync(g->d_as, &a, sizeof a, cudaMemcpyHostToDevice, s));
+    *g->h_as = a;
+    CK(cudaMemcpyAsync(g->d_as, g->h_as, sizeof a, cudaMemcpyHostToDevice, s));
     if (g->nsplit) {
         ++rbsc::launch_counter();
-        k_zero_rows<<<grid_for(g->nsplit, 256), 256, 0, s>>>(g->d_split, g->nsplit, g->d_sig1, g->d_sig2);
+        k_zero_rows<<<grid_for(g->nsplit, 256), 256, 0, s>>>(g->d_split, g->nsplit, g->d_sig);
     }
     CK(cudaMemsetAsync(g->d_grep, 0xff, 4 * (size_t)n, s));
     CK(cudaMemsetAsync(g->d_gcnt, 0, 4 * (size_t)n, s));
+    const unsigned lgrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 8, ceil_div<uint64_t>(n, 256));
     ++rbsc::launch_counter();
-    k_group_reps<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_grep, g->d_gcnt);
+    k_group_reps<<<lgrid, 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_grep, g->d_gcnt);
     ++rbsc::launch_counter();
-    k_build_lists<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_col[0], g->d_grep, g->d_gcnt, g->d_as,
-                                                   g->cb.nodes[0], g->d_pairs);
+    k_build_lists<<<lgrid, kNodeThreads, 0, s>>>(n, g->d_off, g->d_initlab, g->d_col[0], g->d_grep, g->d_gcnt, g->d_as,
+                                                 g->cb.nodes[0], g->d_pairs);
+    ++rbsc::launch_counter();
+    k_publish_list<<<1, 1, 0, s>>>(g->d_as);
     CK(cudaGetLastError());
-    // node list written into buffer 0: publish it, the next compaction writes buffer 1
-    uint32_t cnt = 0;
-    CK(cudaMemcpyAsync(&cnt, reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nodectr), 4, cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    const uint32_t zero = 0, one = 1;
-    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nnodes), &cnt, 4, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, nodectr), &zero, 4, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(reinterpret_cast<char*>(g->d_as) + offsetof(ActiveSet, dst_nodes), &one, 4, cudaMemcpyHostToDevice, s));
-    CK(cudaStreamSynchronize(s));
     return RBSC_OK;
 }
 
@@ -952,15 +946,15 @@ static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
     ++rbsc::launch_counter();
-    k_insert_all<kModeRepair><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_fail, g->d_tab, g->log2tab, g->d_slot);
+    k_insert_all<kModeRepair><<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_fail,
+                                                                                             g->d_tab, g->log2tab, g->d_slot);
     ++rbsc::launch_counter();
-    k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
+    k_relabel_all<<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot, nullptr);
     ++rbsc::launch_counter();
     k_fixpoint<kFixRepair><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0);
     CK(cudaGetLastError());
     // every row signature is recomputed from scratch on the whole graph
-    CK(cudaMemsetAsync(g->d_sig1, 0, 8 * (size_t)n, s));
-    CK(cudaMemsetAsync(g->d_sig2, 0, 4 * (size_t)n, s));
+    CK(cudaMemsetAsync(g->d_sig, 0, sizeof(Sig) * (size_t)n, s));
     return init_active_set(ctx, g);
 }
 
@@ -989,11 +983,13 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     CK(cudaEventRecord(ctx->ev[0], s));
     if (d_init) {
         CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
-        CK(cudaMemsetAsync(g->d_col[0], 0, 4 * (size_t)n, s));
+        const unsigned igrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 8, ceil_div<uint64_t>(n, kNodeThreads));
+        const uint32_t chunk = (uint32_t)(ceil_div<uint64_t>(ceil_div<uint64_t>(n, igrid), kNodeThreads) * kNodeThreads);
         ++rbsc::launch_counter();
-        k_insert_all<kModeInit><<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], d_init, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_init<<<igrid, kNodeThreads, 0, s>>>(n, chunk, g->d_st, d_init, g->d_tab, g->log2tab, g->d_slot);
         ++rbsc::launch_counter();
-        k_relabel_all<<<grid_for(n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot);
+        k_relabel_all<<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot,
+                                                                                        g->d_initlab);
         ++rbsc::launch_counter();
         k_fixpoint<kFixInit><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0);
         CK(cudaGetLastError());
@@ -1003,11 +999,10 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         CK(cudaMemcpyAsync(g->d_st, &hs, sizeof hs, cudaMemcpyHostToDevice, s));
         ++rbsc::launch_counter();
         k_fill_uniform<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0]);
+        ++rbsc::launch_counter();
+        k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_initlab);
         CK(cudaGetLastError());
     }
-    ++rbsc::launch_counter();
-    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_initlab);
-    CK(cudaGetLastError());
     CKS(read_state(ctx, g));
     const uint32_t initial_blocks = hs.prev;
     if (kt) {

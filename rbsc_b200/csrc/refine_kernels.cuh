@@ -84,6 +84,33 @@ struct ActiveSet {
     uint32_t nfollow;          // follower list length
 };
 
+// Per-node signature: the 64-bit and the 32-bit sum side by side in 16 B, so
+// that one store or one load of a node's signature touches one 32-B sector
+// (two separate arrays cost two scattered sectors per node).
+struct __align__(16) Sig {
+    unsigned long long s1;
+    uint32_t s2;
+    uint32_t pad;
+};
+
+__device__ __forceinline__ void sig_store(Sig* p, uint64_t s1, uint32_t s2)
+{
+    *reinterpret_cast<ulonglong2*>(p) = make_ulonglong2(s1, (unsigned long long)s2);
+}
+
+__device__ __forceinline__ void sig_add(Sig* p, uint64_t s1, uint32_t s2)
+{
+    atomicAdd(&p->s1, (unsigned long long)s1);
+    atomicAdd(&p->s2, s2);
+}
+
+__device__ __forceinline__ void sig_load(const Sig* p, uint64_t& s1, uint32_t& s2)
+{
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+    s1 = v.x;
+    s2 = (uint32_t)v.y;
+}
+
 // Node-list flag: the node represents a group of arc-less nodes with the same
 // initial colour, so its block is never a singleton.
 constexpr uint32_t kRepFlag = 0x80000000u;
@@ -224,8 +251,7 @@ __device__ __forceinline__ uint32_t gather_col(const ColT* p)
 
 template <bool WEIGHTED, typename ColT, bool NC = true>
 __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
-                                               const ColT* __restrict__ col, unsigned long long* __restrict__ sig1,
-                                               uint32_t* __restrict__ sig2)
+                                               const ColT* __restrict__ col, Sig* __restrict__ sig)
 {
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t ntiles = as->ntiles;
@@ -295,8 +321,7 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
                 if ((hb >> i) & 1u) {
                     if (nh > 0) {
                         const uint32_t node = rows[kbase + nh];
-                        sig1[node] = cur1;
-                        sig2[node] = cur2;
+                        sig_store(&sig[node], cur1, cur2);
                     }
                     ++nh;
                     cur1 = 0;
@@ -351,11 +376,9 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
             const uint64_t tot1 = cin1 + pre1;
             const uint32_t tot2 = cin2 + pre2;
             if (kbase == k0 && !h0) {  // began in an earlier tile
-                atomicAdd(&sig1[node], (unsigned long long)tot1);
-                atomicAdd(&sig2[node], tot2);
+                sig_add(&sig[node], tot1, tot2);
             } else {
-                sig1[node] = tot1;
-                sig2[node] = tot2;
+                sig_store(&sig[node], tot1, tot2);
             }
         }
         // the last lane of the tile closes the tile's last row
@@ -365,11 +388,9 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
             const bool began_before = (klast == k0 && !h0);
             const uint32_t node = rows[klast];
             if (ends && !began_before) {
-                sig1[node] = c1;
-                sig2[node] = c2;
+                sig_store(&sig[node], c1, c2);
             } else {
-                atomicAdd(&sig1[node], (unsigned long long)c1);
-                atomicAdd(&sig2[node], c2);
+                sig_add(&sig[node], c1, c2);
             }
         }
     }
@@ -379,10 +400,9 @@ template <bool WEIGHTED, typename ColT>
 static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveSet* __restrict__ as,
                                                                    const RoundState* __restrict__ st,
                                                                    const ColT* __restrict__ col,
-                                                                   unsigned long long* __restrict__ sig1,
-                                                                   uint32_t* __restrict__ sig2)
+                                                                   Sig* __restrict__ sig)
 {
-    signature_body<WEIGHTED, ColT>(as, st, col, sig1, sig2);
+    signature_body<WEIGHTED, ColT>(as, st, col, sig);
 }
 
 // First pass when every node starts in one block (the reference's default):
@@ -393,8 +413,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_signature_uniform(const
                                                                            const RoundState* __restrict__ st,
                                                                            const uint64_t* __restrict__ off,
                                                                            const uint64_t* __restrict__ wt, uint32_t c0,
-                                                                           unsigned long long* __restrict__ sig1,
-                                                                           uint32_t* __restrict__ sig2)
+                                                                           Sig* __restrict__ sig)
 {
     const uint32_t K = as->K;
     const uint32_t* __restrict__ rows = as->rows;
@@ -414,8 +433,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_signature_uniform(const
                 w2 += (uint32_t)wt[j];
             }
         }
-        sig1[u] = w * t1;
-        sig2[u] = w2 * t2;
+        sig_store(&sig[u], w * t1, w2 * t2);
     }
 }
 
@@ -493,8 +511,7 @@ __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
 // thread's count of new blocks.
 __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                      const uint32_t* __restrict__ col,
-                                                     const unsigned long long* __restrict__ sig1,
-                                                     const uint32_t* __restrict__ sig2, Entry* __restrict__ tab,
+                                                     const Sig* __restrict__ sig, Entry* __restrict__ tab,
                                                      uint32_t log2size, uint32_t* __restrict__ slot)
 {
     const uint32_t nn = as->nnodes;
@@ -518,8 +535,9 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
         uint32_t k2 = stamp;
         if (need) {
             const uint32_t lab = c & kLabelMask;
-            uint64_t s1 = sig1[u];
-            uint32_t s2 = sig2[u];
+            uint64_t s1;
+            uint32_t s2;
+            sig_load(&sig[u], s1, s2);
             if (hb) {  // test hook: truncated (or, from 64 bits on, no) signatures
                 s1 = (hb >= 64) ? 0ull : (s1 & ((1ull << hb) - 1ull));
                 s2 = 0;
@@ -536,41 +554,148 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
 
 static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                                      const uint32_t* __restrict__ col,
-                                                                     const unsigned long long* __restrict__ sig1,
-                                                                     const uint32_t* __restrict__ sig2,
+                                                                     const Sig* __restrict__ sig,
                                                                      Entry* __restrict__ tab, uint32_t log2size,
                                                                      uint32_t* __restrict__ slot)
 {
     __shared__ BlockReserveSmem<kNodeThreads> sm;
-    const uint32_t made = insert_list_body(as, st, col, sig1, sig2, tab, log2size, slot);
+    const uint32_t made = insert_list_body(as, st, col, sig, tab, log2size, slot);
     block_count<kNodeThreads>(made, &st->count, sm);
 }
 
-// Exact pass over all nodes: initial colours (MODE kModeInit, aux = colours)
-// or the repair of a failed exact check (kModeRepair, aux = failure flags).
+// Exact pass over all nodes: the repair of a failed exact check (kModeRepair,
+// aux = failure flags; the key is (label, failed)) or initial colours
+// (kModeInit, aux = colours; k_insert_init is the fast form).  Grid-stride,
+// one count per block.
 template <int MODE>
 static __global__ void __launch_bounds__(kNodeThreads) k_insert_all(uint32_t n, RoundState* __restrict__ st,
                                                                     const uint32_t* __restrict__ col,
                                                                     const uint32_t* __restrict__ aux, Entry* __restrict__ tab,
                                                                     uint32_t log2size, uint32_t* __restrict__ slot)
 {
-    const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
-    const bool active = u < n;
-    const uint32_t stamp = st->stamp;
-    const uint32_t c = active ? col[u] : kSingleton;
-    const bool need = active && (MODE == kModeInit || !(c & kSingleton));
-    uint64_t k1 = 0;
-    if (need) k1 = (MODE == kModeInit) ? (uint64_t)aux[u] : ((uint64_t)(c & kLabelMask) | ((uint64_t)(aux[u] != 0u) << 32));
-    bool nb = active && !need;
-    insert_warp(need, u, u, false, k1, stamp, stamp, tab, log2size, slot, &st->error, nb);
     __shared__ BlockReserveSmem<kNodeThreads> sm;
-    block_count<kNodeThreads>(nb ? 1u : 0u, &st->count, sm);
+    const uint32_t stamp = st->stamp;
+    uint32_t made = 0;
+    for (uint32_t base = blockIdx.x * kNodeThreads; base < n; base += gridDim.x * kNodeThreads) {
+        const uint32_t u = base + threadIdx.x;
+        const bool active = u < n;
+        const uint32_t c = active ? col[u] : kSingleton;
+        const bool need = active && (MODE == kModeInit || !(c & kSingleton));
+        uint64_t k1 = 0;
+        if (need) k1 = (MODE == kModeInit) ? (uint64_t)aux[u] : ((uint64_t)(c & kLabelMask) | ((uint64_t)(aux[u] != 0u) << 32));
+        bool nb = active && !need;
+        insert_warp(need, u, u, false, k1, stamp, stamp, tab, log2size, slot, &st->error, nb);
+        made += nb ? 1u : 0u;
+    }
+    block_count<kNodeThreads>(made, &st->count, sm);
 }
 
+// Initial pass (key = initial colour, the same keys and table as
+// k_insert_all<kModeInit>).  The initial colours of a large graph usually
+// take few values, and with one probe per warp group every warp of the grid
+// would hit the same few table entries, one after another in L2.  Here each
+// block takes a contiguous stretch of nodes and first combines its keys in a
+// shared-memory table (smallest node and count per key), then makes one
+// global insert per distinct key, then hands the global slots back to its
+// nodes.  A key whose probe sequence in the shared table is full (many
+// distinct keys) goes to the global table per warp group instead.
+constexpr int kInitSlots = 1024;
+constexpr int kInitProbes = 32;
+
+__device__ __forceinline__ int init_probe(const unsigned long long* s_key, uint32_t key)
+{
+    uint32_t h = (key * 0x9e3779b1u) >> (32 - 10);
+    for (int p = 0; p < kInitProbes; ++p, h = (h + 1) & (kInitSlots - 1)) {
+        const unsigned long long k = s_key[h];
+        if (k == (unsigned long long)key) return (int)h;
+        if (k == ~0ull) return -1;
+    }
+    return -1;
+}
+
+static __global__ void __launch_bounds__(kNodeThreads) k_insert_init(uint32_t n, uint32_t chunk, RoundState* __restrict__ st,
+                                                                     const uint32_t* __restrict__ init,
+                                                                     Entry* __restrict__ tab, uint32_t log2size,
+                                                                     uint32_t* __restrict__ slot)
+{
+    static_assert(kInitSlots == 1024, "init_probe hashes to 10 bits");
+    __shared__ unsigned long long s_key[kInitSlots];
+    __shared__ uint32_t s_min[kInitSlots], s_cnt[kInitSlots], s_slot[kInitSlots];
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
+    constexpr unsigned long long kEmpty = ~0ull;
+    for (int i = threadIdx.x; i < kInitSlots; i += kNodeThreads) {
+        s_key[i] = kEmpty;
+        s_min[i] = 0xffffffffu;
+        s_cnt[i] = 0u;
+    }
+    __syncthreads();
+    const uint32_t beg = blockIdx.x * chunk;
+    const uint32_t end = (uint32_t)min((uint64_t)n, (uint64_t)beg + chunk);
+    const uint32_t stamp = st->stamp;
+    const int lane = threadIdx.x & 31;
+    uint32_t made = 0;
+    for (uint32_t base = beg; base < end; base += kNodeThreads) {
+        const uint32_t u = base + threadIdx.x;
+        const bool active = u < end;
+        const uint32_t key = active ? init[u] : 0u;
+        const unsigned am = __ballot_sync(0xffffffffu, active);
+        bool overflow = false;
+        if (active) {
+            const unsigned peers = __match_any_sync(am, key);
+            const int leader = __ffs(peers) - 1;
+            const uint32_t umin = __reduce_min_sync(peers, u);
+            int pos = -1;
+            if (lane == leader) {
+                uint32_t h = (key * 0x9e3779b1u) >> (32 - 10);
+                for (int p = 0; p < kInitProbes; ++p, h = (h + 1) & (kInitSlots - 1)) {
+                    const unsigned long long prev = atomicCAS(&s_key[h], kEmpty, (unsigned long long)key);
+                    if (prev == kEmpty || prev == (unsigned long long)key) {
+                        atomicMin(&s_min[h], umin);
+                        atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
+                        pos = (int)h;
+                        break;
+                    }
+                }
+            }
+            pos = __shfl_sync(peers, pos, leader);
+            overflow = pos < 0;
+        }
+        if (__any_sync(0xffffffffu, overflow)) {
+            bool nb = false;
+            insert_warp(overflow, u, u, false, (uint64_t)key, stamp, stamp, tab, log2size, slot, &st->error, nb);
+            made += nb ? 1u : 0u;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kInitSlots; i += kNodeThreads) {
+        const unsigned long long k = s_key[i];
+        if (k == kEmpty) continue;
+        bool claimed = false;
+        s_slot[i] = table_insert(tab, log2size, k, stamp, stamp, s_min[i], s_cnt[i] > 1u, &claimed, &st->error);
+        made += claimed ? 1u : 0u;
+    }
+    __syncthreads();
+    for (uint32_t base = beg; base < end; base += kNodeThreads) {
+        const uint32_t u = base + threadIdx.x;
+        if (u < end) {
+            const int pos = init_probe(s_key, init[u]);
+            if (pos >= 0) slot[u] = s_slot[pos];
+        }
+    }
+    block_count<kNodeThreads>(made, &st->count, sm);
+}
+
+// New colour word from the table entry of the node's class.  The relabel
+// kernels run after the inserts of their pass completed (an earlier launch),
+// so they may read the table through the read-only path (NC), where the few
+// entries of big classes stay in L1; the persistent kernel inserts and
+// relabels in one launch and reads at L2.
+template <bool NC>
 __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, uint32_t s)
 {
     if (c & kSingleton) return c;
-    const uint32_t v = __ldcg(reinterpret_cast<const uint32_t*>(tab + s) + 3);
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(tab + s) + 3;
+    const uint32_t v = NC ? __ldg(w) : __ldcg(w);
     return (v & kLabelMask) | ((v & kJoined) ? 0u : kSingleton);
 }
 
@@ -578,9 +703,10 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 // position); also zeroes the signatures of the rows that cross a tile edge
 // (the next pass adds into them atomically).  Four list entries per thread
 // and iteration, so their dependent loads overlap.
+template <bool NC>
 __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
                                                   const Entry* __restrict__ tab, const uint32_t* __restrict__ slot,
-                                                  unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
+                                                  Sig* __restrict__ sig)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
@@ -596,37 +722,46 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
         }
 #pragma unroll
         for (int j = 0; j < U; ++j) c[j] = u[j] != 0xffffffffu ? col[u[j]] : kSingleton;
+        // most colours of a late pass do not change: no store (a partial
+        // sector write) for those
 #pragma unroll
-        for (int j = 0; j < U; ++j)
-            if (u[j] != 0xffffffffu) col[u[j]] = relabel_one(c[j], tab, s[j]);
+        for (int j = 0; j < U; ++j) {
+            if (u[j] == 0xffffffffu) continue;
+            const uint32_t nc = relabel_one<NC>(c[j], tab, s[j]);
+            if (nc != c[j]) col[u[j]] = nc;
+        }
     }
     const uint32_t ns = as->nsplit;
     const uint32_t* __restrict__ split = as->split;
     for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < ns; i += stride) {
         const uint32_t node = split[i];
-        sig1[node] = 0ull;
-        sig2[node] = 0u;
+        sig_store(&sig[node], 0ull, 0u);
     }
 }
 
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
                                                                       const Entry* __restrict__ tab,
                                                                       const uint32_t* __restrict__ slot,
-                                                                      unsigned long long* __restrict__ sig1,
-                                                                      uint32_t* __restrict__ sig2)
+                                                                      Sig* __restrict__ sig)
 {
-    relabel_list_body(as, col, tab, slot, sig1, sig2);
+    relabel_list_body<true>(as, col, tab, slot, sig);
 }
 
 // New colours of all nodes (after k_insert_all), in place.
+// Initial pass (initlab non-null): every node is relabelled (col is not read)
+// and its label is also written to initlab.
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n, uint32_t* __restrict__ col,
                                                                      const Entry* __restrict__ tab,
-                                                                     const uint32_t* __restrict__ slot)
+                                                                     const uint32_t* __restrict__ slot,
+                                                                     uint32_t* __restrict__ initlab)
 {
-    const uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x;
-    if (u < n) {
-        const uint32_t c = col[u];
-        if (!(c & kSingleton)) col[u] = relabel_one(c, tab, slot[u]);
+    for (uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x; u < n; u += gridDim.x * kNodeThreads) {
+        uint32_t c = initlab ? 0u : col[u];
+        if (!(c & kSingleton)) {
+            c = relabel_one<true>(c, tab, slot[u]);
+            col[u] = c;
+        }
+        if (initlab) initlab[u] = c & kLabelMask;
     }
 }
 
@@ -806,8 +941,7 @@ static __global__ void k_compact_decide(ActiveSet* as, const RoundState* st, Com
 // builds the destination's row-head bitmap, tile rows and split list.  A row
 // entering the split list gets its signatures zeroed here.
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet* __restrict__ as, CompactBufs bufs,
-                                                                      unsigned long long* __restrict__ sig1,
-                                                                      uint32_t* __restrict__ sig2)
+                                                                      Sig* __restrict__ sig)
 {
     if (!as->do_copy) return;
     const uint32_t nk = as->new_K;
@@ -854,8 +988,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
                 const uint32_t node = drows[k0];
                 const uint32_t p = atomicAdd(&as->splitctr, 1u);
                 bufs.split[d][p] = node;
-                sig1[node] = 0ull;
-                sig2[node] = 0u;
+                sig_store(&sig[node], 0ull, 0u);
             }
         }
     }
@@ -911,7 +1044,8 @@ static __global__ void k_compact_finalize(ActiveSet* as, RoundState* st, Compact
 // (__match_any_sync), then per block in a small shared-memory table, and
 // only then in global memory, where the words are read before any atomic:
 // once a label's minimum and count are settled, later blocks only read.
-constexpr int kRepSlots = 64;
+constexpr int kRepSlots = 256;
+constexpr int kRepProbes = 32;
 static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uint64_t* __restrict__ off,
                                                            const uint32_t* __restrict__ initlab,
                                                            uint32_t* __restrict__ grep, uint32_t* __restrict__ gcnt)
@@ -923,30 +1057,33 @@ static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uin
         s_cnt[i] = 0u;
     }
     __syncthreads();
-    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool dangling = u < n && off[u + 1] == off[u];
-    const unsigned dm = __ballot_sync(0xffffffffu, dangling);
-    if (dangling) {
+    // grid-stride: a block combines all its stretches before touching the
+    // global words, so each hot label sees one update per block, not per
+    // 256 nodes
+    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const uint32_t u = base + threadIdx.x;
+        const bool dangling = u < n && off[u + 1] == off[u];
+        const unsigned dm = __ballot_sync(0xffffffffu, dangling);
+        if (!dangling) continue;
         const uint32_t g = initlab[u];
         const unsigned peers = __match_any_sync(dm, g);
         const uint32_t umin = __reduce_min_sync(peers, u);
-        if ((threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1)) {
-            // open-addressed shared table keyed by label; a full table falls
-            // back to the global words directly
-            uint32_t h = (g * 0x9e3779b1u) >> 26;
-            bool placed = false;
-            for (int p = 0; p < kRepSlots && !placed; ++p, h = (h + 1) & (kRepSlots - 1)) {
-                const uint32_t prev = atomicCAS(&s_lab[h], 0xffffffffu, g);
-                if (prev == 0xffffffffu || prev == g) {
-                    atomicMin(&s_min[h], umin);
-                    atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
-                    placed = true;
-                }
+        if ((threadIdx.x & 31) != (uint32_t)(__ffs(peers) - 1)) continue;
+        // open-addressed shared table keyed by label; a key whose probe
+        // sequence is full goes to the global words directly
+        uint32_t h = (g * 0x9e3779b1u) >> 24;
+        bool placed = false;
+        for (int p = 0; p < kRepProbes && !placed; ++p, h = (h + 1) & (kRepSlots - 1)) {
+            const uint32_t prev = atomicCAS(&s_lab[h], 0xffffffffu, g);
+            if (prev == 0xffffffffu || prev == g) {
+                atomicMin(&s_min[h], umin);
+                atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
+                placed = true;
             }
-            if (!placed) {
-                if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
-                if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
-            }
+        }
+        if (!placed) {
+            if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
+            if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
         }
     }
     __syncthreads();
@@ -959,45 +1096,69 @@ static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uin
 }
 
 // Node list = non-singleton nodes that are not followers (representatives
-// flagged); follower pairs; singleton count.
-static __global__ void k_build_lists(uint32_t n, const uint64_t* __restrict__ off, const uint32_t* __restrict__ initlab,
-                                     const uint32_t* __restrict__ col, const uint32_t* __restrict__ grep,
-                                     const uint32_t* __restrict__ gcnt, ActiveSet* __restrict__ as,
-                                     uint32_t* __restrict__ nodes, uint2* __restrict__ pairs)
+// flagged); follower pairs; singleton count.  Grid-stride, both lists written
+// through shared-memory buffers (few reservations on the two counters).
+constexpr int kListBuf = 2048;
+struct BuildListsSmem {
+    BlockAppend<uint32_t, kListBuf, kNodeThreads> nodes;
+    BlockAppend<uint2, kListBuf, kNodeThreads> pairs;
+    BlockReserveSmem<kNodeThreads> sm;
+};
+
+static __global__ void __launch_bounds__(kNodeThreads) k_build_lists(uint32_t n, const uint64_t* __restrict__ off,
+                                                                     const uint32_t* __restrict__ initlab,
+                                                                     const uint32_t* __restrict__ col,
+                                                                     const uint32_t* __restrict__ grep,
+                                                                     const uint32_t* __restrict__ gcnt,
+                                                                     ActiveSet* __restrict__ as, uint32_t* __restrict__ nodes,
+                                                                     uint2* __restrict__ pairs)
 {
-    __shared__ BlockReserveSmem<kNodeThreads> sm;
-    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    const bool valid = u < n;
-    bool follower = false, rep = false, listed = false, single = false;
-    uint32_t r = 0;
-    if (valid) {
-        single = (col[u] & kSingleton) != 0;
-        if (!single && off[u + 1] == off[u]) {
-            const uint32_t g = initlab[u];
-            if (gcnt[g] >= 2u) {
-                r = grep[g];
-                follower = r != u;
-                rep = r == u;
+    __shared__ BuildListsSmem s;
+    block_append_begin(s.nodes);
+    block_append_begin(s.pairs);
+    uint32_t singles = 0;
+    for (uint32_t base = blockIdx.x * kNodeThreads; base < n; base += gridDim.x * kNodeThreads) {
+        const uint32_t u = base + threadIdx.x;
+        const bool valid = u < n;
+        bool follower = false, rep = false, listed = false, single = false;
+        uint32_t r = 0;
+        if (valid) {
+            single = (col[u] & kSingleton) != 0;
+            if (!single && off[u + 1] == off[u]) {
+                const uint32_t g = initlab[u];
+                if (gcnt[g] >= 2u) {
+                    r = grep[g];
+                    follower = r != u;
+                    rep = r == u;
+                }
             }
+            listed = !single && !follower;
         }
-        listed = !single && !follower;
+        singles += single ? 1u : 0u;
+        block_append(s.nodes, listed, u | (rep ? kRepFlag : 0u), &as->nodectr, nodes);
+        block_append(s.pairs, follower, make_uint2(u, r), &as->nfollow, pairs);
     }
-    const uint32_t p = block_reserve<kNodeThreads>(listed, &as->nodectr, sm);
-    if (listed) nodes[p] = u | (rep ? kRepFlag : 0u);
-    const uint32_t q = block_reserve<kNodeThreads>(follower, &as->nfollow, sm);
-    if (follower) pairs[q] = make_uint2(u, r);
-    block_count<kNodeThreads>(single ? 1u : 0u, &as->retired, sm);
+    block_append_flush(s.nodes, &as->nodectr, nodes);
+    block_append_flush(s.pairs, &as->nfollow, pairs);
+    block_count<kNodeThreads>(singles, &as->retired, s.sm);
+}
+
+// Publishes the node list that k_build_lists wrote into buffer 0 (the next
+// compaction writes buffer 1).
+static __global__ void k_publish_list(ActiveSet* as)
+{
+    as->nnodes = as->nodectr;
+    as->nodectr = 0;
+    as->dst_nodes = 1;
 }
 
 // Zeroes the signatures of the given rows (the split rows of the whole-graph
 // tiling, before a refinement starts on it: an earlier refinement may have
 // left values there that the first pass would add to).
-static __global__ void k_zero_rows(const uint32_t* __restrict__ list, uint32_t count, unsigned long long* __restrict__ sig1,
-                                   uint32_t* __restrict__ sig2)
+static __global__ void k_zero_rows(const uint32_t* __restrict__ list, uint32_t count, Sig* __restrict__ sig)
 {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        sig1[list[i]] = 0ull;
-        sig2[list[i]] = 0u;
+        sig_store(&sig[list[i]], 0ull, 0u);
     }
 }
 
@@ -1062,8 +1223,7 @@ struct PersistArgs {
     ActiveSet* as;
     RoundState* st;
     uint32_t* col;
-    unsigned long long* sig1;
-    uint32_t* sig2;
+    Sig* sig;
     Entry* tab;
     uint32_t log2tab;
     uint64_t tab_entries;
@@ -1080,13 +1240,13 @@ static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(Pe
     for (;;) {
         clear_table_body(a.st, a.tab, a.tab_entries);
         if (!grid_barrier(a.gs, a.st)) return;
-        if (a.weighted) signature_body<true, uint32_t, false>(a.as, a.st, a.col, a.sig1, a.sig2);
-        else signature_body<false, uint32_t, false>(a.as, a.st, a.col, a.sig1, a.sig2);
+        if (a.weighted) signature_body<true, uint32_t, false>(a.as, a.st, a.col, a.sig);
+        else signature_body<false, uint32_t, false>(a.as, a.st, a.col, a.sig);
         if (!grid_barrier(a.gs, a.st)) return;
-        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig1, a.sig2, a.tab, a.log2tab, a.slot);
+        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig, a.tab, a.log2tab, a.slot);
         block_count<kNodeThreads>(made, &a.st->count, sm);
         if (!grid_barrier(a.gs, a.st)) return;
-        relabel_list_body(a.as, a.col, a.tab, a.slot, a.sig1, a.sig2);
+        relabel_list_body<false>(a.as, a.col, a.tab, a.slot, a.sig);
         if (!grid_barrier(a.gs, a.st)) return;
         follow_body(a.as, a.pairs, a.col);
         if (!grid_barrier(a.gs, a.st)) return;

@@ -32,21 +32,21 @@ __device__ __forceinline__ uint64_t masked_sig1(const RoundState* st, uint64_t s
 }
 __device__ __forceinline__ uint32_t masked_sig2(const RoundState* st, uint32_t s) { return st->hash_bits ? 0u : s; }
 
-__global__ void k_sr_init(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ sig2,
+__global__ void k_sr_init(uint32_t n, const RoundState* __restrict__ st, const Sig* __restrict__ sig,
                           uint32_t* __restrict__ perm, unsigned long long* __restrict__ keys)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
         perm[i] = i;
-        keys[i] = masked_sig2(st, sig2[i]);
+        keys[i] = masked_sig2(st, sig[i].s2);
     }
 }
 
 __global__ void k_sr_gather_sig1(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ perm,
-                                 const unsigned long long* __restrict__ sig1, unsigned long long* __restrict__ keys)
+                                 const Sig* __restrict__ sig, unsigned long long* __restrict__ keys)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) keys[i] = masked_sig1(st, sig1[perm[i]]);
+    if (i < n) keys[i] = masked_sig1(st, sig[perm[i]].s1);
 }
 
 __global__ void k_sr_gather_label(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ perm,
@@ -58,16 +58,15 @@ __global__ void k_sr_gather_label(uint32_t n, const uint32_t* __restrict__ col, 
 
 // head[i] = position i starts a new (label, signature) group
 __global__ void k_sr_heads(uint32_t n, const RoundState* __restrict__ st, const uint32_t* __restrict__ col,
-                           const uint32_t* __restrict__ perm, const unsigned long long* __restrict__ sig1,
-                           const uint32_t* __restrict__ sig2, uint32_t* __restrict__ head)
+                           const uint32_t* __restrict__ perm, const Sig* __restrict__ sig, uint32_t* __restrict__ head)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     uint32_t h = 1;
     if (i > 0) {
         const uint32_t a = perm[i - 1], b = perm[i];
-        h = (col[a] & kLabelMask) != (col[b] & kLabelMask) || masked_sig1(st, sig1[a]) != masked_sig1(st, sig1[b]) ||
-            masked_sig2(st, sig2[a]) != masked_sig2(st, sig2[b]);
+        h = (col[a] & kLabelMask) != (col[b] & kLabelMask) || masked_sig1(st, sig[a].s1) != masked_sig1(st, sig[b].s1) ||
+            masked_sig2(st, sig[a].s2) != masked_sig2(st, sig[b].s2);
     }
     head[i] = h;
 }
@@ -85,7 +84,7 @@ __global__ void k_sr_gstart(uint32_t n, const uint32_t* __restrict__ head, const
 __global__ void k_sr_assign(uint32_t n, const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
                             const uint32_t* __restrict__ perm, const uint32_t* __restrict__ head,
                             const uint32_t* __restrict__ gid, const uint32_t* __restrict__ gstart,
-                            unsigned long long* __restrict__ sig1, uint32_t* __restrict__ sig2)
+                            Sig* __restrict__ sig)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) {
@@ -97,8 +96,7 @@ __global__ void k_sr_assign(uint32_t n, const ActiveSet* __restrict__ as, uint32
     const uint32_t* __restrict__ split_rows = as->split;
     for (uint32_t k = i; k < nsplit; k += gridDim.x * blockDim.x) {
         const uint32_t node = split_rows[k];
-        sig1[node] = 0ull;
-        sig2[node] = 0u;
+        sig_store(&sig[node], 0ull, 0u);
     }
 }
 
@@ -150,12 +148,12 @@ rbsc_status launch_sort_relabel(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
     bool alt = false;
     cudaError_t e;
     ++rbsc::launch_counter();
-    k_sr_init<<<grid, 256, 0, s>>>(n, g->d_st, g->d_sig2, p0, k0);
+    k_sr_init<<<grid, 256, 0, s>>>(n, g->d_st, g->d_sig, p0, k0);
     if ((e = radix_sort<uint32_t>(k0, k1, p0, p1, n, 0, 32, g->d_sr_tmp, s, &alt)) != cudaSuccess)
         return rbsc_cuda_fail(ctx, e, "radix_sort (sig2)", __LINE__);
     if (alt) { std::swap(k0, k1); std::swap(p0, p1); }
     ++rbsc::launch_counter();
-    k_sr_gather_sig1<<<grid, 256, 0, s>>>(n, g->d_st, p0, g->d_sig1, k0);
+    k_sr_gather_sig1<<<grid, 256, 0, s>>>(n, g->d_st, p0, g->d_sig, k0);
     if ((e = radix_sort<uint32_t>(k0, k1, p0, p1, n, 0, 64, g->d_sr_tmp, s, &alt)) != cudaSuccess)
         return rbsc_cuda_fail(ctx, e, "radix_sort (sig1)", __LINE__);
     if (alt) { std::swap(k0, k1); std::swap(p0, p1); }
@@ -166,14 +164,14 @@ rbsc_status launch_sort_relabel(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
     if (alt) { std::swap(k0, k1); std::swap(p0, p1); }
     // p0 = sorted node order; p1 is free: use it for the group ids
     ++rbsc::launch_counter();
-    k_sr_heads<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], p0, g->d_sig1, g->d_sig2, g->d_sr_head);
+    k_sr_heads<<<grid, 256, 0, s>>>(n, g->d_st, g->d_col[0], p0, g->d_sig, g->d_sr_head);
     uint32_t* count = reinterpret_cast<uint32_t*>(reinterpret_cast<char*>(g->d_st) + offsetof(RoundState, count));
     if ((e = exclusive_scan<uint32_t, uint32_t>(g->d_sr_head, p1, n, count, g->d_sr_tmp, s)) != cudaSuccess)
         return rbsc_cuda_fail(ctx, e, "exclusive_scan (heads)", __LINE__);
     ++rbsc::launch_counter();
     k_sr_gstart<<<grid, 256, 0, s>>>(n, g->d_sr_head, p1, g->d_sr_gstart);
     ++rbsc::launch_counter();
-    k_sr_assign<<<grid, 256, 0, s>>>(n, g->d_as, g->d_col[0], p0, g->d_sr_head, p1, g->d_sr_gstart, g->d_sig1, g->d_sig2);
+    k_sr_assign<<<grid, 256, 0, s>>>(n, g->d_as, g->d_col[0], p0, g->d_sr_head, p1, g->d_sr_gstart, g->d_sig);
     if ((e = cudaGetLastError()) != cudaSuccess) return rbsc_cuda_fail(ctx, e, "sort relabel launch", __LINE__);
     return RBSC_OK;
 }
