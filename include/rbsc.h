@@ -145,6 +145,11 @@ void rbsc_opts_default(rbsc_opts* opts);
  * rbsc.cu:234-270).  Returns NULL on failure; see rbsc_last_error(NULL). */
 rbsc_ctx* rbsc_ctx_create(int32_t device, const rbsc_opts* opts);
 void rbsc_ctx_destroy(rbsc_ctx* ctx);
+/* A context keeps the device and pinned buffers of freed graphs and
+ * one-shot refinements and hands them out again (no reference counterpart:
+ * the reference allocates per run).  rbsc_ctx_trim gives the unused ones
+ * back to CUDA; rbsc_ctx_destroy does so too. */
+void rbsc_ctx_trim(rbsc_ctx* ctx);
 const char* rbsc_last_error(const rbsc_ctx* ctx);
 rbsc_status rbsc_ctx_set_opts(rbsc_ctx* ctx, const rbsc_opts* opts);
 

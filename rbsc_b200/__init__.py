@@ -131,6 +131,10 @@ class Context:
         except Exception:
             pass
 
+    def trim(self):
+        """Gives the cached device / pinned buffers back to CUDA (rbsc_ctx_trim)."""
+        self._lib.rbsc_ctx_trim(self._h)
+
     def set_opts(self, **kw):
         for k, v in kw.items():
             if k == "verify" or k == "use_graph":

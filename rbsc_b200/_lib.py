@@ -34,7 +34,7 @@ EXPORTED = [
     "rbsc_ctx_set_opts", "rbsc_refine", "rbsc_graph_upload", "rbsc_graph_from_device", "rbsc_graph_free",
     "rbsc_graph_info", "rbsc_graph_device_csr", "rbsc_graph_refine", "rbsc_graph_refine_device",
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
-    "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc",
+    "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
 ]
 
 NOALLOC_MAX_NODES = 16384
@@ -142,6 +142,8 @@ def load():
     lib.rbsc_ctx_create.argtypes = [ctypes.c_int32, P(Opts)]
     lib.rbsc_ctx_create.restype = vp
     lib.rbsc_ctx_destroy.argtypes = [vp]
+    lib.rbsc_ctx_trim.argtypes = [vp]
+    lib.rbsc_ctx_trim.restype = None
     lib.rbsc_last_error.argtypes = [vp]
     lib.rbsc_last_error.restype = ctypes.c_char_p
     lib.rbsc_ctx_set_opts.argtypes = [vp, P(Opts)]
@@ -163,7 +165,7 @@ def load():
     lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
     for name in EXPORTED:
-        if name not in ("rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy",
+        if name not in ("rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
                         "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):
             getattr(lib, name).restype = ctypes.c_int32
     _lib = lib

@@ -91,6 +91,35 @@ __device__ __forceinline__ uint32_t block_reserve(bool take, uint32_t* counter, 
     return pos;
 }
 
+// Like block_reserve, with `cnt` positions per thread: returns the first of
+// the thread's cnt consecutive positions.  Block-collective.
+template <int BLOCK>
+__device__ __forceinline__ uint32_t block_reserve_n(uint32_t cnt, uint32_t* counter, BlockReserveSmem<BLOCK>& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) sm.warp_pre[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t run = 0;
+        for (int w = 0; w < BLOCK / 32; ++w) {
+            const uint32_t c = sm.warp_pre[w];
+            sm.warp_pre[w] = run;
+            run += c;
+        }
+        sm.base = run ? atomicAdd(counter, run) : 0u;
+    }
+    __syncthreads();
+    const uint32_t pos = (uint32_t)sm.base + sm.warp_pre[warp] + incl - cnt;
+    __syncthreads();
+    return pos;
+}
+
 // Sum over the block of a per-thread count, added to `counter` with one
 // atomic per block.  Called by all threads of the block.
 template <int BLOCK>

@@ -151,20 +151,21 @@ extern "C" rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint3
     k_rmat_emit<<<(unsigned)ceil_div<uint64_t>(m0 + 1, 256), 256, 0, s>>>(m0, scale, sorted, keep, pos, g->d_idx, g->d_off);
     CKG(cudaGetLastError());
     CKG(cudaStreamSynchronize(s));
-    cudaFree(keys0); keys0 = nullptr;
-    cudaFree(keys1); keys1 = nullptr;
-    cudaFree(keep); keep = nullptr;
-    cudaFree(pos); pos = nullptr;
-    cudaFree(tmp); tmp = nullptr;
+    dev_free(ctx, (void*&)keys0);
+    dev_free(ctx, (void*&)keys1);
+    dev_free(ctx, (void*&)keep);
+    dev_free(ctx, (void*&)pos);
+    dev_free(ctx, tmp);
     CKGS(graph_prepare(ctx, g));
     *out = g;
     g = nullptr;
 done:
-    if (keys0) cudaFree(keys0);
-    if (keys1) cudaFree(keys1);
-    if (keep) cudaFree(keep);
-    if (pos) cudaFree(pos);
-    if (tmp) cudaFree(tmp);
+    cudaStreamSynchronize(s);
+    dev_free(ctx, (void*&)keys0);
+    dev_free(ctx, (void*&)keys1);
+    dev_free(ctx, (void*&)keep);
+    dev_free(ctx, (void*&)pos);
+    dev_free(ctx, tmp);
     if (g) rbsc_graph_free(g);
     return st;
 }

@@ -1,15 +1,31 @@
 // internal.h -- definitions shared by the host translation units of librbsc.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <string>
+#include <unordered_map>
 #include <cuda_runtime.h>
 
 #include "../../include/rbsc.h"
 
 #include "refine_kernels.cuh"
 
+// Cached device (or pinned host) blocks of a context.  Buffers of freed
+// graphs and temporaries go back here and are handed out again to later
+// requests of about the same size: repeated one-shot refinements reuse
+// memory instead of paying for cudaMalloc / cudaFree (and the first touch of
+// fresh pages) every call.
+struct MemPool {
+    bool pinned = false;
+    std::multimap<size_t, void*> free_blocks;  // size -> block, not in use
+    std::unordered_map<void*, size_t> sizes;   // every block the pool allocated
+    size_t cached = 0;                         // bytes in free_blocks
+};
+
 struct rbsc_ctx {
     int device = 0;
+    MemPool dpool;
+    MemPool hpool{true};
     rbsc_opts opts{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
@@ -43,6 +59,7 @@ struct rbsc_graph {
     uint32_t* d_slot = nullptr;
     uint32_t* d_out = nullptr;
     void* d_rank = nullptr;          // first pass: dense class ranks (uint8 / uint16)
+    uint32_t* d_srank = nullptr;     // rank of the initial class claimed at each table slot
     uint32_t* d_init = nullptr;
     rbsc::Entry* d_tab = nullptr;
     uint32_t log2tab = 0;
@@ -95,6 +112,9 @@ struct rbsc_graph {
 rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);
 rbsc_status rbsc_cuda_fail(rbsc_ctx* ctx, cudaError_t e, const char* what, int line);
 rbsc_status dev_alloc(rbsc_ctx* ctx, void** p, size_t bytes);
+void dev_free(rbsc_ctx* ctx, void*& p);
+rbsc_status host_alloc(rbsc_ctx* ctx, void** p, size_t bytes);
+void host_free(rbsc_ctx* ctx, void*& p);
 rbsc_status ensure_temp(rbsc_ctx* ctx, rbsc_graph* g, size_t bytes);
 rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g);
 rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted);

@@ -63,29 +63,109 @@ rbsc_status rbsc_cuda_fail(rbsc_ctx* ctx, cudaError_t e, const char* what, int l
 // ---------------------------------------------------------------------------
 // device buffers
 // ---------------------------------------------------------------------------
-rbsc_status dev_alloc(rbsc_ctx* ctx, void** p, size_t bytes)
+// Block sizes: small requests in powers of two (at least 4 KB), large ones in
+// whole 2 MB pages, so that a repeated request finds its block again.
+static size_t pool_round(size_t bytes)
 {
-    *p = nullptr;
-    if (bytes == 0) bytes = 16;
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return rbsc_fail(ctx, RBSC_ERR_OOM, "cudaMalloc of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    if (bytes <= 4096) return 4096;
+    if (bytes < (2u << 20)) {
+        size_t b = 4096;
+        while (b < bytes) b <<= 1;
+        return b;
     }
-    return RBSC_OK;
+    return (bytes + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
 }
 
-static void dev_free(void*& p)
+// The pool keeps at most this many bytes of unused blocks.
+static constexpr size_t kPoolCacheMax = (size_t)48 << 30;
+
+static void pool_raw_free(MemPool& p, void* b)
 {
-    if (p) cudaFree(p);
+    if (p.pinned) cudaFreeHost(b);
+    else cudaFree(b);
+}
+
+// Gives every unused block back to CUDA.
+static void pool_release(MemPool& p)
+{
+    for (auto& kv : p.free_blocks) {
+        p.sizes.erase(kv.second);
+        pool_raw_free(p, kv.second);
+    }
+    p.free_blocks.clear();
+    p.cached = 0;
+}
+
+static rbsc_status pool_alloc(rbsc_ctx* ctx, MemPool& p, void** out, size_t bytes)
+{
+    *out = nullptr;
+    const size_t want = pool_round(bytes);
+    // best fit among the unused blocks, if it wastes at most half
+    auto it = p.free_blocks.lower_bound(want);
+    if (it != p.free_blocks.end() && it->first <= 2 * want) {
+        *out = it->second;
+        p.cached -= it->first;
+        p.free_blocks.erase(it);
+        return RBSC_OK;
+    }
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        void* b = nullptr;
+        const cudaError_t e = p.pinned ? cudaMallocHost(&b, want) : cudaMalloc(&b, want);
+        if (e == cudaSuccess) {
+            p.sizes[b] = want;
+            *out = b;
+            return RBSC_OK;
+        }
+        cudaGetLastError();
+        if (attempt == 0 && p.cached) {
+            pool_release(p);  // out of memory with blocks cached: give them back and retry
+            continue;
+        }
+        return rbsc_fail(ctx, RBSC_ERR_OOM, "%s of %zu bytes failed: %s", p.pinned ? "cudaMallocHost" : "cudaMalloc", want,
+                         cudaGetErrorString(e));
+    }
+    return RBSC_ERR_OOM;
+}
+
+static void pool_free(MemPool& p, void* b)
+{
+    auto it = p.sizes.find(b);
+    if (it == p.sizes.end()) return;  // not ours (cannot happen)
+    p.free_blocks.emplace(it->second, b);
+    p.cached += it->second;
+    // over the cap: drop the largest unused blocks
+    while (p.cached > kPoolCacheMax && !p.free_blocks.empty()) {
+        auto last = std::prev(p.free_blocks.end());
+        p.cached -= last->first;
+        p.sizes.erase(last->second);
+        pool_raw_free(p, last->second);
+        p.free_blocks.erase(last);
+    }
+}
+
+rbsc_status dev_alloc(rbsc_ctx* ctx, void** p, size_t bytes) { return pool_alloc(ctx, ctx->dpool, p, bytes); }
+
+// Returns a block to the context's pool.  Work already queued on the
+// context's stream that uses the block stays ordered before any later use,
+// since every later user is queued on the same stream.
+void dev_free(rbsc_ctx* ctx, void*& p)
+{
+    if (p) pool_free(ctx->dpool, p);
+    p = nullptr;
+}
+
+rbsc_status host_alloc(rbsc_ctx* ctx, void** p, size_t bytes) { return pool_alloc(ctx, ctx->hpool, p, bytes); }
+
+void host_free(rbsc_ctx* ctx, void*& p)
+{
+    if (p) pool_free(ctx->hpool, p);
     p = nullptr;
 }
 
 rbsc_status ensure_temp(rbsc_ctx* ctx, rbsc_graph* g, size_t bytes)
 {
     if (g->tmp_bytes >= bytes) return RBSC_OK;
-    dev_free(g->d_tmp);
+    dev_free(ctx, g->d_tmp);
     g->tmp_bytes = 0;
     CKS(dev_alloc(ctx, &g->d_tmp, bytes));
     g->tmp_bytes = bytes;
@@ -148,7 +228,18 @@ extern "C" void rbsc_ctx_destroy(rbsc_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto& ev : ctx->ev) cudaEventDestroy(ev);
     cudaStreamDestroy(ctx->stream);
+    pool_release(ctx->dpool);
+    pool_release(ctx->hpool);
     delete ctx;
+}
+
+extern "C" void rbsc_ctx_trim(rbsc_ctx* ctx)
+{
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    pool_release(ctx->dpool);
+    pool_release(ctx->hpool);
 }
 
 extern "C" const char* rbsc_last_error(const rbsc_ctx* ctx)
@@ -172,50 +263,49 @@ static void graph_release_refine(rbsc_graph* g)
     if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
     g->loop_exec = nullptr;
     g->loop_graph = nullptr;
-    dev_free((void*&)g->d_col[0]);
-    dev_free((void*&)g->d_as);
-    dev_free((void*&)g->d_gsync);
-    dev_free((void*&)g->d_pairs);
-    dev_free((void*&)g->d_grep);
-    dev_free((void*&)g->d_gcnt);
+    dev_free(g->ctx, (void*&)g->d_col[0]);
+    dev_free(g->ctx, (void*&)g->d_as);
+    dev_free(g->ctx, (void*&)g->d_gsync);
+    dev_free(g->ctx, (void*&)g->d_pairs);
+    dev_free(g->ctx, (void*&)g->d_grep);
+    dev_free(g->ctx, (void*&)g->d_gcnt);
     for (int d = 0; d < 2; ++d) {
-        dev_free((void*&)g->cb.rows[d]);
-        dev_free((void*&)g->cb.off[d]);
-        dev_free((void*&)g->cb.src[d]);
-        dev_free((void*&)g->cb.idx[d]);
-        dev_free((void*&)g->cb.wt[d]);
-        dev_free((void*&)g->cb.head8[d]);
-        dev_free((void*&)g->cb.tile_row[d]);
-        dev_free((void*&)g->cb.split[d]);
-        dev_free((void*&)g->cb.nodes[d]);
+        dev_free(g->ctx, (void*&)g->cb.rows[d]);
+        dev_free(g->ctx, (void*&)g->cb.off[d]);
+        dev_free(g->ctx, (void*&)g->cb.src[d]);
+        dev_free(g->ctx, (void*&)g->cb.idx[d]);
+        dev_free(g->ctx, (void*&)g->cb.wt[d]);
+        dev_free(g->ctx, (void*&)g->cb.head8[d]);
+        dev_free(g->ctx, (void*&)g->cb.tile_row[d]);
+        dev_free(g->ctx, (void*&)g->cb.split[d]);
+        dev_free(g->ctx, (void*&)g->cb.nodes[d]);
     }
-    dev_free((void*&)g->d_initlab);
-    dev_free((void*&)g->d_sig);
-    dev_free((void*&)g->d_slot);
-    dev_free((void*&)g->d_tab);
-    dev_free((void*&)g->d_st);
-    dev_free((void*&)g->d_out);
-    dev_free((void*&)g->d_rank);
-    dev_free((void*&)g->d_init);
-    dev_free((void*&)g->d_vflag);
-    dev_free((void*&)g->d_vrow);
-    dev_free((void*&)g->d_vl8);
-    dev_free((void*&)g->d_vl32);
-    dev_free((void*&)g->d_vllong);
-    dev_free((void*&)g->d_vdeg);
-    dev_free((void*&)g->d_fail);
-    dev_free((void*&)g->d_keys[0]);
-    dev_free((void*&)g->d_keys[1]);
-    dev_free((void*&)g->d_vals[0]);
-    dev_free((void*&)g->d_vals[1]);
-    dev_free((void*&)g->d_small);
-    dev_free(g->d_tmp);
+    dev_free(g->ctx, (void*&)g->d_initlab);
+    dev_free(g->ctx, (void*&)g->d_sig);
+    dev_free(g->ctx, (void*&)g->d_slot);
+    dev_free(g->ctx, (void*&)g->d_tab);
+    dev_free(g->ctx, (void*&)g->d_srank);
+    dev_free(g->ctx, (void*&)g->d_st);
+    dev_free(g->ctx, (void*&)g->d_out);
+    dev_free(g->ctx, (void*&)g->d_rank);
+    dev_free(g->ctx, (void*&)g->d_init);
+    dev_free(g->ctx, (void*&)g->d_vflag);
+    dev_free(g->ctx, (void*&)g->d_vrow);
+    dev_free(g->ctx, (void*&)g->d_vl8);
+    dev_free(g->ctx, (void*&)g->d_vl32);
+    dev_free(g->ctx, (void*&)g->d_vllong);
+    dev_free(g->ctx, (void*&)g->d_vdeg);
+    dev_free(g->ctx, (void*&)g->d_fail);
+    dev_free(g->ctx, (void*&)g->d_keys[0]);
+    dev_free(g->ctx, (void*&)g->d_keys[1]);
+    dev_free(g->ctx, (void*&)g->d_vals[0]);
+    dev_free(g->ctx, (void*&)g->d_vals[1]);
+    dev_free(g->ctx, (void*&)g->d_small);
+    dev_free(g->ctx, g->d_tmp);
     g->tmp_bytes = 0;
     g->key_cap = 0;
-    if (g->h_st) cudaFreeHost(g->h_st);
-    g->h_st = nullptr;
-    if (g->h_as) cudaFreeHost(g->h_as);
-    g->h_as = nullptr;
+    host_free(g->ctx, (void*&)g->h_st);
+    host_free(g->ctx, (void*&)g->h_as);
     g->bufs = false;
     sortrelabel_release(g);
 }
@@ -226,14 +316,14 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
     cudaSetDevice(g->ctx->device);
     cudaStreamSynchronize(g->ctx->stream);
     graph_release_refine(g);
-    dev_free((void*&)g->d_off);
-    dev_free((void*&)g->d_idx);
-    dev_free((void*&)g->d_wt);
-    dev_free((void*&)g->d_rows);
-    dev_free(g->d_roff);
-    dev_free((void*&)g->d_tile_row);
-    dev_free((void*&)g->d_split);
-    dev_free((void*&)g->d_head8);
+    dev_free(g->ctx, (void*&)g->d_off);
+    dev_free(g->ctx, (void*&)g->d_idx);
+    dev_free(g->ctx, (void*&)g->d_wt);
+    dev_free(g->ctx, (void*&)g->d_rows);
+    dev_free(g->ctx, g->d_roff);
+    dev_free(g->ctx, (void*&)g->d_tile_row);
+    dev_free(g->ctx, (void*&)g->d_split);
+    dev_free(g->ctx, (void*&)g->d_head8);
     delete g;
 }
 
@@ -263,7 +353,7 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
     // validation (device-side, one error word)
     uint32_t* d_err = nullptr;
     CKS(dev_alloc(ctx, (void**)&d_err, sizeof(uint32_t) * 4));
-    struct Guard { uint32_t*& p; ~Guard() { if (p) cudaFree(p); } } guard{d_err};
+    struct Guard { rbsc_ctx* c; uint32_t*& p; ~Guard() { dev_free(c, (void*&)p); } } guard{ctx, d_err};
     CK(cudaMemsetAsync(d_err, 0, sizeof(uint32_t) * 4, s));
     ++rbsc::launch_counter();
     k_validate<<<grid_for(std::max<uint64_t>(n, 1), 256) > 65535u * 16 ? 65535u * 16 : grid_for(std::max<uint64_t>(n, 1), 256), 256, 0, s>>>(n, m, g->d_off, g->d_idx, d_err);
@@ -278,7 +368,7 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)n + 1) + 1024));
     uint32_t* d_pos = nullptr;
     CKS(dev_alloc(ctx, (void**)&d_pos, sizeof(uint32_t) * ((size_t)n + 1)));
-    struct Guard2 { uint32_t*& p; ~Guard2() { if (p) cudaFree(p); } } guard2{d_pos};
+    struct Guard2 { rbsc_ctx* c; uint32_t*& p; ~Guard2() { dev_free(c, (void*&)p); } } guard2{ctx, d_pos};
     ++rbsc::launch_counter();
     k_nonempty_flags<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_off, d_pos);
     CK(cudaGetLastError());
@@ -329,7 +419,7 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
         CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)K + 1) + 1024));
         uint32_t* d_sp = nullptr;
         CKS(dev_alloc(ctx, (void**)&d_sp, sizeof(uint32_t) * ((size_t)K + 1)));
-        struct Guard3 { uint32_t*& p; ~Guard3() { if (p) cudaFree(p); } } guard3{d_sp};
+        struct Guard3 { rbsc_ctx* c; uint32_t*& p; ~Guard3() { dev_free(c, (void*&)p); } } guard3{ctx, d_sp};
         if (g->off32) {
             ++rbsc::launch_counter();
             k_split_flags<uint32_t><<<grid_for(K, 256), 256, 0, s>>>(K, (const uint32_t*)g->d_roff, d_sp);
@@ -428,7 +518,7 @@ static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device
             e = cudaGetLastError();
         }
         cudaStreamSynchronize(s);
-        cudaFree(tmp);
+        dev_free(ctx, tmp);
     }
     if (e == cudaSuccess && c->m) e = cudaMemcpyAsync(g->d_idx, c->indices, sizeof(uint32_t) * c->m, kind, s);
     if (e == cudaSuccess && c->weights && c->m) e = cudaMemcpyAsync(g->d_wt, c->weights, sizeof(uint64_t) * c->m, kind, s);
@@ -485,9 +575,10 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_small, 256));
     g->log2tab = std::max<uint32_t>(10, log2_ceil(2ull * n));
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
+    CKS(dev_alloc(ctx, (void**)&g->d_srank, (size_t)4 << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
-    CK(cudaMallocHost((void**)&g->h_st, sizeof(RoundState)));
-    CK(cudaMallocHost((void**)&g->h_as, sizeof(ActiveSet)));
+    CKS(host_alloc(ctx, (void**)&g->h_st, sizeof(RoundState)));
+    CKS(host_alloc(ctx, (void**)&g->h_as, sizeof(ActiveSet)));
     // active set: node lists, followers, group representatives, compacted arc sets
     CKS(dev_alloc(ctx, (void**)&g->d_as, sizeof(ActiveSet)));
     CKS(dev_alloc(ctx, (void**)&g->d_gsync, sizeof(GridSync)));
@@ -583,10 +674,10 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab, g->log2tab, g->d_slot);
         if (t) CK(cudaEventRecord(t->ev[3], s));
         ++rbsc::launch_counter();
-        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_col[0], g->d_tab, g->d_slot, g->d_sig);
+        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_tab, g->d_slot, g->d_sig);
     }
     ++rbsc::launch_counter();
-    k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_pairs, g->d_col[0]);
+    k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_pairs, g->d_col[0]);
     if (t) CK(cudaEventRecord(t->ev[4], s));
     ++rbsc::launch_counter();
     k_fixpoint<kFixHash><<<1, 1, 0, s>>>(g->d_st, g->d_as, hash ? 1 : 0);
@@ -893,10 +984,10 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
         if (nkeys >= (1ull << 32))
             return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "exact check: %llu arcs in long rows (limit 2^32)", (unsigned long long)nkeys);
         if (nkeys > g->key_cap) {
-            dev_free((void*&)g->d_keys[0]);
-            dev_free((void*&)g->d_keys[1]);
-            dev_free((void*&)g->d_vals[0]);
-            dev_free((void*&)g->d_vals[1]);
+            dev_free(g->ctx, (void*&)g->d_keys[0]);
+            dev_free(g->ctx, (void*&)g->d_keys[1]);
+            dev_free(g->ctx, (void*&)g->d_vals[0]);
+            dev_free(g->ctx, (void*&)g->d_vals[1]);
             g->key_cap = 0;
             CKS(dev_alloc(ctx, (void**)&g->d_keys[0], 8 * nkeys));
             CKS(dev_alloc(ctx, (void**)&g->d_keys[1], 8 * nkeys));
@@ -986,10 +1077,11 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         const unsigned igrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 8, ceil_div<uint64_t>(n, kNodeThreads));
         const uint32_t chunk = (uint32_t)(ceil_div<uint64_t>(ceil_div<uint64_t>(n, igrid), kNodeThreads) * kNodeThreads);
         ++rbsc::launch_counter();
-        k_insert_init<<<igrid, kNodeThreads, 0, s>>>(n, chunk, g->d_st, d_init, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_init<<<igrid, kNodeThreads, 0, s>>>(n, chunk, g->d_st, d_init, g->d_tab, g->log2tab, g->d_slot, g->d_srank);
         ++rbsc::launch_counter();
         k_relabel_all<<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot,
-                                                                                        g->d_initlab);
+                                                                                        g->d_initlab, g->d_st, g->d_srank,
+                                                                                        g->d_rank);
         ++rbsc::launch_counter();
         k_fixpoint<kFixInit><<<1, 1, 0, s>>>(g->d_st, g->d_as, 0);
         CK(cudaGetLastError());
@@ -1032,10 +1124,13 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     if (g->m > 0 && ctx->opts.relabel != RBSC_RELABEL_SORT) {
         if (initial_blocks == 1) {
             first = kPassUniform;
-            CK(cudaMemcpyAsync(&c0, g->d_col[0], 4, cudaMemcpyDeviceToHost, s));
-            CK(cudaStreamSynchronize(s));
+            c0 = 0;  // the one class is labelled by node 0
         } else if (initial_blocks <= 65536) {
             first = initial_blocks <= 256 ? kPassRank8 : kPassRank16;
+        }
+        // k_relabel_all wrote the ranks when k_insert_init ranked every class;
+        // otherwise: ranks of the class heads in label order, by a scan
+        if ((first == kPassRank8 || first == kPassRank16) && !(d_init && !hs.rank_bad && hs.ranks == initial_blocks)) {
             CKS(ensure_temp(ctx, g, scan_temp_bytes<uint32_t>((uint64_t)n + 1) + 1024));
             ++rbsc::launch_counter();
             k_class_heads<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_slot);

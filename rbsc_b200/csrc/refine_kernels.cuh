@@ -33,7 +33,7 @@ constexpr int kRoundLog = 64;
 // k_fixpoint (one thread) advances it.
 struct RoundState {
     uint32_t round;          // completed signature passes
-    uint32_t parity;         // unused (colours are updated in place)
+    uint32_t rep_changed;    // a representative's colour changed in the running pass
     uint32_t count;          // blocks counted by the running pass
     uint32_t prev;           // blocks after the last completed pass
     uint32_t done;           // fixpoint reached
@@ -43,6 +43,8 @@ struct RoundState {
     uint32_t clear_pending;  // table must be cleared before the running pass
     uint32_t hash_bits;      // test hook: signatures truncated to this many bits (0 = off)
     uint32_t handoff;        // the active set is small: the persistent kernel takes over
+    uint32_t ranks;          // initial classes given a dense rank by k_insert_init
+    uint32_t rank_bad;       // k_insert_init could not rank every class (dense ranks by scan instead)
     uint32_t pad;
     uint64_t seed;
     uint32_t round_blocks[kRoundLog];
@@ -613,10 +615,15 @@ __device__ __forceinline__ int init_probe(const unsigned long long* s_key, uint3
     return -1;
 }
 
+//
+// Every class that a block claims gets a dense rank (0, 1, ... in claiming
+// order) in srank[slot]; the first signature pass gathers these ranks as
+// 8- or 16-bit colours when there are few classes.  A class claimed on the
+// per-warp path gets none (rank_bad is raised and the ranks come from a scan).
 static __global__ void __launch_bounds__(kNodeThreads) k_insert_init(uint32_t n, uint32_t chunk, RoundState* __restrict__ st,
                                                                      const uint32_t* __restrict__ init,
                                                                      Entry* __restrict__ tab, uint32_t log2size,
-                                                                     uint32_t* __restrict__ slot)
+                                                                     uint32_t* __restrict__ slot, uint32_t* __restrict__ srank)
 {
     static_assert(kInitSlots == 1024, "init_probe hashes to 10 bits");
     __shared__ unsigned long long s_key[kInitSlots];
@@ -664,15 +671,27 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_init(uint32_t n,
             bool nb = false;
             insert_warp(overflow, u, u, false, (uint64_t)key, stamp, stamp, tab, log2size, slot, &st->error, nb);
             made += nb ? 1u : 0u;
+            if (nb) st->rank_bad = 1u;
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kInitSlots; i += kNodeThreads) {
+    constexpr int kPer = kInitSlots / kNodeThreads;
+    uint32_t claims = 0;
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int i = threadIdx.x + j * kNodeThreads;
         const unsigned long long k = s_key[i];
-        if (k == kEmpty) continue;
         bool claimed = false;
-        s_slot[i] = table_insert(tab, log2size, k, stamp, stamp, s_min[i], s_cnt[i] > 1u, &claimed, &st->error);
-        made += claimed ? 1u : 0u;
+        if (k != kEmpty) s_slot[i] = table_insert(tab, log2size, k, stamp, stamp, s_min[i], s_cnt[i] > 1u, &claimed, &st->error);
+        s_cnt[i] = claimed ? 1u : 0u;  // s_cnt is free from here on: the claimed flags
+        claims += claimed ? 1u : 0u;
+    }
+    made += claims;
+    uint32_t r0 = block_reserve_n<kNodeThreads>(claims, &st->ranks, sm);
+#pragma unroll
+    for (int j = 0; j < kPer; ++j) {
+        const int i = threadIdx.x + j * kNodeThreads;
+        if (s_cnt[i]) srank[s_slot[i]] = r0++;
     }
     __syncthreads();
     for (uint32_t base = beg; base < end; base += kNodeThreads) {
@@ -704,9 +723,9 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 // (the next pass adds into them atomically).  Four list entries per thread
 // and iteration, so their dependent loads overlap.
 template <bool NC>
-__device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
-                                                  const Entry* __restrict__ tab, const uint32_t* __restrict__ slot,
-                                                  Sig* __restrict__ sig)
+__device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
+                                                  uint32_t* __restrict__ col, const Entry* __restrict__ tab,
+                                                  const uint32_t* __restrict__ slot, Sig* __restrict__ sig)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
@@ -714,21 +733,28 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
     constexpr int U = 4;
     for (uint32_t i0 = blockIdx.x * kNodeThreads + threadIdx.x; i0 < nn; i0 += U * stride) {
         uint32_t u[U], s[U], c[U];
+        bool rep[U];
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             const uint32_t i = i0 + j * stride;
-            u[j] = i < nn ? (nodes[i] & ~kRepFlag) : 0xffffffffu;
+            const uint32_t e = i < nn ? nodes[i] : 0xffffffffu;
+            u[j] = e == 0xffffffffu ? e : (e & ~kRepFlag);
+            rep[j] = e != 0xffffffffu && (e & kRepFlag);
             s[j] = i < nn ? slot[i] : 0u;
         }
 #pragma unroll
         for (int j = 0; j < U; ++j) c[j] = u[j] != 0xffffffffu ? col[u[j]] : kSingleton;
         // most colours of a late pass do not change: no store (a partial
-        // sector write) for those
+        // sector write) for those; a changed representative makes k_follow
+        // run in this pass
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             if (u[j] == 0xffffffffu) continue;
             const uint32_t nc = relabel_one<NC>(c[j], tab, s[j]);
-            if (nc != c[j]) col[u[j]] = nc;
+            if (nc != c[j]) {
+                col[u[j]] = nc;
+                if (rep[j]) st->rep_changed = 1u;
+            }
         }
     }
     const uint32_t ns = as->nsplit;
@@ -739,27 +765,37 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
     }
 }
 
-static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as, uint32_t* __restrict__ col,
+static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as,
+                                                                      RoundState* __restrict__ st, uint32_t* __restrict__ col,
                                                                       const Entry* __restrict__ tab,
                                                                       const uint32_t* __restrict__ slot,
                                                                       Sig* __restrict__ sig)
 {
-    relabel_list_body<true>(as, col, tab, slot, sig);
+    relabel_list_body<true>(as, st, col, tab, slot, sig);
 }
 
 // New colours of all nodes (after k_insert_all), in place.
 // Initial pass (initlab non-null): every node is relabelled (col is not read)
-// and its label is also written to initlab.
+// and its label is also written to initlab; with at most 65536 classes, all
+// ranked by k_insert_init, the class rank goes to rank (8 or 16 bits).
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n, uint32_t* __restrict__ col,
                                                                      const Entry* __restrict__ tab,
                                                                      const uint32_t* __restrict__ slot,
-                                                                     uint32_t* __restrict__ initlab)
+                                                                     uint32_t* __restrict__ initlab,
+                                                                     const RoundState* __restrict__ st = nullptr,
+                                                                     const uint32_t* __restrict__ srank = nullptr,
+                                                                     void* __restrict__ rank = nullptr)
 {
+    const uint32_t classes = st ? st->count : 0xffffffffu;
+    const int rank_bytes = (!st || st->rank_bad || classes > 65536u) ? 0 : (classes <= 256u ? 1 : 2);
     for (uint32_t u = blockIdx.x * kNodeThreads + threadIdx.x; u < n; u += gridDim.x * kNodeThreads) {
         uint32_t c = initlab ? 0u : col[u];
         if (!(c & kSingleton)) {
-            c = relabel_one<true>(c, tab, slot[u]);
+            const uint32_t s = slot[u];
+            c = relabel_one<true>(c, tab, s);
             col[u] = c;
+            if (rank_bytes == 1) static_cast<uint8_t*>(rank)[u] = (uint8_t)__ldg(srank + s);
+            else if (rank_bytes == 2) static_cast<uint16_t*>(rank)[u] = (uint16_t)__ldg(srank + s);
         }
         if (initlab) initlab[u] = c & kLabelMask;
     }
@@ -767,9 +803,14 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n,
 
 // Followers (arc-less nodes that are not their group's representative) take
 // the representative's colour.  pairs[i] = (follower, representative).
-__device__ __forceinline__ void follow_body(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
-                                            uint32_t* __restrict__ col)
+__device__ __forceinline__ void follow_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
+                                            const uint2* __restrict__ pairs, uint32_t* __restrict__ col)
 {
+    // the representatives' colours are those of their groups: they change
+    // in the pass after the lists are built, and then only when a block of
+    // arc-less nodes loses a member with arcs that merged into it by a hash
+    // collision; nothing to copy otherwise
+    if (!*(const volatile uint32_t*)&st->rep_changed) return;
     const uint32_t nf = as->nfollow;
     const uint32_t stride = gridDim.x * kNodeThreads;
     for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < nf; i += stride) {
@@ -778,10 +819,11 @@ __device__ __forceinline__ void follow_body(const ActiveSet* __restrict__ as, co
     }
 }
 
-static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet* __restrict__ as, const uint2* __restrict__ pairs,
-                                                                uint32_t* __restrict__ col)
+static __global__ void __launch_bounds__(kNodeThreads) k_follow(const ActiveSet* __restrict__ as,
+                                                                const RoundState* __restrict__ st,
+                                                                const uint2* __restrict__ pairs, uint32_t* __restrict__ col)
 {
-    follow_body(as, pairs, col);
+    follow_body(as, st, pairs, col);
 }
 
 // k_fixpoint: one thread.  Closes the running pass and decides whether the
@@ -797,6 +839,7 @@ __device__ __forceinline__ void fixpoint_body(RoundState* st, const ActiveSet* a
 {
     uint32_t cnt = st->count;
     st->count = 0;
+    st->rep_changed = 0u;
     if (MODE == kFixHash) {
         if (add_retired) cnt += as->retired;
         const uint32_t r = st->round + 1u;
@@ -1057,33 +1100,46 @@ static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uin
         s_cnt[i] = 0u;
     }
     __syncthreads();
-    // grid-stride: a block combines all its stretches before touching the
-    // global words, so each hot label sees one update per block, not per
-    // 256 nodes
-    for (uint32_t base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t u = base + threadIdx.x;
-        const bool dangling = u < n && off[u + 1] == off[u];
-        const unsigned dm = __ballot_sync(0xffffffffu, dangling);
-        if (!dangling) continue;
-        const uint32_t g = initlab[u];
-        const unsigned peers = __match_any_sync(dm, g);
-        const uint32_t umin = __reduce_min_sync(peers, u);
-        if ((threadIdx.x & 31) != (uint32_t)(__ffs(peers) - 1)) continue;
-        // open-addressed shared table keyed by label; a key whose probe
-        // sequence is full goes to the global words directly
-        uint32_t h = (g * 0x9e3779b1u) >> 24;
-        bool placed = false;
-        for (int p = 0; p < kRepProbes && !placed; ++p, h = (h + 1) & (kRepSlots - 1)) {
-            const uint32_t prev = atomicCAS(&s_lab[h], 0xffffffffu, g);
-            if (prev == 0xffffffffu || prev == g) {
-                atomicMin(&s_min[h], umin);
-                atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
-                placed = true;
-            }
+    // grid-stride, 4 nodes per thread and step (their loads overlap): a block
+    // combines all its stretches before touching the global words, so each
+    // hot label sees one update per block, not per 256 nodes
+    constexpr int U = 4;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x * U; base < n; base += stride * U) {
+        bool dang[U];
+        uint32_t lab[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + j * blockDim.x + threadIdx.x;
+            dang[j] = u < n && off[u + 1] == off[u];
         }
-        if (!placed) {
-            if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
-            if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
+#pragma unroll
+        for (int j = 0; j < U; ++j) lab[j] = dang[j] ? initlab[base + j * blockDim.x + threadIdx.x] : 0u;
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + j * blockDim.x + threadIdx.x;
+            const unsigned dm = __ballot_sync(0xffffffffu, dang[j]);
+            if (!dang[j]) continue;
+            const uint32_t g = lab[j];
+            const unsigned peers = __match_any_sync(dm, g);
+            const uint32_t umin = __reduce_min_sync(peers, u);
+            if ((threadIdx.x & 31) != (uint32_t)(__ffs(peers) - 1)) continue;
+            // open-addressed shared table keyed by label; a key whose probe
+            // sequence is full goes to the global words directly
+            uint32_t h = (g * 0x9e3779b1u) >> 24;
+            bool placed = false;
+            for (int p = 0; p < kRepProbes && !placed; ++p, h = (h + 1) & (kRepSlots - 1)) {
+                const uint32_t prev = atomicCAS(&s_lab[h], 0xffffffffu, g);
+                if (prev == 0xffffffffu || prev == g) {
+                    atomicMin(&s_min[h], umin);
+                    atomicAdd(&s_cnt[h], (uint32_t)__popc(peers));
+                    placed = true;
+                }
+            }
+            if (!placed) {
+                if (*(volatile uint32_t*)&grep[g] > umin) atomicMin(&grep[g], umin);
+                if (*(volatile uint32_t*)&gcnt[g] < 2u) atomicAdd(&gcnt[g], (uint32_t)__popc(peers));
+            }
         }
     }
     __syncthreads();
@@ -1117,26 +1173,43 @@ static __global__ void __launch_bounds__(kNodeThreads) k_build_lists(uint32_t n,
     block_append_begin(s.nodes);
     block_append_begin(s.pairs);
     uint32_t singles = 0;
-    for (uint32_t base = blockIdx.x * kNodeThreads; base < n; base += gridDim.x * kNodeThreads) {
-        const uint32_t u = base + threadIdx.x;
-        const bool valid = u < n;
-        bool follower = false, rep = false, listed = false, single = false;
-        uint32_t r = 0;
-        if (valid) {
-            single = (col[u] & kSingleton) != 0;
-            if (!single && off[u + 1] == off[u]) {
-                const uint32_t g = initlab[u];
-                if (gcnt[g] >= 2u) {
-                    r = grep[g];
-                    follower = r != u;
-                    rep = r == u;
-                }
-            }
-            listed = !single && !follower;
+    // 4 nodes per thread and step: their dependent loads (offsets, then the
+    // initial label, then the group words) overlap
+    constexpr int U = 4;
+    const uint32_t stride = gridDim.x * kNodeThreads;
+    for (uint32_t base = blockIdx.x * kNodeThreads * U; base < n; base += stride * U) {
+        bool single[U], dang[U];
+        uint32_t g[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + j * kNodeThreads + threadIdx.x;
+            single[j] = u < n && (col[u] & kSingleton) != 0;
+            dang[j] = u < n && !single[j] && off[u + 1] == off[u];
         }
-        singles += single ? 1u : 0u;
-        block_append(s.nodes, listed, u | (rep ? kRepFlag : 0u), &as->nodectr, nodes);
-        block_append(s.pairs, follower, make_uint2(u, r), &as->nfollow, pairs);
+#pragma unroll
+        for (int j = 0; j < U; ++j) g[j] = dang[j] ? initlab[base + j * kNodeThreads + threadIdx.x] : 0u;
+        uint32_t gc[U], gr[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            gc[j] = dang[j] ? gcnt[g[j]] : 0u;
+            gr[j] = dang[j] ? grep[g[j]] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + j * kNodeThreads + threadIdx.x;
+            const bool valid = u < n;
+            bool follower = false, rep = false;
+            uint32_t r = 0;
+            if (dang[j] && gc[j] >= 2u) {
+                r = gr[j];
+                follower = r != u;
+                rep = r == u;
+            }
+            const bool listed = valid && !single[j] && !follower;
+            singles += single[j] ? 1u : 0u;
+            block_append(s.nodes, listed, u | (rep ? kRepFlag : 0u), &as->nodectr, nodes);
+            block_append(s.pairs, follower, make_uint2(u, r), &as->nfollow, pairs);
+        }
     }
     block_append_flush(s.nodes, &as->nodectr, nodes);
     block_append_flush(s.pairs, &as->nfollow, pairs);
@@ -1246,9 +1319,9 @@ static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(Pe
         const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig, a.tab, a.log2tab, a.slot);
         block_count<kNodeThreads>(made, &a.st->count, sm);
         if (!grid_barrier(a.gs, a.st)) return;
-        relabel_list_body<false>(a.as, a.col, a.tab, a.slot, a.sig);
+        relabel_list_body<false>(a.as, a.st, a.col, a.tab, a.slot, a.sig);
         if (!grid_barrier(a.gs, a.st)) return;
-        follow_body(a.as, a.pairs, a.col);
+        follow_body(a.as, a.st, a.pairs, a.col);
         if (!grid_barrier(a.gs, a.st)) return;
         if (blockIdx.x == 0 && threadIdx.x == 0) fixpoint_body<kFixHash>(a.st, a.as, 1);
         if (!grid_barrier(a.gs, a.st)) return;

@@ -102,21 +102,15 @@ __global__ void k_sr_assign(uint32_t n, const ActiveSet* __restrict__ as, uint32
 
 }  // namespace
 
-static void sr_free(void*& p)
-{
-    if (p) cudaFree(p);
-    p = nullptr;
-}
-
 void sortrelabel_release(rbsc_graph* g)
 {
-    sr_free((void*&)g->d_sr_keys[0]);
-    sr_free((void*&)g->d_sr_keys[1]);
-    sr_free((void*&)g->d_sr_perm[0]);
-    sr_free((void*&)g->d_sr_perm[1]);
-    sr_free((void*&)g->d_sr_head);
-    sr_free((void*&)g->d_sr_gstart);
-    sr_free(g->d_sr_tmp);
+    dev_free(g->ctx, (void*&)g->d_sr_keys[0]);
+    dev_free(g->ctx, (void*&)g->d_sr_keys[1]);
+    dev_free(g->ctx, (void*&)g->d_sr_perm[0]);
+    dev_free(g->ctx, (void*&)g->d_sr_perm[1]);
+    dev_free(g->ctx, (void*&)g->d_sr_head);
+    dev_free(g->ctx, (void*&)g->d_sr_gstart);
+    dev_free(g->ctx, g->d_sr_tmp);
     g->sr_tmp_bytes = 0;
     g->sr_bufs = false;
 }

@@ -189,6 +189,38 @@ def test_resident_graph_repeatable(ctx, scale):
     g.free()
 
 
+@pytest.mark.parametrize("classes", [200, 3000, 50000])
+def test_many_initial_classes(ctx, classes):
+    """Initial colours with 200 / 3000 / 50000 values on 1.5M nodes: 8-bit and
+    16-bit dense ranks from the initial inserts, and (50000: more distinct
+    colours per block than the shared-memory table holds) the ranks from the
+    scan instead."""
+    off, idx = G.er_directed(1_500_000, 3_000_000, seed=3)
+    init = np.random.default_rng(5).integers(0, classes, size=1_500_000).astype(np.uint32) * np.uint32(7919)
+    ex = oracle.refine_exact(off, idx, init=init)
+    r = ctx.refine(off, idx, init=init)
+    _check_against(r, ex.labels, ex.blocks, ex.rounds)
+    assert r.initial_blocks == ex.round_blocks[0] == len(np.unique(init))
+
+
+def test_buffer_pool_reuse():
+    """One-shot refinements of graphs of different sizes on one context reuse
+    the context's cached buffers (stale contents must not leak into the next
+    refinement); trimming the cache in between changes nothing."""
+    cases = []
+    for i, (n, m) in enumerate([(3000, 12000), (800, 2000), (3000, 12000), (5000, 30000)]):
+        off, idx = G.er_directed(n, m, seed=40 + i)
+        init = np.random.default_rng(i).integers(0, 3, size=n).astype(np.uint32)
+        cases.append((off, idx, init, oracle.refine_exact(off, idx, init=init)))
+    with R.Context(0) as c:
+        for k in range(2):
+            for off, idx, init, ex in cases:
+                r = c.refine(off, idx, init=init)
+                _check_against(r, ex.labels, ex.blocks, ex.rounds)
+            if k == 0:
+                c.trim()
+
+
 def test_seed_independence_and_idempotence(ctx):
     off, idx = G.rmat(15, 16, seed=6)
     a = ctx.refine(off, idx)
