@@ -34,6 +34,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
@@ -310,6 +312,8 @@ def run_ours(args, rank, world, local_rank):
            "h2d_ms": e2e_res[-1].h2d_ms, "d2h_ms": e2e_res[-1].d2h_ms,
            "path": "rbsc_refine (C ABI): pinned host CSR + colours in, labels out"}
 
+    batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline_reference()
@@ -322,7 +326,7 @@ def run_ours(args, rank, world, local_rank):
                 "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel}
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "batched": batched}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -330,6 +334,91 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def _pinned(n, dtype):
+    import torch
+    tdt = {np.uint32: torch.int32, np.uint64: torch.int64}[dtype]
+    return torch.empty(max(int(n), 1), dtype=tdt, pin_memory=True).numpy().view(dtype)
+
+
+def _pinned_copy(a):
+    out = _pinned(a.size, a.dtype.type)
+    out[: a.size] = a
+    return out[: a.size]
+
+
+def run_batched(args, ctx, world, dist):
+    """Small-graph batch: graphs/s of one batch refinement (all graphs side by
+    side in one resident graph, one shared colour namespace) against one
+    refinement call per graph, on the same GPU.  Inputs generated off the
+    clock; both paths take host buffers and return host results."""
+    import torch
+    import rbsc_b200 as R
+    G = args.batch_graphs
+    off, idx, gn, lab = R.gen_wl_batch(G, 10, 500, 8, seed=args.seed)
+    n, m = len(off) - 1, len(idx)
+    off_p, idx_p, lab_p = _pinned_copy(off), _pinned_copy(idx), _pinned_copy(lab)
+    bufs = R.batch_buffers(n, G, alloc=lambda k, dt: _pinned(k, dt))
+    rg = ctx.upload(off_p, idx_p)
+    for _ in range(2):
+        rg.batch_refine(gn, lab_p, out=bufs)
+    res_t, res_dev = [], []
+    for _ in range(args.batch_steps):
+        t0 = time.perf_counter()
+        b = rg.batch_refine(gn, lab_p, out=bufs)
+        res_t.append(time.perf_counter() - t0)
+        res_dev.append(b.stats.device_ms)
+    rg.free()
+    ctx.batch_refine(off_p, idx_p, gn, lab_p, out=bufs)
+    one_t = []
+    for _ in range(args.batch_steps):
+        t0 = time.perf_counter()
+        b = ctx.batch_refine(off_p, idx_p, gn, lab_p, out=bufs)
+        one_t.append(time.perf_counter() - t0)
+    # one refinement call per graph, on the first `sample` graphs
+    S = min(args.batch_sample, G)
+    subs = []
+    for k in range(S):
+        a, e = int(gn[k]), int(gn[k + 1])
+        o = off[a: e + 1].astype(np.int64)
+        subs.append(((o - o[0]).astype(np.uint64), (idx[o[0]: o[-1]].astype(np.int64) - a).astype(np.uint32), lab[a:e]))
+    for o, ix, l in subs[:20]:
+        ctx.refine(o, ix, init=l)
+    t0 = time.perf_counter()
+    per = [ctx.refine(o, ix, init=l) for o, ix, l in subs]
+    per_t = time.perf_counter() - t0
+    for k, r1 in enumerate(per):  # each graph's partition = its part of the batch result
+        assert np.array_equal(r1.labels, b.local[int(gn[k]): int(gn[k + 1])])
+    gs = [ctx.upload(o, ix) for o, ix, _ in subs]
+    for gg, (_, _, l) in zip(gs, subs):  # buffers and captured loop in place
+        gg.refine(l)
+    t0 = time.perf_counter()
+    for gg, (_, _, l) in zip(gs, subs):
+        gg.refine(l)
+    per_res_t = time.perf_counter() - t0
+    for gg in gs:
+        gg.free()
+    ts = [float(np.median(one_t)), float(np.median(res_t)), per_t, per_res_t]
+    if dist is not None:
+        t = torch.tensor(ts, dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ts = t.tolist()
+    one_s, res_s, per_t, per_res_t = ts
+    return {"workload": f"{G} graphs: n ~ U[10, 500]; even: Erdos-Renyi p = 4/(n-1), odd: random 3-regular; "
+                        "symmetric arcs; labels U{1..8}",
+            "graphs": G * world, "nodes": n, "arcs": m, "rounds": b.stats.rounds, "blocks": b.stats.blocks,
+            "graphs_per_s": G * world / one_s, "ms": 1000.0 * one_s,
+            "resident_graphs_per_s": G * world / res_s, "resident_ms": 1000.0 * res_s,
+            "device_ms": float(np.median(res_dev)),
+            "per_launch_graphs_per_s": S * world / per_t, "per_launch_resident_graphs_per_s": S * world / per_res_t,
+            "per_launch_sample": S,
+            "speedup": (G / one_s) / (S / per_t), "speedup_resident": (G / res_s) / (S / per_res_t),
+            "paths": {"batched": "rbsc_batch_refine: host CSR + labels in (pinned), colours, local labels, "
+                                 "histograms, fingerprints out",
+                      "batched_resident": "rbsc_graph_batch_refine on the uploaded batch",
+                      "per_launch": "rbsc_refine per graph: host CSR + labels in, labels out",
+                      "per_launch_resident": "rbsc_graph_refine per uploaded graph (each refined once before)"}}
 
 
 def main():
@@ -344,6 +433,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--relabel", choices=["hash", "sort"], default="hash")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--batch-graphs", type=int, default=100000, help="small-graph batch size (0: skip)")
+    ap.add_argument("--batch-steps", type=int, default=5)
+    ap.add_argument("--batch-sample", type=int, default=1000, help="graphs refined one call each")
     args = ap.parse_args()
     rank, world, local_rank = env_rank()
     if args.impl == "reference":

@@ -213,6 +213,52 @@ rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_fa
 rbsc_status rbsc_gen_rmat_host(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
                                uint64_t seed, int32_t threads, rbsc_host_graph* out);
 
+/* ---- batches of small graphs (no reference counterpart) ------------------
+ * Many graphs side by side in one CSR over global node ids (no arc between
+ * two graphs), graph i owning nodes [graph_nodes[i], graph_nodes[i+1]).  They
+ * are refined together, as their disjoint union, so that colours form one
+ * namespace shared by all graphs: a colour is the smallest global node id of
+ * its class over the whole batch.  Two graphs are told apart by colour
+ * refinement (1-WL) iff their colour histograms differ.  Each graph's own
+ * partition is the one a refinement of that graph alone gives. */
+typedef struct {
+    uint32_t num_graphs;
+    uint64_t* graph_nodes;    /* num_graphs+1                                          */
+    uint32_t* labels;         /* n initial labels                                      */
+    rbsc_host_graph csr;      /* the graphs side by side, global node ids               */
+} rbsc_graph_batch;
+
+/* Output arrays (host memory, each may be NULL). */
+typedef struct {
+    uint32_t* colors;         /* n: shared colour of each node                         */
+    uint32_t* local;          /* n: smallest local node id of the node's block in its
+                                 own graph (the canonical label of a refinement of
+                                 that graph alone)                                       */
+    uint32_t* blocks;         /* num_graphs: blocks of each graph                       */
+    uint64_t* fingerprint;    /* num_graphs: 64-bit digest of the colour histogram      */
+    uint64_t* hist_offsets;   /* num_graphs+1: entries of each graph's histogram        */
+    uint32_t* hist_colors;    /* up to n: a graph's colours, increasing                 */
+    uint32_t* hist_counts;    /* up to n: its nodes of that colour                      */
+} rbsc_batch_result;
+
+/* Seeded generator of the small-graph batch: num_graphs graphs with node
+ * counts uniform in [nmin, nmax]; even-numbered graphs Erdos-Renyi with edge
+ * probability 4/(n-1), odd-numbered random 3-regular (n rounded down to
+ * even, at least 4); symmetric arcs; labels uniform in {1..num_labels}.
+ * Free with rbsc_graph_batch_free. */
+rbsc_status rbsc_gen_wl_batch(uint32_t num_graphs, uint32_t nmin, uint32_t nmax, uint32_t num_labels,
+                              uint64_t seed, int32_t threads, rbsc_graph_batch* out);
+void rbsc_graph_batch_free(rbsc_graph_batch* b);
+
+/* One-shot batch refinement: host CSR of the batch in, per-graph results out. */
+rbsc_status rbsc_batch_refine(rbsc_ctx* ctx, const rbsc_csr* graphs, const uint64_t* graph_nodes,
+                              uint32_t num_graphs, const uint32_t* init_colors, rbsc_batch_result* out,
+                              rbsc_stats* stats);
+/* The same on a resident graph holding the batch (rbsc_graph_upload). */
+rbsc_status rbsc_graph_batch_refine(rbsc_ctx* ctx, rbsc_graph* g, const uint64_t* graph_nodes,
+                                    uint32_t num_graphs, const uint32_t* init_colors,
+                                    rbsc_batch_result* out, rbsc_stats* stats);
+
 /* ---- refinement without device allocation -------------------------------- */
 
 /* No counterpart in the reference (which allocates everything it uses,

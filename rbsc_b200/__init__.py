@@ -27,7 +27,8 @@ from . import _lib
 from ._lib import RELABEL_HASH, RELABEL_SORT, RbscError
 
 __all__ = ["Context", "Graph", "Result", "RbscError", "run", "parse_arcs", "gen_rmat_host",
-           "RELABEL_HASH", "RELABEL_SORT", "degree_bucket_colors"]
+           "RELABEL_HASH", "RELABEL_SORT", "degree_bucket_colors", "gen_wl_batch", "BatchResult",
+           "batch_buffers"]
 
 RMAT_ABC = (0.57, 0.19, 0.19)
 
@@ -159,6 +160,13 @@ class Context:
                                                 None if out is None else out.ctypes.data, ctypes.byref(st)), self._h)
         return _result(st, None if out is None else out[: c.n])
 
+    def batch_refine(self, off, idx, graph_nodes, init=None, out=None) -> BatchResult:
+        """One-shot refinement of a batch of graphs side by side
+        (rbsc_batch_refine).  `out`: optional arrays from batch_buffers."""
+        c, keep = _csr(off, idx, None)
+        return _batch_call(lambda *a: _check(self._lib, self._lib.rbsc_batch_refine(self._h, ctypes.byref(c), *a), self._h),
+                           int(c.n), graph_nodes, init, out)
+
     def upload(self, off, idx, wt=None) -> "Graph":
         c, keep = _csr(off, idx, wt)
         h = ctypes.c_void_p()
@@ -213,6 +221,13 @@ class Graph:
         _check(lib, lib.rbsc_graph_refine(self.ctx._h, self._h, None if init_a is None else init_a.ctypes.data,
                                           None if out is None else out.ctypes.data, ctypes.byref(st)), self.ctx._h)
         return _result(st, None if out is None else out[: self.n])
+
+    def batch_refine(self, graph_nodes, init=None, out=None) -> BatchResult:
+        """This resident graph holds a batch of graphs side by side
+        (rbsc_graph_batch_refine).  `out`: optional arrays from batch_buffers."""
+        lib = self.ctx._lib
+        return _batch_call(lambda *a: _check(lib, lib.rbsc_graph_batch_refine(self.ctx._h, self._h, *a), self.ctx._h),
+                           self.n, graph_nodes, init, out)
 
     def refine_device(self, d_init: int | None = None, d_out: int | None = None) -> Result:
         """Refinement with device-resident initial colours / labels (raw
@@ -278,6 +293,73 @@ def gen_rmat_host(scale: int, edge_factor: int, a=RMAT_ABC[0], b=RMAT_ABC[1], c=
     _check(lib, lib.rbsc_gen_rmat_host(scale, edge_factor, a, b, c, seed, threads, ctypes.byref(hg)), None)
     off, idx, _ = _host_graph_to_numpy(lib, hg)
     return off, idx
+
+
+def gen_wl_batch(num_graphs: int, nmin: int = 10, nmax: int = 500, num_labels: int = 8, seed: int = 1,
+                 threads: int = 0):
+    """The small-graph batch (rbsc_gen_wl_batch): (offsets uint64, indices
+    uint32, graph_nodes uint64[num_graphs+1], labels uint32) of the graphs side
+    by side over global node ids."""
+    lib = _lib.load()
+    b = _lib.GraphBatch()
+    _check(lib, lib.rbsc_gen_wl_batch(num_graphs, nmin, nmax, num_labels, seed, threads, ctypes.byref(b)), None)
+    try:
+        n, m, G = int(b.csr.n), int(b.csr.m), int(b.num_graphs)
+        off = np.ctypeslib.as_array(b.csr.offsets, shape=(n + 1,)).copy()
+        idx = np.ctypeslib.as_array(b.csr.indices, shape=(max(m, 1),))[:m].copy()
+        gn = np.ctypeslib.as_array(b.graph_nodes, shape=(G + 1,)).copy()
+        labels = np.ctypeslib.as_array(b.labels, shape=(max(n, 1),))[:n].copy()
+    finally:
+        lib.rbsc_graph_batch_free(ctypes.byref(b))
+    return off, idx, gn, labels
+
+
+@dataclass
+class BatchResult:
+    """Per-graph results of a batch refinement (rbsc_batch_result)."""
+    colors: np.ndarray        # shared colour of every node (smallest global node id of its class)
+    local: np.ndarray         # smallest local node id of each node's block in its own graph
+    blocks: np.ndarray        # blocks per graph
+    fingerprint: np.ndarray   # 64-bit digest of each graph's colour histogram
+    hist_offsets: np.ndarray  # histogram entries of each graph
+    hist_colors: np.ndarray
+    hist_counts: np.ndarray
+    stats: Result
+
+    def histogram(self, g: int):
+        a, b = int(self.hist_offsets[g]), int(self.hist_offsets[g + 1])
+        return self.hist_colors[a:b], self.hist_counts[a:b]
+
+
+_BATCH_FIELDS = (("colors", "n", np.uint32), ("local", "n", np.uint32), ("blocks", "G", np.uint32),
+                 ("fingerprint", "G", np.uint64), ("hist_offsets", "G1", np.uint64), ("hist_colors", "n", np.uint32),
+                 ("hist_counts", "n", np.uint32))
+
+
+def batch_buffers(n: int, num_graphs: int, alloc=np.empty) -> dict:
+    """Output arrays for a batch refinement of n nodes in num_graphs graphs;
+    `alloc(shape, dtype)` may return pinned memory (e.g. a view of a pinned
+    torch tensor) for faster copies."""
+    size = {"n": max(n, 1), "G": max(num_graphs, 1), "G1": num_graphs + 1}
+    return {k: alloc(size[s], dt) for k, s, dt in _BATCH_FIELDS}
+
+
+def _batch_call(fn, n: int, graph_nodes, init, out=None):
+    gn = np.ascontiguousarray(graph_nodes, dtype=np.uint64)
+    G = len(gn) - 1
+    init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+    arrs = out if out is not None else batch_buffers(n, G)
+    for k, s, dt in _BATCH_FIELDS:
+        need = {"n": n, "G": G, "G1": G + 1}[s]
+        a = arrs[k]
+        assert a.dtype == dt and a.flags.c_contiguous and a.size >= need, k
+    out = _lib.BatchResult(*(arrs[k].ctypes.data for k in ("colors", "local", "blocks", "fingerprint", "hist_offsets",
+                                                            "hist_colors", "hist_counts")))
+    st = _lib.Stats()
+    fn(gn.ctypes.data, G, None if init_a is None else init_a.ctypes.data, ctypes.byref(out), ctypes.byref(st))
+    H = int(arrs["hist_offsets"][G])
+    return BatchResult(arrs["colors"][:n], arrs["local"][:n], arrs["blocks"][:G], arrs["fingerprint"][:G],
+                       arrs["hist_offsets"], arrs["hist_colors"][:H], arrs["hist_counts"][:H], _result(st, None))
 
 
 def degree_bucket_colors(off) -> np.ndarray:

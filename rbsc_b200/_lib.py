@@ -35,6 +35,7 @@ EXPORTED = [
     "rbsc_graph_info", "rbsc_graph_device_csr", "rbsc_graph_refine", "rbsc_graph_refine_device",
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
+    "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
 ]
 
 NOALLOC_MAX_NODES = 16384
@@ -124,6 +125,27 @@ class HostGraph(ctypes.Structure):
     ]
 
 
+class GraphBatch(ctypes.Structure):
+    _fields_ = [
+        ("num_graphs", ctypes.c_uint32),
+        ("graph_nodes", ctypes.POINTER(ctypes.c_uint64)),
+        ("labels", ctypes.POINTER(ctypes.c_uint32)),
+        ("csr", HostGraph),
+    ]
+
+
+class BatchResult(ctypes.Structure):
+    _fields_ = [
+        ("colors", ctypes.c_void_p),
+        ("local", ctypes.c_void_p),
+        ("blocks", ctypes.c_void_p),
+        ("fingerprint", ctypes.c_void_p),
+        ("hist_offsets", ctypes.c_void_p),
+        ("hist_colors", ctypes.c_void_p),
+        ("hist_counts", ctypes.c_void_p),
+    ]
+
+
 _lib = None
 
 
@@ -160,12 +182,19 @@ def load():
     lib.rbsc_refine_noalloc.argtypes = [P(Csr), vp, vp, vp, P(Opts), vp]
     lib.rbsc_parse_arcs.argtypes = [ctypes.c_char_p, ctypes.c_size_t, P(HostGraph)]
     lib.rbsc_host_graph_free.argtypes = [P(HostGraph)]
+    lib.rbsc_gen_wl_batch.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint64,
+                                      ctypes.c_int32, P(GraphBatch)]
+    lib.rbsc_graph_batch_free.argtypes = [P(GraphBatch)]
+    lib.rbsc_graph_batch_free.restype = None
+    lib.rbsc_batch_refine.argtypes = [vp, P(Csr), vp, ctypes.c_uint32, vp, P(BatchResult), P(Stats)]
+    lib.rbsc_graph_batch_refine.argtypes = [vp, vp, vp, ctypes.c_uint32, vp, P(BatchResult), P(Stats)]
     lib.rbsc_gen_rmat_device.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_uint64, P(vp)]
     lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
     for name in EXPORTED:
         if name not in ("rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
+                        "rbsc_graph_batch_free",
                         "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):
             getattr(lib, name).restype = ctypes.c_int32
     _lib = lib
