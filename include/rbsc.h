@@ -95,6 +95,9 @@ typedef struct {
     uint64_t kernel_launches; /* kernels of this library launched by the call            */
     double init_ms;           /* device time: initial colours + active-set setup          */
     double loop_ms;           /* device time: the signature passes (all rounds)          */
+    double first_signature_ms;   /* k_signature of the first pass, when launched from the
+                                    host (few initial classes), else 0                    */
+    uint64_t first_signature_arcs; /* arcs that launch processed                         */
 } rbsc_stats;
 
 /* Per-kernel device time of one refinement, measured with CUDA events around

@@ -56,6 +56,8 @@ class Result:
     kernel_launches: int = 0
     init_ms: float = 0.0
     loop_ms: float = 0.0
+    first_signature_ms: float = 0.0
+    first_signature_arcs: int = 0
 
 
 def _result(st: _lib.Stats, labels) -> Result:
@@ -63,7 +65,8 @@ def _result(st: _lib.Stats, labels) -> Result:
     return Result(labels, int(st.blocks), int(st.rounds), int(st.done), int(st.verified), int(st.repairs),
                   int(st.initial_blocks), float(st.time_s), float(st.device_ms), float(st.verify_ms),
                   float(st.h2d_ms), float(st.d2h_ms), int(st.h2d_bytes), int(st.d2h_bytes), rb,
-                  int(st.kernel_launches), float(st.init_ms), float(st.loop_ms))
+                  int(st.kernel_launches), float(st.init_ms), float(st.loop_ms), float(st.first_signature_ms),
+                  int(st.first_signature_arcs))
 
 
 def _check(lib, status: int, ctx=None):

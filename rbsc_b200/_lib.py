@@ -74,6 +74,8 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_uint64),
         ("init_ms", ctypes.c_double),
         ("loop_ms", ctypes.c_double),
+        ("first_signature_ms", ctypes.c_double),
+        ("first_signature_arcs", ctypes.c_uint64),
     ]
 
 

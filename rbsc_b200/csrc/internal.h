@@ -29,6 +29,7 @@ struct rbsc_ctx {
     rbsc_opts opts{};
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
+    cudaEvent_t ev_sig[2] = {};  // around the host-launched first signature kernel
     int sm_count = 148;
     std::string err;
 };
@@ -106,6 +107,8 @@ struct rbsc_graph {
     cudaGraphExec_t loop_exec = nullptr;
     int loop_relabel = -1;
     int loop_no_persist = -1;
+    float first_sig_ms = 0.f;       // the last refinement's first signature kernel
+    uint64_t first_sig_arcs = 0;
     uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop
 };
 
