@@ -333,6 +333,7 @@ def run_ours(args, rank, world, local_rank):
            "path": "rbsc_refine (C ABI): pinned host CSR + colours in, labels out"}
 
     batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
+    served = None if args.serve_requests <= 0 else run_served(args, world, dist, local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -346,7 +347,8 @@ def run_ours(args, rank, world, local_rank):
                 "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "batched": batched}
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "batched": batched,
+                "served": served}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -441,6 +443,107 @@ def run_batched(args, ctx, world, dist):
                       "per_launch_resident": "rbsc_graph_refine per uploaded graph (each refined once before)"}}
 
 
+def served_pool(args):
+    """Distinct graphs of the served mix, generated on the host off the clock:
+    arcs log-uniform in [1e3, 5e7], kinds in turn a random lift (x32 of an
+    Erdos-Renyi base of mean degree 8), R-MAT (a, b, c as the main workload,
+    edge factor about 16) and Erdos-Renyi (mean degree 8); int32 heads."""
+    import rbsc_b200 as R
+    rng = np.random.default_rng(args.seed + 77)
+    pool = []
+    for k in range(args.serve_pool):
+        e = float(np.exp(rng.uniform(np.log(1e3), np.log(5e7))))
+        seed = args.seed * 1000 + k
+        if k % 3 == 0:
+            off, idx = R.gen_lift_host(max(2, int(round(e / (8 * 32)))), 8.0, 32, seed=seed)
+            kind = "lift"
+        elif k % 3 == 1:
+            scale = max(4, int(round(np.log2(e / 16))))
+            off, idx = R.gen_rmat_host(scale, max(1, int(round(e / 2 ** scale))), seed=seed)
+            kind = "rmat"
+        else:
+            off, idx = R.gen_er_host(max(2, int(e / 8)), 8.0, seed=seed)
+            kind = "er"
+        pool.append((kind, _pinned_copy(off), _pinned_copy(idx)))
+    return pool
+
+
+def run_served(args, world, dist, local_rank):
+    """Served refinement (the served-stream configuration): a Poisson stream of
+    requests drawn from a pool of seeded graphs, through a server with
+    continuous batching (several slots whose work overlaps on the GPU,
+    admission by device footprint, small jobs packed into one batch
+    refinement) against the same stream through a server with one slot and no
+    packing (one graph per launch, in arrival order).  Latency = submit to
+    labels in host memory; every partition is checked against a refinement
+    of the same graph alone."""
+    import torch
+    import rbsc_b200 as R
+    pool = served_pool(args)
+    rng = np.random.default_rng(args.seed + 99)
+    N = args.serve_requests
+    pick = rng.integers(0, len(pool), size=N)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, size=N))
+    ref = {}
+    with R.Context(local_rank) as c:
+        for k in sorted(set(pick.tolist())):
+            _, off, idx = pool[k]
+            ref[k] = c.refine(off, idx)
+
+    def start(slots, pack):
+        kw = dict(slots=slots) if pack else dict(slots=slots, pack_max_graphs=1)
+        srv = R.Server(local_rank, **kw)
+        for _ in range(2):   # every slot's buffer pool warmed on every pool graph
+            ids = [srv.submit(off, idx) for _, off, idx in pool]
+            for j in ids:
+                srv.wait(j)
+        return srv
+
+    def run(srv, poisson):
+        st0 = srv.stats()
+        ids = []
+        t0 = time.perf_counter()
+        for i in range(N):
+            if poisson:
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+            _, off, idx = pool[pick[i]]
+            ids.append(srv.submit(off, idx))
+        res = [srv.wait(j) for j in ids]
+        span = time.perf_counter() - t0
+        st = srv.stats()
+        for i, r in enumerate(res):
+            a = ref[int(pick[i])]
+            assert r.status == 0 and r.blocks == a.blocks and np.array_equal(r.labels, a.labels), r.error
+        lat = np.array([r.latency_ms for r in res])
+        q = np.array([r.queue_ms for r in res])
+        sv = np.array([r.service_ms for r in res])
+        dec = np.array_split(lat, 10)
+        return {"graphs_per_s": N / span, "span_s": span, "p50_ms": float(np.percentile(lat, 50)),
+                "p99_ms": float(np.percentile(lat, 99)), "mean_ms": float(lat.mean()),
+                "queue_ms_mean": float(q.mean()), "service_ms_mean": float(sv.mean()),
+                "service_ms_p50": float(np.percentile(sv, 50)), "service_ms_p99": float(np.percentile(sv, 99)),
+                "latency_mean_by_arrival_decile_ms": [float(d.mean()) for d in dec],
+                "packed_jobs": st["packed_jobs"] - st0["packed_jobs"], "executions": st["batches"] - st0["batches"],
+                "peak_busy_slots": st["peak_busy_slots"], "peak_reserved_bytes": st["peak_reserved"]}
+
+    with start(args.serve_slots, True) as srv:
+        served, served_sat = run(srv, True), run(srv, False)
+    with start(1, False) as srv:
+        serial, serial_sat = run(srv, True), run(srv, False)
+    out = {"workload": f"Poisson stream at {args.serve_rate:g} req/s, {N} requests drawn uniformly from "
+                       f"{len(pool)} seeded graphs: arcs log-uniform in [1e3, 5e7], kinds in turn random lift x32 / "
+                       f"R-MAT / Erdos-Renyi, uniform initial colours",
+           "requests": N, "pool_arcs": [int(len(p[2])) for p in pool],
+           "served": served, "serial": serial, "served_saturated": served_sat, "serial_saturated": serial_sat,
+           "slots": args.serve_slots, "bit_exact": True,
+           "paths": {"served": "rbsc_serve_submit / rbsc_serve_wait: several slots, packing, footprint admission",
+                     "serial": "the same server with one slot and no packing: one rbsc_refine per request in order"}}
+    out["saturated_speedup"] = out["served_saturated"]["graphs_per_s"] / out["serial_saturated"]["graphs_per_s"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -456,6 +559,10 @@ def main():
     ap.add_argument("--batch-graphs", type=int, default=100000, help="small-graph batch size (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-sample", type=int, default=1000, help="graphs refined one call each")
+    ap.add_argument("--serve-requests", type=int, default=600, help="served stream length (0: skip)")
+    ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
+    ap.add_argument("--serve-pool", type=int, default=48, help="distinct graphs the requests draw from")
+    ap.add_argument("--serve-slots", type=int, default=2)
     ap.add_argument("--no-persist", action="store_true",
                     help="every pass as separate launches (no persistent kernel for small active sets)")
     ap.add_argument("--profile-refine", action="store_true",

@@ -216,6 +216,16 @@ rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_fa
 rbsc_status rbsc_gen_rmat_host(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
                                uint64_t seed, int32_t threads, rbsc_host_graph* out);
 
+/* Directed Erdos-Renyi G(n, p), p = mean_degree / (n - 1), no self-loops,
+ * rows sorted; and its random lift: every node copied `lift` times, every
+ * arc (u, v) of a G(base_n, p) base becoming the arcs (u*lift + i,
+ * v*lift + pi(i)) for a uniform permutation pi per base arc.  Counter-based:
+ * the same arguments give the same graph for any thread count.  Free with
+ * rbsc_host_graph_free. */
+rbsc_status rbsc_gen_er_host(uint32_t n, double mean_degree, uint64_t seed, int32_t threads, rbsc_host_graph* out);
+rbsc_status rbsc_gen_lift_host(uint32_t base_n, double mean_degree, uint32_t lift, uint64_t seed, int32_t threads,
+                               rbsc_host_graph* out);
+
 /* ---- batches of small graphs (no reference counterpart) ------------------
  * Many graphs side by side in one CSR over global node ids (no arc between
  * two graphs), graph i owning nodes [graph_nodes[i], graph_nodes[i+1]).  They
@@ -261,6 +271,94 @@ rbsc_status rbsc_batch_refine(rbsc_ctx* ctx, const rbsc_csr* graphs, const uint6
 rbsc_status rbsc_graph_batch_refine(rbsc_ctx* ctx, rbsc_graph* g, const uint64_t* graph_nodes,
                                     uint32_t num_graphs, const uint32_t* init_colors,
                                     rbsc_batch_result* out, rbsc_stats* stats);
+
+/* ---- serving: continuous batching of refinement jobs ---------------------
+ * No counterpart in the reference, which refines one graph per process run
+ * (rbsc.cu:182-497).  A server owns `slots` executors on one device, each a
+ * context with its own stream and host thread, so the jobs of different slots
+ * overlap on the GPU.  Jobs are admitted in arrival order as a slot and device
+ * memory free up: a job is started only while the estimated device footprint
+ * of all running work stays within `hbm_budget` (rbsc_serve_footprint).  When
+ * the oldest waiting job is small (at most pack_max_arcs arcs, unweighted),
+ * it is started together with the other small jobs waiting behind it, up to
+ * pack_max_graphs jobs and pack_arc_budget arcs, as one batch refinement of
+ * their disjoint union (rbsc_batch_refine): every job still gets exactly the
+ * labels and block count a refinement of its graph alone gives.
+ *
+ * A job's host buffers (CSR, initial colours, output labels) belong to the
+ * caller and must stay valid and unchanged until the job's result has been
+ * collected by rbsc_serve_poll or rbsc_serve_wait (each result is handed out
+ * once).  Every call is thread-safe. */
+#define RBSC_PENDING 1               /* serving: the job has not finished yet    */
+
+typedef struct rbsc_server rbsc_server;
+
+typedef struct {
+    int32_t device;
+    uint32_t slots;           /* executors (contexts / streams / host threads), 0 = 2 */
+    uint64_t hbm_budget;      /* bytes of device memory running work may take;
+                                 0 = half of the device's free memory at creation     */
+    uint64_t pack_max_arcs;   /* jobs of at most this many arcs are packed, 0 = 2^18  */
+    uint32_t pack_max_graphs; /* jobs per packed batch, 0 = 4096; 1 = never pack      */
+    uint64_t pack_arc_budget; /* arcs (and nodes) per packed batch, 0 = 2^22          */
+    uint32_t queue_cap;       /* jobs waiting to start, 0 = 65536; submit beyond
+                                 returns RBSC_ERR_BUSY                                */
+    rbsc_opts opts;           /* refinement options of every job (no_persist is forced
+                                 on: a cooperative grid must not share the GPU with
+                                 the other slots' kernels)                            */
+    int32_t dry_run;          /* TEST HOOK: 1 = no GPU work at all; each job "runs" for
+                                 dry_run_ns_per_arc * arcs + 20 us of host sleep and
+                                 writes no labels (exercises admission and packing)   */
+    uint32_t dry_run_ns_per_arc;
+} rbsc_serve_opts;
+
+typedef struct {
+    int32_t status;           /* RBSC_OK or the job's error                            */
+    uint32_t blocks;          /* blocks of the job's partition                         */
+    uint32_t rounds;          /* passes of the refinement that ran it (for a packed job,
+                                 the passes of the whole batch)                        */
+    uint32_t packed;          /* jobs in the batch it ran in (1 = alone)               */
+    uint32_t slot;            /* executor that ran it                                  */
+    uint32_t pad;
+    uint64_t footprint;       /* device bytes admitted for its batch                   */
+    double queue_ms;          /* submit -> start                                        */
+    double service_ms;        /* start -> labels in host memory                          */
+    double latency_ms;        /* submit -> finished                                      */
+    char error[128];          /* message when status != RBSC_OK                         */
+} rbsc_serve_result;
+
+typedef struct {
+    uint64_t submitted, completed, failed, rejected;
+    uint64_t batches;         /* executions started (packs and single jobs)            */
+    uint64_t packed_jobs;     /* jobs that ran inside a pack of two or more            */
+    uint64_t queued, running; /* now                                                   */
+    uint64_t reserved;        /* admitted footprint of running work, now               */
+    uint64_t peak_reserved;   /* its maximum so far                                    */
+    uint32_t peak_busy_slots; /* most slots busy at once                               */
+    uint32_t slots;
+    uint64_t hbm_budget;
+} rbsc_serve_stats;
+
+void rbsc_serve_opts_default(rbsc_serve_opts* opts);
+/* Device bytes the server reserves for a refinement of `graphs` graphs with n
+ * nodes and m arcs in total (an upper estimate of what the refinement
+ * allocates). */
+uint64_t rbsc_serve_footprint(uint64_t n, uint64_t m, int32_t weighted, uint32_t graphs);
+rbsc_status rbsc_serve_create(const rbsc_serve_opts* opts, rbsc_server** out);
+/* Finishes the running work, cancels the waiting jobs and frees everything. */
+void rbsc_serve_destroy(rbsc_server* srv);
+const char* rbsc_serve_last_error(const rbsc_server* srv);
+/* Queues a job.  init_colors: NULL or n colours; out_labels: NULL or n uint32
+ * (canonical labels).  RBSC_ERR_TOO_LARGE when the job alone exceeds the
+ * budget, RBSC_ERR_BUSY when the queue is full. */
+rbsc_status rbsc_serve_submit(rbsc_server* srv, const rbsc_csr* host_graph, const uint32_t* init_colors,
+                              uint32_t* out_labels, uint64_t* job_id);
+/* RBSC_OK (result filled, job released), RBSC_PENDING, or RBSC_ERR_INVALID
+ * for an unknown job. */
+rbsc_status rbsc_serve_poll(rbsc_server* srv, uint64_t job_id, rbsc_serve_result* result);
+/* Like poll, waiting up to timeout_ms (< 0: no limit). */
+rbsc_status rbsc_serve_wait(rbsc_server* srv, uint64_t job_id, int64_t timeout_ms, rbsc_serve_result* result);
+rbsc_status rbsc_serve_stats_get(rbsc_server* srv, rbsc_serve_stats* stats);
 
 /* ---- refinement without device allocation -------------------------------- */
 

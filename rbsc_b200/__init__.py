@@ -28,7 +28,7 @@ from ._lib import RELABEL_HASH, RELABEL_SORT, RbscError
 
 __all__ = ["Context", "Graph", "Result", "RbscError", "run", "parse_arcs", "gen_rmat_host",
            "RELABEL_HASH", "RELABEL_SORT", "degree_bucket_colors", "gen_wl_batch", "BatchResult",
-           "batch_buffers"]
+           "batch_buffers", "gen_er_host", "gen_lift_host", "Server", "ServeResult", "serve_footprint"]
 
 RMAT_ABC = (0.57, 0.19, 0.19)
 
@@ -317,6 +317,26 @@ def gen_wl_batch(num_graphs: int, nmin: int = 10, nmax: int = 500, num_labels: i
     return off, idx, gn, labels
 
 
+def gen_er_host(n: int, mean_degree: float, seed: int = 1, threads: int = 0):
+    """Directed Erdos-Renyi G(n, mean_degree / (n-1)) without self-loops
+    (rbsc_gen_er_host): (offsets uint64, indices uint32)."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    _check(lib, lib.rbsc_gen_er_host(n, float(mean_degree), seed, threads, ctypes.byref(hg)), None)
+    off, idx, _ = _host_graph_to_numpy(lib, hg)
+    return off, idx
+
+
+def gen_lift_host(base_n: int, mean_degree: float, lift: int, seed: int = 1, threads: int = 0):
+    """Random lift of a directed Erdos-Renyi base graph (rbsc_gen_lift_host):
+    (offsets uint64, indices uint32) of base_n * lift nodes."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    _check(lib, lib.rbsc_gen_lift_host(base_n, float(mean_degree), lift, seed, threads, ctypes.byref(hg)), None)
+    off, idx, _ = _host_graph_to_numpy(lib, hg)
+    return off, idx
+
+
 @dataclass
 class BatchResult:
     """Per-graph results of a batch refinement (rbsc_batch_result)."""
@@ -363,6 +383,122 @@ def _batch_call(fn, n: int, graph_nodes, init, out=None):
     H = int(arrs["hist_offsets"][G])
     return BatchResult(arrs["colors"][:n], arrs["local"][:n], arrs["blocks"][:G], arrs["fingerprint"][:G],
                        arrs["hist_offsets"], arrs["hist_colors"][:H], arrs["hist_counts"][:H], _result(st, None))
+
+
+@dataclass
+class ServeResult:
+    """The result of one served job (rbsc_serve_result)."""
+    labels: np.ndarray | None
+    status: int
+    blocks: int
+    rounds: int
+    packed: int          # jobs in the batch it ran in (1 = alone)
+    slot: int
+    footprint: int
+    queue_ms: float
+    service_ms: float
+    latency_ms: float
+    error: str
+
+
+def serve_footprint(n: int, m: int, weighted: bool = False, graphs: int = 1) -> int:
+    """Device bytes a server reserves for a refinement (rbsc_serve_footprint)."""
+    return int(_lib.load().rbsc_serve_footprint(n, m, 1 if weighted else 0, graphs))
+
+
+class Server:
+    """Refinement service with continuous batching (rbsc_serve_*): `slots`
+    executors on one device, admission by device footprint within
+    `hbm_budget`, small jobs packed into one batch refinement.  The arrays of
+    a submitted job are kept alive here until its result is collected."""
+
+    def __init__(self, device: int = 0, slots: int = 2, hbm_budget: int = 0, pack_max_arcs: int = 0,
+                 pack_max_graphs: int = 0, pack_arc_budget: int = 0, queue_cap: int = 0, verify: bool = True,
+                 seed: int | None = None, dry_run_ns_per_arc: int | None = None):
+        self._lib = _lib.load()
+        o = _lib.ServeOpts()
+        self._lib.rbsc_serve_opts_default(ctypes.byref(o))
+        o.device, o.slots, o.hbm_budget = device, slots, hbm_budget
+        o.pack_max_arcs, o.pack_max_graphs, o.pack_arc_budget, o.queue_cap = (pack_max_arcs, pack_max_graphs,
+                                                                              pack_arc_budget, queue_cap)
+        o.opts.verify = 1 if verify else 0
+        if seed is not None:
+            o.opts.seed = seed
+        if dry_run_ns_per_arc is not None:
+            o.dry_run, o.dry_run_ns_per_arc = 1, dry_run_ns_per_arc
+        h = ctypes.c_void_p()
+        st = self._lib.rbsc_serve_create(ctypes.byref(o), ctypes.byref(h))
+        if st != _lib.RBSC_OK:
+            raise RbscError(st, self._lib.rbsc_serve_last_error(None).decode())
+        self._h = h
+        self._keep = {}
+
+    def _fail(self, st):
+        raise RbscError(st, self._lib.rbsc_serve_last_error(self._h).decode())
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.rbsc_serve_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, off, idx, wt=None, init=None, labels: bool = True) -> int:
+        """Queues a job; returns its id.  Raises RbscError with RBSC_ERR_BUSY
+        (-8) when the queue is full and RBSC_ERR_TOO_LARGE (-7) when the job
+        exceeds the budget."""
+        c, keep = _csr(off, idx, wt)
+        init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+        out = np.zeros(max(c.n, 1), dtype=np.uint32) if labels else None
+        jid = ctypes.c_uint64()
+        st = self._lib.rbsc_serve_submit(self._h, ctypes.byref(c), None if init_a is None else init_a.ctypes.data,
+                                         None if out is None else out.ctypes.data, ctypes.byref(jid))
+        if st != _lib.RBSC_OK:
+            self._fail(st)
+        self._keep[jid.value] = (c, keep, init_a, out)
+        return int(jid.value)
+
+    def _collect(self, jid: int, r: _lib.ServeResult) -> ServeResult:
+        c, _, _, out = self._keep.pop(jid)
+        return ServeResult(None if out is None else out[: c.n], int(r.status), int(r.blocks), int(r.rounds),
+                           int(r.packed), int(r.slot), int(r.footprint), float(r.queue_ms), float(r.service_ms),
+                           float(r.latency_ms), r.error.decode(errors="replace"))
+
+    def poll(self, jid: int) -> ServeResult | None:
+        r = _lib.ServeResult()
+        st = self._lib.rbsc_serve_poll(self._h, jid, ctypes.byref(r))
+        if st == _lib.RBSC_PENDING:
+            return None
+        if st != _lib.RBSC_OK:
+            self._fail(st)
+        return self._collect(jid, r)
+
+    def wait(self, jid: int, timeout_ms: int = -1) -> ServeResult | None:
+        r = _lib.ServeResult()
+        st = self._lib.rbsc_serve_wait(self._h, jid, timeout_ms, ctypes.byref(r))
+        if st == _lib.RBSC_PENDING:
+            return None
+        if st != _lib.RBSC_OK:
+            self._fail(st)
+        return self._collect(jid, r)
+
+    def stats(self) -> dict:
+        s = _lib.ServeStats()
+        st = self._lib.rbsc_serve_stats_get(self._h, ctypes.byref(s))
+        if st != _lib.RBSC_OK:
+            self._fail(st)
+        return {k: int(getattr(s, k)) for k, _ in _lib.ServeStats._fields_}
 
 
 def degree_bucket_colors(off) -> np.ndarray:

@@ -23,7 +23,9 @@ STATUS_NAMES = {
     -6: "RBSC_ERR_PARSE",
     -7: "RBSC_ERR_TOO_LARGE",
     -8: "RBSC_ERR_BUSY",
+    1: "RBSC_PENDING",
 }
+RBSC_PENDING = 1
 
 RELABEL_HASH = 0
 RELABEL_SORT = 1
@@ -36,6 +38,9 @@ EXPORTED = [
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
+    "rbsc_gen_er_host", "rbsc_gen_lift_host",
+    "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
+    "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
 
 NOALLOC_MAX_NODES = 16384
@@ -148,6 +153,55 @@ class BatchResult(ctypes.Structure):
     ]
 
 
+class ServeOpts(ctypes.Structure):
+    _fields_ = [
+        ("device", ctypes.c_int32),
+        ("slots", ctypes.c_uint32),
+        ("hbm_budget", ctypes.c_uint64),
+        ("pack_max_arcs", ctypes.c_uint64),
+        ("pack_max_graphs", ctypes.c_uint32),
+        ("pack_arc_budget", ctypes.c_uint64),
+        ("queue_cap", ctypes.c_uint32),
+        ("opts", Opts),
+        ("dry_run", ctypes.c_int32),
+        ("dry_run_ns_per_arc", ctypes.c_uint32),
+    ]
+
+
+class ServeResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int32),
+        ("blocks", ctypes.c_uint32),
+        ("rounds", ctypes.c_uint32),
+        ("packed", ctypes.c_uint32),
+        ("slot", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
+        ("footprint", ctypes.c_uint64),
+        ("queue_ms", ctypes.c_double),
+        ("service_ms", ctypes.c_double),
+        ("latency_ms", ctypes.c_double),
+        ("error", ctypes.c_char * 128),
+    ]
+
+
+class ServeStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_uint64),
+        ("completed", ctypes.c_uint64),
+        ("failed", ctypes.c_uint64),
+        ("rejected", ctypes.c_uint64),
+        ("batches", ctypes.c_uint64),
+        ("packed_jobs", ctypes.c_uint64),
+        ("queued", ctypes.c_uint64),
+        ("running", ctypes.c_uint64),
+        ("reserved", ctypes.c_uint64),
+        ("peak_reserved", ctypes.c_uint64),
+        ("peak_busy_slots", ctypes.c_uint32),
+        ("slots", ctypes.c_uint32),
+        ("hbm_budget", ctypes.c_uint64),
+    ]
+
+
 _lib = None
 
 
@@ -194,8 +248,25 @@ def load():
                                          ctypes.c_double, ctypes.c_uint64, P(vp)]
     lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_gen_er_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_gen_lift_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
+                                       ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_serve_opts_default.argtypes = [P(ServeOpts)]
+    lib.rbsc_serve_opts_default.restype = None
+    lib.rbsc_serve_footprint.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32]
+    lib.rbsc_serve_footprint.restype = ctypes.c_uint64
+    lib.rbsc_serve_create.argtypes = [P(ServeOpts), P(vp)]
+    lib.rbsc_serve_destroy.argtypes = [vp]
+    lib.rbsc_serve_destroy.restype = None
+    lib.rbsc_serve_last_error.argtypes = [vp]
+    lib.rbsc_serve_last_error.restype = ctypes.c_char_p
+    lib.rbsc_serve_submit.argtypes = [vp, P(Csr), vp, vp, P(ctypes.c_uint64)]
+    lib.rbsc_serve_poll.argtypes = [vp, ctypes.c_uint64, P(ServeResult)]
+    lib.rbsc_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int64, P(ServeResult)]
+    lib.rbsc_serve_stats_get.argtypes = [vp, P(ServeStats)]
     for name in EXPORTED:
-        if name not in ("rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
+        if name not in ("rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_destroy",
+                        "rbsc_serve_last_error","rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
                         "rbsc_graph_batch_free",
                         "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):
             getattr(lib, name).restype = ctypes.c_int32

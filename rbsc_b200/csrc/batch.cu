@@ -235,6 +235,7 @@ extern "C" rbsc_status rbsc_batch_refine(rbsc_ctx* ctx, const rbsc_csr* graphs, 
     rbsc_graph* g = nullptr;
     rbsc_status st = rbsc_graph_upload(ctx, graphs, &g);
     if (st != RBSC_OK) return st;
+    g->oneshot = true;
     st = rbsc_graph_batch_refine(ctx, g, graph_nodes, num_graphs, init_colors, out, stats);
     rbsc_graph_free(g);
     if (st == RBSC_OK && stats) stats->time_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();

@@ -20,6 +20,7 @@ struct MemPool {
     std::multimap<size_t, void*> free_blocks;  // size -> block, not in use
     std::unordered_map<void*, size_t> sizes;   // every block the pool allocated
     size_t cached = 0;                         // bytes in free_blocks
+    size_t cap = (size_t)48 << 30;             // most bytes of unused blocks kept
 };
 
 struct rbsc_ctx {
@@ -110,6 +111,8 @@ struct rbsc_graph {
     float first_sig_ms = 0.f;       // the last refinement's first signature kernel
     uint64_t first_sig_arcs = 0;
     uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop
+    bool oneshot = false;       // refined once and freed (rbsc_refine): capturing and
+                                // instantiating the loop graph would cost more than it saves
 };
 
 rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);

@@ -76,9 +76,6 @@ static size_t pool_round(size_t bytes)
     return (bytes + (2u << 20) - 1) & ~(size_t)((2u << 20) - 1);
 }
 
-// The pool keeps at most this many bytes of unused blocks.
-static constexpr size_t kPoolCacheMax = (size_t)48 << 30;
-
 static void pool_raw_free(MemPool& p, void* b)
 {
     if (p.pinned) cudaFreeHost(b);
@@ -134,7 +131,7 @@ static void pool_free(MemPool& p, void* b)
     p.free_blocks.emplace(it->second, b);
     p.cached += it->second;
     // over the cap: drop the largest unused blocks
-    while (p.cached > kPoolCacheMax && !p.free_blocks.empty()) {
+    while (p.cached > p.cap && !p.free_blocks.empty()) {
         auto last = std::prev(p.free_blocks.end());
         p.cached -= last->first;
         p.sizes.erase(last->second);
@@ -854,7 +851,7 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
 // host-driven loop), until the fixpoint, an error or the hand-off.
 static rbsc_status run_passes(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels)
 {
-    if (ctx->opts.use_graph && !kt) {
+    if (ctx->opts.use_graph && !kt && !g->oneshot) {
         CKS(build_loop_graph(ctx, g));
         const uint32_t r0 = g->h_st->round;
         CK(cudaGraphLaunch(g->loop_exec, ctx->stream));
@@ -1279,6 +1276,7 @@ extern "C" rbsc_status rbsc_refine(rbsc_ctx* ctx, const rbsc_csr* host_graph, co
     double up_ms = 0;
     uint64_t up_bytes = 0;
     CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes));
+    g->oneshot = true;
     rbsc_status st = rbsc_graph_refine(ctx, g, init_colors, out_labels, stats);
     rbsc_graph_free(g);
     if (st == RBSC_OK && stats) {
