@@ -196,6 +196,35 @@ rbsc_status rbsc_graph_profile(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_i
  * computed on the device from the resident offsets. */
 rbsc_status rbsc_graph_degree_colors(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* d_colors);
 
+/* ---- the reference's edge-batch (quotient) mode ----------------------------
+ * rbsc.cu:292-487 (rbsc_aggressive.cu:487 with `aggressive`): when the arcs do
+ * not fit one batch of edge_batch_size arcs, the reference refines each batch
+ * of arcs on its own (its sources in one block, arc-less nodes of batch 0 in
+ * another, every other node alone), gives every batch class a global id,
+ * replaces the graph by its quotient (one representative run per class, heads
+ * renamed, parallel arcs merged with summed weights) and repeats until one
+ * batch holds all arcs (the coarsest partition: done = 1) or the node count
+ * stops shrinking (done = 0, a partition finer than the coarsest one).  This
+ * entry point reproduces that mode: the same `nodes` and `done` as the
+ * reference's program for the same edge_batch_size, every batch refined
+ * exactly on the device.  edge_batch_size 0 = all arcs (one batch).
+ * init colours are not part of this mode (the reference has none).
+ * out_labels (host, n uint32, may be NULL): canonical labels of the final
+ * partition of the input nodes.  stats->blocks = the "nodes" line,
+ * stats->done, stats->time_s (wall), stats->rounds = passes of all batch
+ * refinements. */
+typedef struct {
+    uint32_t iterations;      /* outer (quotient) iterations                         */
+    uint32_t last_batches;    /* batches of the last iteration                       */
+    uint64_t batches_total;   /* batches over all iterations                         */
+    uint64_t local_refinements; /* batches that were refined (non-empty after trimming) */
+    uint64_t last_arcs;       /* arcs of the last quotient graph                      */
+} rbsc_edge_batch_info;
+
+rbsc_status rbsc_refine_edge_batches(rbsc_ctx* ctx, const rbsc_csr* host_graph, uint64_t edge_batch_size,
+                                     int32_t aggressive, uint32_t* out_labels, rbsc_stats* stats,
+                                     rbsc_edge_batch_info* info);
+
 /* ---- input formats (reference: read_graph, rbsc.cu:156-180) -------------- */
 
 /* Parses arcs-cuda text ("N\nM\n" + M lines "u wt v", arcs grouped by u;

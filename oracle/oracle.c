@@ -337,3 +337,170 @@ int orc_refine_rsc(uint32_t n, const uint64_t* off, const uint32_t* idx, const u
     free(w); free(z); free(ord); free(tmp); free(lab);
     return status;
 }
+
+
+/* batches = ceil((double)edge_n / max_batch_edge_n) (rbsc.cu:295) */
+static double ceil_u64_div_double(uint64_t a, uint64_t b)
+{
+    const double q = (double)a / (double)b;
+    const double t = (double)(uint64_t)q;
+    return t < q ? t + 1.0 : t;
+}
+
+/* ceil(new_edge_n / (float)max_batch_edge_n) in single precision
+ * (rbsc_aggressive.cu:487) */
+static float ceilf_u64_div_float(uint64_t a, uint64_t b)
+{
+    const float q = (float)a / (float)b;
+    const float t = (float)(uint64_t)q;
+    return t < q ? t + 1.0f : t;
+}
+
+/* ------------------------------------------------------------------ */
+/* the reference GPU program's edge-batch (quotient) mode              */
+/* ------------------------------------------------------------------ */
+#define ORC_OFF_BATCH 0
+#define ORC_IN_BATCH 1
+#define ORC_DANGLING 2
+#define ORC_NOT_INIT UINT64_MAX
+
+/*
+ * The outer loop of src/rbsc/rbsc.cu:292-487 for one GPU, restated; the stop
+ * test of src/rbsc/rbsc_aggressive.cu:487 when `aggressive` is set.  Each
+ * batch's local refinement (rbsc.cu:346-425: in-batch sources start in one
+ * block, dangling nodes of batch 0 in another, every other node alone;
+ * refined over the batch's arcs to the fixpoint) is computed exactly by
+ * orc_refine_exact instead of by hashed sums.
+ *
+ *   off/idx/wt: the graph; its rows in node order are the reference's arc
+ *     list grouped by start (rbsc.cu:168-180).
+ *   batch: max_batch_edge_n (rbsc.cu:204); 0 = all arcs.
+ *   labels_out[n]: canonical labels of the final partition: each original
+ *     node's class after the last iteration, composed over the iterations.
+ *   blocks_out: new_node_n, the "nodes" line (rbsc.cu:494); done_out: 1 iff
+ *     the last iteration had one batch (rbsc.cu:493); iters_out: iterations.
+ * Returns 0.  A graph without arcs has no batch: blocks 0, done 0, as the
+ * reference prints; its labels are then the coarsest partition (one block).
+ */
+int orc_refine_edge_batches(uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt, uint64_t batch,
+                            int aggressive, uint32_t* labels_out, uint32_t* blocks_out, uint32_t* done_out,
+                            uint32_t* iters_out)
+{
+    const uint64_t E = off[n];
+    uint32_t* es = (uint32_t*)malloc(sizeof(uint32_t) * (E ? E : 1));
+    uint32_t* ee = (uint32_t*)malloc(sizeof(uint32_t) * (E ? E : 1));
+    uint64_t* ew = (uint64_t*)malloc(sizeof(uint64_t) * (E ? E : 1));
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint64_t k = off[u]; k < off[u + 1]; ++k) {
+            es[k] = u;
+            ee[k] = idx[k];
+            ew[k] = wt ? wt[k] : 1u;
+        }
+    size_t nn = n ? n : 1;
+    uint32_t* cls = (uint32_t*)malloc(sizeof(uint32_t) * nn);
+    uint32_t* w = (uint32_t*)malloc(sizeof(uint32_t) * nn);
+    uint8_t* mask = (uint8_t*)malloc(nn);
+    uint32_t* lab = (uint32_t*)malloc(sizeof(uint32_t) * nn);
+    uint32_t* init = (uint32_t*)malloc(sizeof(uint32_t) * nn);
+    uint32_t* label_map = (uint32_t*)malloc(sizeof(uint32_t) * nn);
+    uint64_t* loff = (uint64_t*)malloc(sizeof(uint64_t) * (nn + 1));
+    uint32_t* lidx = (uint32_t*)malloc(sizeof(uint32_t) * (E ? E : 1));
+    uint64_t* lwt = (uint64_t*)malloc(sizeof(uint64_t) * (E ? E : 1));
+    uint64_t* widx = (uint64_t*)malloc(sizeof(uint64_t) * nn);
+    uint8_t* considered = (uint8_t*)malloc(nn);
+    for (uint32_t u = 0; u < n; ++u) cls[u] = u;
+    if (batch == 0) batch = E ? E : 1;
+
+    uint32_t node_n = n, new_node_n = n, iters = 0;
+    uint64_t edge_n = E, new_edge_n = E, batches = 0;
+    do {
+        node_n = new_node_n;
+        edge_n = new_edge_n;
+        new_node_n = 0;
+        batches = (uint64_t)ceil_u64_div_double(edge_n, batch);
+        for (uint32_t i = 0; i < node_n; ++i) w[i] = node_n;
+        for (uint64_t b = 0; b < batches; ++b) {
+            uint64_t bs = b * batch, be = bs + batch < edge_n ? bs + batch : edge_n;
+            for (uint32_t i = 0; i < node_n; ++i) mask[i] = b == 0 ? ORC_DANGLING : ORC_OFF_BATCH;
+            uint64_t nbs = ORC_NOT_INIT, nbe = ORC_NOT_INIT;
+            for (uint64_t i = bs; i < be; ++i) {
+                if ((!i || es[i - 1] != es[i]) && nbs == ORC_NOT_INIT) nbs = i;
+                if (i && nbs != ORC_NOT_INIT && es[i - 1] != es[i]) nbe = i;
+                mask[es[i]] = ORC_IN_BATCH;
+            }
+            if (be == edge_n || es[be] != es[be - 1]) nbe = be;
+            if (nbs == ORC_NOT_INIT || nbe == ORC_NOT_INIT) continue;
+            for (uint64_t i = 0; i < nbs; ++i) mask[es[i]] = ORC_OFF_BATCH;
+            for (uint64_t i = nbe; i < edge_n; ++i) mask[es[i]] = ORC_OFF_BATCH;
+            /* the batch as a CSR over all node_n nodes (rows in node order) */
+            for (uint32_t i = 0; i <= node_n; ++i) loff[i] = 0;
+            for (uint64_t i = nbs; i < nbe; ++i) ++loff[es[i] + 1];
+            for (uint32_t i = 0; i < node_n; ++i) loff[i + 1] += loff[i];
+            for (uint32_t i = 0; i < node_n; ++i) widx[i] = loff[i];
+            for (uint64_t i = nbs; i < nbe; ++i) {
+                const uint64_t p = widx[es[i]]++;
+                lidx[p] = ee[i];
+                lwt[p] = ew[i];
+            }
+            for (uint32_t i = 0; i < node_n; ++i)
+                init[i] = mask[i] == ORC_IN_BATCH ? 0u : (mask[i] == ORC_DANGLING ? 1u : i + 2u);
+            uint32_t r = 0, bl = 0;
+            orc_refine_exact(node_n, loff, lidx, lwt, init, lab, &r, &bl, NULL, node_n + 2);
+            /* fresh global ids in the order the batch's classes first appear (rbsc.cu:427-445) */
+            for (uint32_t i = 0; i < node_n; ++i) label_map[i] = node_n;
+            for (uint32_t i = 0; i < node_n; ++i) {
+                if (!mask[i]) continue;
+                const uint32_t l = lab[i];
+                if (label_map[l] == node_n) label_map[l] = new_node_n++;
+                w[i] = label_map[l];
+            }
+        }
+        if (batches > 1) {
+            /* quotient (rbsc.cu:451-487): one representative run per class,
+             * heads renamed to classes, parallel arcs merged, arc order kept */
+            new_edge_n = 0;
+            uint64_t first_edge_i = 0;
+            uint32_t current_node = 0;
+            int counting = 0;
+            for (uint32_t i = 0; i < node_n; ++i) {
+                widx[i] = edge_n;
+                considered[i] = 0;
+                if (w[i] == node_n) w[i] = new_node_n++;
+            }
+            for (uint64_t i = 0; i < edge_n; ++i) {
+                if (!i || es[i] != current_node) {
+                    current_node = es[i];
+                    counting = !considered[w[current_node]];
+                    first_edge_i = new_edge_n;
+                    considered[w[es[i]]] = 1;
+                }
+                if (counting) {
+                    es[i] = w[es[i]];
+                    ee[i] = w[ee[i]];
+                    if (widx[ee[i]] == edge_n || widx[ee[i]] < first_edge_i) {
+                        es[new_edge_n] = es[i];
+                        ee[new_edge_n] = ee[i];
+                        ew[new_edge_n] = ew[i];
+                        widx[ee[i]] = new_edge_n;
+                        ++new_edge_n;
+                    } else {
+                        ew[widx[ee[i]]] += ew[i];
+                    }
+                }
+            }
+        }
+        if (batches > 0)
+            for (uint32_t u = 0; u < n; ++u) cls[u] = w[cls[u]];
+        ++iters;
+    } while (batches > 1 && node_n > new_node_n &&
+             (!aggressive || (float)batches > ceilf_u64_div_float(new_edge_n, batch)));
+
+    if (batches == 0) for (uint32_t u = 0; u < n; ++u) cls[u] = 0;
+    orc_canonicalize(n, cls, labels_out);
+    *blocks_out = new_node_n;
+    *done_out = batches == 1;
+    *iters_out = iters;
+    free(es); free(ee); free(ew); free(cls); free(w); free(mask); free(lab); free(init); free(label_map);
+    free(loff); free(lidx); free(lwt); free(widx); free(considered);
+    return 0;
+}

@@ -65,6 +65,9 @@ def _load():
         lib.orc_rsc_randomize.restype = ctypes.c_uint64
         lib.orc_write_arcs.argtypes = [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p, _u64p]
         lib.orc_write_arcs.restype = ctypes.c_int
+        lib.orc_refine_edge_batches.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, ctypes.c_uint64, ctypes.c_int,
+                                                _u32p, _u32p, _u32p, _u32p]
+        lib.orc_refine_edge_batches.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -114,6 +117,27 @@ def refine_exact(off, idx, wt=None, init=None, max_rounds: int | None = None) ->
                               ctypes.byref(rounds), ctypes.byref(blocks), _p32(rb), max_rounds)
     return OracleResult(labels[:n].copy(), blocks.value, rounds.value, None,
                         [int(x) for x in rb[: rounds.value + 1]], st)
+
+
+@dataclass
+class EdgeBatchResult:
+    labels: np.ndarray      # canonical labels of the final partition
+    blocks: int             # the reference's "nodes" line (new_node_n)
+    done: int               # 1 iff the last iteration had one batch
+    iterations: int
+
+
+def refine_edge_batches(off, idx, wt=None, batch: int = 0, aggressive: bool = False) -> EdgeBatchResult:
+    """The reference GPU program's edge-batch (quotient) mode, restated with
+    exact local refinements (oracle.c: orc_refine_edge_batches)."""
+    lib = _load()
+    n = len(off) - 1
+    off, idx, wt = _csr(off, idx, wt)
+    labels = np.zeros(max(n, 1), dtype=np.uint32)
+    bl, dn, it = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+    lib.orc_refine_edge_batches(n, _p64(off), _p32(idx), _p64(wt), batch, 1 if aggressive else 0, _p32(labels),
+                                ctypes.byref(bl), ctypes.byref(dn), ctypes.byref(it))
+    return EdgeBatchResult(labels[:n].copy(), bl.value, dn.value, it.value)
 
 
 def refine_rsc(off, idx, wt=None, init=None, max_rounds: int | None = None) -> OracleResult:

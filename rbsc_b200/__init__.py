@@ -163,6 +163,22 @@ class Context:
                                                 None if out is None else out.ctypes.data, ctypes.byref(st)), self._h)
         return _result(st, None if out is None else out[: c.n])
 
+    def refine_edge_batches(self, off, idx, wt=None, edge_batch_size: int = 0, aggressive: bool = False,
+                            labels: bool = True):
+        """The reference's edge-batch (quotient) mode (rbsc_refine_edge_batches):
+        returns (Result, info dict).  Result.blocks / .done are the reference
+        program's "nodes" / "done" lines for this edge_batch_size."""
+        c, keep = _csr(off, idx, wt)
+        out = np.zeros(max(c.n, 1), dtype=np.uint32) if labels else None
+        st = _lib.Stats()
+        info = _lib.EdgeBatchInfo()
+        _check(self._lib, self._lib.rbsc_refine_edge_batches(self._h, ctypes.byref(c), edge_batch_size,
+                                                             1 if aggressive else 0,
+                                                             None if out is None else out.ctypes.data,
+                                                             ctypes.byref(st), ctypes.byref(info)), self._h)
+        return (_result(st, None if out is None else out[: c.n]),
+                {k: int(getattr(info, k)) for k, _ in _lib.EdgeBatchInfo._fields_})
+
     def batch_refine(self, off, idx, graph_nodes, init=None, out=None) -> BatchResult:
         """One-shot refinement of a batch of graphs side by side
         (rbsc_batch_refine).  `out`: optional arrays from batch_buffers."""

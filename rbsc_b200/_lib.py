@@ -38,7 +38,7 @@ EXPORTED = [
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
-    "rbsc_gen_er_host", "rbsc_gen_lift_host",
+    "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches",
     "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
     "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
@@ -153,6 +153,16 @@ class BatchResult(ctypes.Structure):
     ]
 
 
+class EdgeBatchInfo(ctypes.Structure):
+    _fields_ = [
+        ("iterations", ctypes.c_uint32),
+        ("last_batches", ctypes.c_uint32),
+        ("batches_total", ctypes.c_uint64),
+        ("local_refinements", ctypes.c_uint64),
+        ("last_arcs", ctypes.c_uint64),
+    ]
+
+
 class ServeOpts(ctypes.Structure):
     _fields_ = [
         ("device", ctypes.c_int32),
@@ -251,6 +261,7 @@ def load():
     lib.rbsc_gen_er_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
     lib.rbsc_gen_lift_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
                                        ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_refine_edge_batches.argtypes = [vp, P(Csr), ctypes.c_uint64, ctypes.c_int32, vp, P(Stats), P(EdgeBatchInfo)]
     lib.rbsc_serve_opts_default.argtypes = [P(ServeOpts)]
     lib.rbsc_serve_opts_default.restype = None
     lib.rbsc_serve_footprint.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32]

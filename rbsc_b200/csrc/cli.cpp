@@ -8,16 +8,21 @@
 // number of blocks.  On failure a message goes to stdout and the exit code is
 // EXIT_FAILURE, as the reference's CHECK_* macros do (rbsc.cu:15-47).
 //
-// edge_batch_size: accepted for compatibility.  The whole graph is refined in
-// device memory whatever its value (the result is always the coarsest
-// partition, done = 1).  gpus: accepted; one process drives one GPU (device 0
-// unless RBSC_DEVICE is set).
+// edge_batch_size: as in the reference.  At least M (or absent): one batch,
+// the coarsest partition (done = 1).  Below M: the reference's edge-batch
+// (quotient) mode, rbsc.cu:292-487, with the same `done` and `nodes` as the
+// reference's program prints (rbsc_refine_edge_batches).  gpus: accepted; one
+// process drives one GPU (device 0 unless RBSC_DEVICE is set).
 //
-// Extra options (after the positional ones; none changes the three lines):
+// Extra options (after the positional ones):
 //   --dump-partition FILE   write the canonical label of every node, one per line
-//   --init-colors FILE      initial colours, one uint32 per line (N lines)
+//   --init-colors FILE      initial colours, one uint32 per line (N lines);
+//                           refines exactly in one batch
 //   --stats                 print a JSON line with rounds and timings to stderr
 //   --relabel sort|hash     relabel strategy (default hash)
+//   --aggressive            the stop test of the reference's rbsc_aggressive
+//                           program (rbsc_aggressive.cu:487) in edge-batch mode
+//   --exact                 the coarsest partition whatever edge_batch_size is
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -39,20 +44,21 @@ int main(int argc, char** argv)
 {
     const char* dump = nullptr;
     const char* init_path = nullptr;
-    bool want_stats = false;
+    bool want_stats = false, aggressive = false, exact = false;
     int relabel = RBSC_RELABEL_HASH;
     std::vector<const char*> pos;
     for (int i = 1; i < argc; ++i) {
         if (!std::strcmp(argv[i], "--dump-partition") && i + 1 < argc) dump = argv[++i];
         else if (!std::strcmp(argv[i], "--init-colors") && i + 1 < argc) init_path = argv[++i];
         else if (!std::strcmp(argv[i], "--stats")) want_stats = true;
+        else if (!std::strcmp(argv[i], "--aggressive")) aggressive = true;
+        else if (!std::strcmp(argv[i], "--exact")) exact = true;
         else if (!std::strcmp(argv[i], "--relabel") && i + 1 < argc) relabel = !std::strcmp(argv[++i], "sort") ? RBSC_RELABEL_SORT : RBSC_RELABEL_HASH;
         else pos.push_back(argv[i]);
     }
     // positional arguments, as rbsc.cu:204-205 reads them
     unsigned long long edge_batch = pos.size() >= 1 ? std::strtoull(pos[0], nullptr, 10) : 0;
     unsigned long long gpus = pos.size() >= 2 ? std::strtoull(pos[1], nullptr, 10) : 1;
-    (void)edge_batch;
     (void)gpus;
 
     std::string text;
@@ -102,7 +108,10 @@ int main(int argc, char** argv)
     csr.weights = hg.weights;
     std::vector<uint32_t> labels(hg.n);
     rbsc_stats st;
-    rbsc_status rc = rbsc_refine(ctx, &csr, init.empty() ? nullptr : init.data(), hg.n ? labels.data() : nullptr, &st);
+    const bool batched = !exact && init.empty() && edge_batch > 0 && edge_batch < hg.m;
+    rbsc_status rc = batched ? rbsc_refine_edge_batches(ctx, &csr, edge_batch, aggressive ? 1 : 0,
+                                                        hg.n ? labels.data() : nullptr, &st, nullptr)
+                             : rbsc_refine(ctx, &csr, init.empty() ? nullptr : init.data(), hg.n ? labels.data() : nullptr, &st);
     if (rc != RBSC_OK) {
         std::printf("refinement failed: %s\n", rbsc_last_error(ctx));
         rbsc_ctx_destroy(ctx);
