@@ -98,6 +98,10 @@ typedef struct {
     double first_signature_ms;   /* k_signature of the first pass, when launched from the
                                     host (few initial classes), else 0                    */
     uint64_t first_signature_arcs; /* arcs that launch processed                         */
+    uint64_t streamed_bytes;  /* host->device bytes of the streamed signature passes
+                                 (graphs from rbsc_graph_upload_streamed)                */
+    uint32_t streamed_passes; /* signature passes that streamed the arcs                */
+    uint32_t pad;
 } rbsc_stats;
 
 /* Per-kernel device time of one refinement, measured with CUDA events around
@@ -174,6 +178,21 @@ rbsc_status rbsc_graph_upload(rbsc_ctx* ctx, const rbsc_csr* host_graph, rbsc_gr
 /* Same from a CSR already in device memory (pointers into this context's
  * device); the arrays are copied, the caller keeps ownership of its own. */
 rbsc_status rbsc_graph_from_device(rbsc_ctx* ctx, const rbsc_csr* device_graph, rbsc_graph** out);
+/* A resident graph whose arcs stay in host memory: for graphs whose arcs do
+ * not fit (or should not live in) device memory.  Offsets, the per-row tiling
+ * and all refinement state live on the device; a signature pass over the full
+ * arc set streams the heads (and weights) in batches of batch_arcs arcs (0 = a
+ * quarter of M) through two device buffers, copying the next batch on a side
+ * stream while the signature kernel reads the current one.  Once the arcs of
+ * non-singleton rows fit resident_arcs (0 = min(M, 2^31)) they are compacted
+ * into device memory and later passes run from there.  The exact check and the
+ * compaction read the host arrays directly (mapped page-locked memory).  The
+ * caller's indices / weights must stay valid and unchanged while the graph
+ * exists; pageable arrays are page-locked here (cudaHostRegister) for its
+ * lifetime.  No reference counterpart: the reference's batches
+ * (rbsc.cu:302-345) change the result; this mode is exact. */
+rbsc_status rbsc_graph_upload_streamed(rbsc_ctx* ctx, const rbsc_csr* host_graph, uint64_t batch_arcs,
+                                       uint64_t resident_arcs, rbsc_graph** out);
 void rbsc_graph_free(rbsc_graph* g);
 rbsc_status rbsc_graph_info(const rbsc_graph* g, uint32_t* n, uint64_t* m);
 /* Device pointers of the resident CSR (offsets are uint64). */

@@ -58,6 +58,8 @@ class Result:
     loop_ms: float = 0.0
     first_signature_ms: float = 0.0
     first_signature_arcs: int = 0
+    streamed_bytes: int = 0
+    streamed_passes: int = 0
 
 
 def _result(st: _lib.Stats, labels) -> Result:
@@ -66,7 +68,7 @@ def _result(st: _lib.Stats, labels) -> Result:
                   int(st.initial_blocks), float(st.time_s), float(st.device_ms), float(st.verify_ms),
                   float(st.h2d_ms), float(st.d2h_ms), int(st.h2d_bytes), int(st.d2h_bytes), rb,
                   int(st.kernel_launches), float(st.init_ms), float(st.loop_ms), float(st.first_signature_ms),
-                  int(st.first_signature_arcs))
+                  int(st.first_signature_arcs), int(st.streamed_bytes), int(st.streamed_passes))
 
 
 def _check(lib, status: int, ctx=None):
@@ -191,6 +193,19 @@ class Context:
         h = ctypes.c_void_p()
         _check(self._lib, self._lib.rbsc_graph_upload(self._h, ctypes.byref(c), ctypes.byref(h)), self._h)
         return Graph(self, h)
+
+    def upload_streamed(self, off, idx, wt=None, batch_arcs: int = 0, resident_arcs: int = 0) -> "Graph":
+        """A resident graph whose arcs stay in host memory and are streamed to
+        the device in batches of batch_arcs arcs during the signature passes
+        (rbsc_graph_upload_streamed).  The arrays are kept alive by the
+        returned Graph."""
+        c, keep = _csr(off, idx, wt)
+        h = ctypes.c_void_p()
+        _check(self._lib, self._lib.rbsc_graph_upload_streamed(self._h, ctypes.byref(c), batch_arcs, resident_arcs,
+                                                               ctypes.byref(h)), self._h)
+        g = Graph(self, h)
+        g._keep = keep
+        return g
 
     def from_device(self, n: int, m: int, d_off: int, d_idx: int, d_wt: int | None = None,
                     offset_bytes: int = 8) -> "Graph":

@@ -38,7 +38,7 @@ EXPORTED = [
     "rbsc_graph_degree_colors", "rbsc_parse_arcs", "rbsc_host_graph_free", "rbsc_gen_rmat_device",
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
-    "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches",
+    "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches", "rbsc_graph_upload_streamed",
     "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
     "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
@@ -81,6 +81,9 @@ class Stats(ctypes.Structure):
         ("loop_ms", ctypes.c_double),
         ("first_signature_ms", ctypes.c_double),
         ("first_signature_arcs", ctypes.c_uint64),
+        ("streamed_bytes", ctypes.c_uint64),
+        ("streamed_passes", ctypes.c_uint32),
+        ("pad", ctypes.c_uint32),
     ]
 
 
@@ -237,6 +240,7 @@ def load():
     lib.rbsc_ctx_set_opts.argtypes = [vp, P(Opts)]
     lib.rbsc_refine.argtypes = [vp, P(Csr), vp, vp, P(Stats)]
     lib.rbsc_graph_upload.argtypes = [vp, P(Csr), P(vp)]
+    lib.rbsc_graph_upload_streamed.argtypes = [vp, P(Csr), ctypes.c_uint64, ctypes.c_uint64, P(vp)]
     lib.rbsc_graph_from_device.argtypes = [vp, P(Csr), P(vp)]
     lib.rbsc_graph_free.argtypes = [vp]
     lib.rbsc_graph_info.argtypes = [vp, P(ctypes.c_uint32), P(ctypes.c_uint64)]

@@ -113,6 +113,23 @@ struct rbsc_graph {
     uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop
     bool oneshot = false;       // refined once and freed (rbsc_refine): capturing and
                                 // instantiating the loop graph would cost more than it saves
+
+    // arcs kept in host memory (rbsc_graph_upload_streamed): d_idx / d_wt are
+    // device-accessible views of page-locked host arrays; a signature pass
+    // over them copies chunks of tiles into d_chunk on copy_stream
+    bool host_arcs = false;
+    bool arcs_on_host = false;      // the active set still uses the host arcs
+    void* reg_idx = nullptr;        // host ranges page-locked here, released at free
+    void* reg_wt = nullptr;
+    uint32_t chunk_tiles = 0;
+    uint32_t* d_chunk[2] = {nullptr, nullptr};
+    uint64_t* d_chunk_wt[2] = {nullptr, nullptr};
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr};
+    cudaEvent_t ev_used[2] = {nullptr, nullptr};
+    uint64_t resident_cap = 0;      // arcs the compacted (device) arc sets hold
+    uint64_t streamed_bytes = 0;    // copied by the streamed passes of the last refinement
+    uint32_t streamed_passes = 0;
 };
 
 rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);

@@ -316,6 +316,20 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
     cudaStreamSynchronize(g->ctx->stream);
     graph_release_refine(g);
     dev_free(g->ctx, (void*&)g->d_off);
+    if (g->host_arcs) {
+        if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
+        for (int i = 0; i < 2; ++i) {
+            dev_free(g->ctx, (void*&)g->d_chunk[i]);
+            dev_free(g->ctx, (void*&)g->d_chunk_wt[i]);
+            if (g->ev_copied[i]) cudaEventDestroy(g->ev_copied[i]);
+            if (g->ev_used[i]) cudaEventDestroy(g->ev_used[i]);
+        }
+        if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
+        if (g->reg_idx) cudaHostUnregister(g->reg_idx);
+        if (g->reg_wt) cudaHostUnregister(g->reg_wt);
+        g->d_idx = nullptr;  // host memory of the caller
+        g->d_wt = nullptr;
+    }
     dev_free(g->ctx, (void*&)g->d_idx);
     dev_free(g->ctx, (void*&)g->d_wt);
     dev_free(g->ctx, (void*&)g->d_rows);
@@ -551,6 +565,96 @@ extern "C" rbsc_status rbsc_graph_from_device(rbsc_ctx* ctx, const rbsc_csr* dev
     return graph_load(ctx, device_graph, true, out, nullptr, nullptr);
 }
 
+// Device-accessible view of a host array: page-locked memory is used as it
+// is; pageable memory is registered (mapped, read-only) and *reg records it.
+static rbsc_status map_host(rbsc_ctx* ctx, const void* p, size_t bytes, void** dev, void** reg)
+{
+    *dev = nullptr;
+    *reg = nullptr;
+    cudaPointerAttributes at;
+    cudaError_t e = cudaPointerGetAttributes(&at, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        at.type = cudaMemoryTypeUnregistered;
+    }
+    if (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged)
+        return rbsc_fail(ctx, RBSC_ERR_INVALID, "streamed graph: arcs must be in host memory");
+    if (at.type != cudaMemoryTypeHost) {
+        e = cudaHostRegister(const_cast<void*>(p), bytes, cudaHostRegisterMapped | cudaHostRegisterReadOnly);
+        if (e != cudaSuccess) return rbsc_cuda_fail(ctx, e, "cudaHostRegister", __LINE__);
+        *reg = const_cast<void*>(p);
+    }
+    e = cudaHostGetDevicePointer(dev, const_cast<void*>(p), 0);
+    if (e != cudaSuccess) {
+        if (*reg) cudaHostUnregister(*reg);
+        *reg = nullptr;
+        return rbsc_cuda_fail(ctx, e, "cudaHostGetDevicePointer", __LINE__);
+    }
+    return RBSC_OK;
+}
+
+extern "C" rbsc_status rbsc_graph_upload_streamed(rbsc_ctx* ctx, const rbsc_csr* c, uint64_t batch_arcs, uint64_t resident_arcs,
+                                                  rbsc_graph** out)
+{
+    if (!out) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null output");
+    *out = nullptr;
+    CKS(check_csr_args(ctx, c));
+    CK(cudaSetDevice(ctx->device));
+    rbsc_graph* g = new (std::nothrow) rbsc_graph();
+    if (!g) return rbsc_fail(ctx, RBSC_ERR_OOM, "out of host memory");
+    struct Guard { rbsc_graph*& g; ~Guard() { if (g) rbsc_graph_free(g); } } guard{g};
+    g->ctx = ctx;
+    g->n = c->n;
+    g->m = c->m;
+    g->weighted = c->weights != nullptr;
+    g->host_arcs = true;
+    g->arcs_on_host = true;
+    cudaStream_t s = ctx->stream;
+    if (c->m) {
+        void* dv = nullptr;
+        CKS(map_host(ctx, c->indices, 4 * (size_t)c->m, &dv, &g->reg_idx));
+        g->d_idx = static_cast<uint32_t*>(dv);
+        if (c->weights) {
+            CKS(map_host(ctx, c->weights, 8 * (size_t)c->m, &dv, &g->reg_wt));
+            g->d_wt = static_cast<uint64_t*>(dv);
+        }
+    }
+    // offsets in device memory (widened to 64 bits)
+    CKS(dev_alloc(ctx, (void**)&g->d_off, sizeof(uint64_t) * ((size_t)g->n + 1)));
+    const size_t offb = (size_t)c->offset_bytes * ((size_t)c->n + 1);
+    if (c->offset_bytes == 8) {
+        CK(cudaMemcpyAsync(g->d_off, c->offsets, offb, cudaMemcpyHostToDevice, s));
+    } else {
+        void* tmp = nullptr;
+        CKS(dev_alloc(ctx, &tmp, offb));
+        cudaError_t e = cudaMemcpyAsync(tmp, c->offsets, offb, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) {
+            ++rbsc::launch_counter();
+            k_widen_offsets<uint32_t><<<grid_for((uint64_t)c->n + 1, 256), 256, 0, s>>>((uint64_t)c->n + 1, (const uint32_t*)tmp, g->d_off);
+            e = cudaGetLastError();
+        }
+        cudaStreamSynchronize(s);
+        dev_free(ctx, tmp);
+        if (e != cudaSuccess) return rbsc_cuda_fail(ctx, e, "offsets", __LINE__);
+    }
+    CK(cudaStreamSynchronize(s));
+    CKS(graph_prepare(ctx, g));  // validates the heads (read from host memory)
+    const uint64_t batch = batch_arcs ? batch_arcs : std::max<uint64_t>(1, ceil_div<uint64_t>(c->m, 4));
+    g->chunk_tiles = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(batch, kTileEdges), std::max<uint32_t>(g->ntiles, 1)));
+    g->resident_cap = resident_arcs ? resident_arcs : std::min<uint64_t>(std::max<uint64_t>(c->m, 1), 1ull << 31);
+    const size_t chunk = (size_t)g->chunk_tiles * kTileEdges;
+    for (int i = 0; i < 2; ++i) {
+        CKS(dev_alloc(ctx, (void**)&g->d_chunk[i], 4 * chunk));
+        if (g->weighted) CKS(dev_alloc(ctx, (void**)&g->d_chunk_wt[i], 8 * chunk));
+        CK(cudaEventCreateWithFlags(&g->ev_copied[i], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&g->ev_used[i], cudaEventDisableTiming));
+    }
+    CK(cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking));
+    *out = g;
+    g = nullptr;
+    return RBSC_OK;
+}
+
 // ---------------------------------------------------------------------------
 // refinement
 // ---------------------------------------------------------------------------
@@ -584,21 +688,25 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_pairs, 8 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_grep, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_gcnt, 4 * n));
-    g->compact_arcs = g->m > 0 && g->m < (1ull << 32);
+    g->compact_arcs = g->m > 0;
     const size_t K = std::max<uint32_t>(g->K, 1);
-    const size_t tiles = std::max<uint32_t>(g->ntiles, 1);
-    const size_t mpad = tiles * kTileEdges;
+    // compacted arc sets: as large as the graph's own (in device memory), or
+    // the resident capacity of a streamed graph; k_compact_decide copies only
+    // what fits (and what fits 32-bit offsets)
+    const size_t cap = g->host_arcs ? (size_t)std::max<uint64_t>(g->resident_cap, 1) : (size_t)std::max<uint64_t>(g->m, 1);
+    const size_t ctiles = ceil_div<uint64_t>(std::min<uint64_t>(cap, 0xffffffffull), kTileEdges);
+    const size_t cpad = ctiles * kTileEdges;
     for (int d = 0; d < 2; ++d) {
         CKS(dev_alloc(ctx, (void**)&g->cb.nodes[d], 4 * n));
         if (!g->compact_arcs) continue;
         CKS(dev_alloc(ctx, (void**)&g->cb.rows[d], 4 * K));
         CKS(dev_alloc(ctx, (void**)&g->cb.off[d], 4 * (K + 1)));
-        CKS(dev_alloc(ctx, (void**)&g->cb.src[d], 4 * K));
-        CKS(dev_alloc(ctx, (void**)&g->cb.idx[d], 4 * mpad));
-        if (g->weighted) CKS(dev_alloc(ctx, (void**)&g->cb.wt[d], 8 * mpad));
-        CKS(dev_alloc(ctx, (void**)&g->cb.head8[d], mpad / 8 + 16));
-        CKS(dev_alloc(ctx, (void**)&g->cb.tile_row[d], 4 * (tiles + 1)));
-        CKS(dev_alloc(ctx, (void**)&g->cb.split[d], 4 * (tiles + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->cb.src[d], 8 * K));
+        CKS(dev_alloc(ctx, (void**)&g->cb.idx[d], 4 * cpad));
+        if (g->weighted) CKS(dev_alloc(ctx, (void**)&g->cb.wt[d], 8 * cpad));
+        CKS(dev_alloc(ctx, (void**)&g->cb.head8[d], cpad / 8 + 16));
+        CKS(dev_alloc(ctx, (void**)&g->cb.tile_row[d], 4 * (ctiles + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->cb.split[d], 4 * (ctiles + 1)));
     }
     CK(cudaMemsetAsync(g->d_sig, 0, sizeof(Sig) * n, ctx->stream));
     CK(cudaMemsetAsync(g->d_tab, 0, sizeof(Entry) << g->log2tab, ctx->stream));
@@ -626,6 +734,51 @@ struct PassTimer {
 // First-pass gather variants (see k_signature / k_signature_uniform).
 enum FirstPass { kPassFull = 0, kPassUniform = 1, kPassRank8 = 2, kPassRank16 = 3 };
 
+template <typename ColT>
+static void launch_signature_chunk(bool weighted, unsigned grid, cudaStream_t s, const ActiveSet* as, const RoundState* st,
+                                   const ColT* col, Sig* sig, TileRange r)
+{
+    ++rbsc::launch_counter();
+    if (weighted) k_signature_chunk<true, ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r);
+    else k_signature_chunk<false, ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r);
+}
+
+// The signature kernel over arcs in host memory: chunks of chunk_tiles tiles
+// are copied into two device buffers on copy_stream; chunk c's copy waits
+// until the kernel that read its buffer (chunk c-2) is done, and its kernel
+// waits for the copy, so copies run beside the kernels of earlier chunks.
+static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, int first)
+{
+    const uint64_t m = g->m;
+    const uint32_t ntiles = g->ntiles;
+    for (uint32_t t0 = 0, c = 0; t0 < ntiles; t0 += g->chunk_tiles, ++c) {
+        const uint32_t t1 = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)t0 + g->chunk_tiles);
+        const uint64_t a0 = (uint64_t)t0 * kTileEdges, a1 = std::min<uint64_t>(m, (uint64_t)t1 * kTileEdges);
+        const int slot = (int)(c & 1u);
+        CK(cudaStreamWaitEvent(g->copy_stream, g->ev_used[slot], 0));
+        CK(cudaMemcpyAsync(g->d_chunk[slot], g->d_idx + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        if (g->weighted)
+            CK(cudaMemcpyAsync(g->d_chunk_wt[slot], g->d_wt + a0, 8 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        CK(cudaEventRecord(g->ev_copied[slot], g->copy_stream));
+        CK(cudaStreamWaitEvent(s, g->ev_copied[slot], 0));
+        const TileRange r{t0, t1, g->d_chunk[slot], g->weighted ? g->d_chunk_wt[slot] : nullptr, a0};
+        const unsigned grid = persistent_grid(ctx, t1 - t0, kTileThreads / 32);
+        if (first == kPassRank8)
+            launch_signature_chunk<uint8_t>(g->weighted, grid, s, g->d_as, g->d_st, reinterpret_cast<const uint8_t*>(g->d_rank),
+                                            g->d_sig, r);
+        else if (first == kPassRank16)
+            launch_signature_chunk<uint16_t>(g->weighted, grid, s, g->d_as, g->d_st,
+                                             reinterpret_cast<const uint16_t*>(g->d_rank), g->d_sig, r);
+        else
+            launch_signature_chunk<uint32_t>(g->weighted, grid, s, g->d_as, g->d_st, g->d_col[0], g->d_sig, r);
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(g->ev_used[slot], s));
+        g->streamed_bytes += (a1 - a0) * (g->weighted ? 12 : 4);
+    }
+    ++g->streamed_passes;
+    return RBSC_OK;
+}
+
 static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cudaGraphConditionalHandle h, int use_handle,
                                PassTimer* t = nullptr, int first = kPassFull, uint32_t c0 = 0)
 {
@@ -639,7 +792,10 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (t) CK(cudaEventRecord(t->ev[1], s));
     // the host-launched first pass is never captured: time its signature kernel
     if (first != kPassFull) CK(cudaEventRecord(ctx->ev_sig[0], s));
-    if (g->m > 0) {
+    const bool streamed = g->arcs_on_host && g->m > 0 && first != kPassUniform;
+    if (streamed) {
+        CKS(stream_signature(ctx, g, s, first));
+    } else if (g->m > 0) {
         const unsigned blocks = persistent_grid(ctx, g->ntiles, kTileThreads / 32);
         ++rbsc::launch_counter();
         if (first == kPassUniform) {
@@ -697,7 +853,9 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig);
     }
     ++rbsc::launch_counter();
-    const bool persist = hash && !ctx->opts.no_persist;
+    // no hand-off to the persistent kernel from a pass over host arcs: the
+    // next pass sees whether the compaction brought them into device memory
+    const bool persist = hash && !ctx->opts.no_persist && !g->arcs_on_host;
     k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb, persist ? kPersistArcs : 0ull, kPersistNodes, h, use_handle);
     if (t) CK(cudaEventRecord(t->ev[5], s));
     CK(cudaGetLastError());
@@ -748,7 +906,13 @@ static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
 static rbsc_status read_state(rbsc_ctx* ctx, rbsc_graph* g)
 {
     CK(cudaMemcpyAsync(g->h_st, g->d_st, sizeof(RoundState), cudaMemcpyDeviceToHost, ctx->stream));
+    // a streamed graph: did the last pass's compaction bring the arcs into
+    // device memory?
+    const uint32_t* idx = nullptr;
+    if (g->arcs_on_host)
+        CK(cudaMemcpyAsync(&idx, &g->d_as->idx, sizeof idx, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
+    if (g->arcs_on_host) g->arcs_on_host = idx == g->d_idx;
     return RBSC_OK;
 }
 
@@ -851,7 +1015,18 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
 // host-driven loop), until the fixpoint, an error or the hand-off.
 static rbsc_status run_passes(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt, uint64_t* graph_kernels)
 {
-    if (ctx->opts.use_graph && !kt && !g->oneshot) {
+    // passes over host arcs run from the host (each streams its chunks)
+    // until a compaction brings the active arcs into device memory
+    const bool graph_loop = ctx->opts.use_graph && !kt && !g->oneshot;
+    if (graph_loop && g->arcs_on_host) {
+        CKS(ensure_sort_relabel_bufs(ctx, g));
+        while (g->arcs_on_host) {
+            CKS(launch_pass(ctx, g, ctx->stream, cudaGraphConditionalHandle(), 0));
+            CKS(read_state(ctx, g));
+            if (g->h_st->done || g->h_st->error || g->h_st->handoff) return RBSC_OK;
+        }
+    }
+    if (graph_loop) {
         CKS(build_loop_graph(ctx, g));
         const uint32_t r0 = g->h_st->round;
         CK(cudaGraphLaunch(g->loop_exec, ctx->stream));
@@ -922,6 +1097,9 @@ static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
     a.nsplit = g->nsplit;
     a.nodes = g->cb.nodes[0];
     a.compact_arcs = g->compact_arcs ? 1u : 0u;
+    a.dst_cap = g->host_arcs ? g->resident_cap : std::max<uint64_t>(g->m, 1);
+    a.arcctr = 0;
+    g->arcs_on_host = g->host_arcs;
     *g->h_as = a;
     CK(cudaMemcpyAsync(g->d_as, g->h_as, sizeof a, cudaMemcpyHostToDevice, s));
     if (g->nsplit) {
@@ -1074,6 +1252,8 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     CKS(ensure_refine_bufs(ctx, g));
     g->first_sig_ms = 0.f;
     g->first_sig_arcs = 0;
+    g->streamed_bytes = 0;
+    g->streamed_passes = 0;
     RoundState& hs = *g->h_st;
     std::memset(&hs, 0, sizeof hs);
     hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);
@@ -1209,6 +1389,8 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         stats->loop_ms = loop_ms;
         stats->first_signature_ms = g->first_sig_ms;
         stats->first_signature_arcs = g->first_sig_arcs;
+        stats->streamed_bytes = g->streamed_bytes;
+        stats->streamed_passes = g->streamed_passes;
     }
     if (kt) kt->total_ms = total_ms;
     return RBSC_OK;

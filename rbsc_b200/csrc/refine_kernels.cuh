@@ -82,8 +82,10 @@ struct ActiveSet {
     uint32_t new_m;
     uint32_t dst_arcs;         // which compacted arc buffer the next rebuild writes
     uint32_t dst_nodes;        // which node-list buffer the next compaction writes
-    uint32_t compact_arcs;     // arc-set compaction allowed (M < 2^32)
+    uint32_t compact_arcs;     // arc-set compaction allowed
     uint32_t nfollow;          // follower list length
+    uint64_t dst_cap;          // arcs the compaction buffers hold
+    unsigned long long arcctr; // arcs of the kept rows, counted without the 32-bit limit of rowctr
 };
 
 // Per-node signature: the 64-bit and the 32-bit sum side by side in 16 B, so
@@ -121,7 +123,7 @@ constexpr uint32_t kRepFlag = 0x80000000u;
 struct CompactBufs {
     uint32_t* rows[2];
     uint32_t* off[2];      // uint32 offsets (K+1)
-    uint32_t* src[2];      // where each row's arcs start in the source arc set
+    uint64_t* src[2];      // where each row's arcs start in the source arc set
     uint32_t* idx[2];
     uint64_t* wt[2];
     uint8_t* head8[2];
@@ -251,22 +253,36 @@ __device__ __forceinline__ uint32_t gather_col(const ColT* p)
     else return (uint32_t)__ldcg(p);
 }
 
-template <bool WEIGHTED, typename ColT, bool NC = true>
+// A range of tiles [lo, hi) whose heads (and weights) were copied to a chunk
+// buffer that starts at arc `base` (streamed arc sets); the default range is
+// every tile, read from the active set's own arrays.
+struct TileRange {
+    uint32_t lo, hi;
+    const uint32_t* idx;
+    const uint64_t* wt;
+    uint64_t base;
+};
+
+template <bool WEIGHTED, typename ColT, bool NC = true, bool RANGE = false>
 __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
-                                               const ColT* __restrict__ col, Sig* __restrict__ sig)
+                                               const ColT* __restrict__ col, Sig* __restrict__ sig,
+                                               TileRange rng = TileRange{0u, 0u, nullptr, nullptr, 0ull})
 {
     const uint32_t lane = threadIdx.x & 31;
-    const uint32_t ntiles = as->ntiles;
+    const uint32_t ntiles = RANGE ? rng.hi : as->ntiles;
     const uint64_t m = as->m;
     const uint32_t* __restrict__ rows = as->rows;
     const uint32_t* __restrict__ tile_row = as->tile_row;
     const uint8_t* __restrict__ head8 = as->head8;
-    const uint32_t* __restrict__ idx = as->idx;
-    const uint64_t* __restrict__ wt = as->wt;
+    // RANGE: idx[e - base] / wt[e - base] hold arc e of the chunk
+    const uint32_t* __restrict__ idx = RANGE ? rng.idx : as->idx;
+    const uint64_t* __restrict__ wt = RANGE ? rng.wt : as->wt;
+    const uint64_t ebase = RANGE ? rng.base : 0ull;
     const uint64_t salt = pass_salt1(st->seed, st->round);
     const uint32_t warps = gridDim.x * (kTileThreads / 32);
 
-    for (uint32_t tile = blockIdx.x * (kTileThreads / 32) + (threadIdx.x >> 5); tile < ntiles; tile += warps) {
+    for (uint32_t tile = (RANGE ? rng.lo : 0u) + blockIdx.x * (kTileThreads / 32) + (threadIdx.x >> 5); tile < ntiles;
+         tile += warps) {
         const uint64_t tbeg = (uint64_t)tile * kTileEdges;
         const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
         const uint64_t tend = tbeg + tlen;
@@ -281,7 +297,7 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
         static_assert(sizeof(ColT) <= 4, "colour type");
         if (cnt == kEdgesPerThread) {
             hb = *reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3));
-            const uint4* p = reinterpret_cast<const uint4*>(idx + tbeg + a);
+            const uint4* p = reinterpret_cast<const uint4*>(idx + (tbeg - ebase) + a);
             const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1), q2 = __ldcs(p + 2), q3 = __ldcs(p + 3);
             c[0] = gather_col<NC>(col + q0.x); c[1] = gather_col<NC>(col + q0.y);
             c[2] = gather_col<NC>(col + q0.z); c[3] = gather_col<NC>(col + q0.w);
@@ -294,11 +310,11 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
         } else {
             if (cnt) hb = (uint32_t)(*reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3))) & ((1u << cnt) - 1u);
 #pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? gather_col<NC>(col + __ldcs(idx + tbeg + a + i)) : 0u;
+            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? gather_col<NC>(col + __ldcs(idx + (tbeg - ebase) + a + i)) : 0u;
         }
         if (WEIGHTED) {
 #pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + tbeg + a + i) : 0ull;
+            for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + (tbeg - ebase) + a + i) : 0ull;
         }
 
         // row of arc a-1 (or of arc a when arc a does not start a row):
@@ -405,6 +421,16 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveS
                                                                    Sig* __restrict__ sig)
 {
     signature_body<WEIGHTED, ColT>(as, st, col, sig);
+}
+
+// The same over the tiles of one streamed chunk (see TileRange).
+template <bool WEIGHTED, typename ColT>
+static __global__ void __launch_bounds__(kTileThreads) k_signature_chunk(const ActiveSet* __restrict__ as,
+                                                                         const RoundState* __restrict__ st,
+                                                                         const ColT* __restrict__ col,
+                                                                         Sig* __restrict__ sig, TileRange rng)
+{
+    signature_body<WEIGHTED, ColT, true, true>(as, st, col, sig, rng);
 }
 
 // First pass when every node starts in one block (the reference's default):
@@ -902,6 +928,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
     __shared__ unsigned long long s_warp[kNodeThreads / 32];
+    __shared__ unsigned long long s_warp_arcs[kNodeThreads / 32];
     __shared__ unsigned long long s_base;
     if (st->done || st->error || !as->compact_arcs) return;
     const uint32_t K = as->K;
@@ -912,12 +939,13 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
     const uint32_t d = as->dst_arcs;
     uint32_t* __restrict__ drows = bufs.rows[d];
     uint32_t* __restrict__ doff = bufs.off[d];
-    uint32_t* __restrict__ dsrc = bufs.src[d];
+    uint64_t* __restrict__ dsrc = bufs.src[d];
     const uint32_t stride = gridDim.x * kNodeThreads;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t base = blockIdx.x * kNodeThreads; base < K; base += stride) {
         const uint32_t k = base + threadIdx.x;
-        uint32_t node = 0, deg = 0, start = 0;
+        uint32_t node = 0, deg = 0;
+        uint64_t start = 0;
         bool keep = false;
         if (k < K) {
             node = rows[k];
@@ -925,28 +953,35 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
             if (keep) {
                 const uint64_t b = r64 ? roff64[k] : roff32[k];
                 const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
-                start = (uint32_t)b;
+                start = b;
                 deg = (uint32_t)(e - b);
             }
         }
-        // per-thread (rows, arcs) packed: rows in the high half
+        // per-thread (rows, arcs) packed: rows in the high half; the packed
+        // arcs are exact while the kept arcs stay below 2^32, which arcctr
+        // (64-bit) tells k_compact_decide
         unsigned long long v = keep ? ((1ull << 32) | deg) : 0ull;
         unsigned long long incl = v;
+        unsigned long long arcs = deg;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += t;
+            arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
         }
         if (lane == 31) s_warp[warp] = incl;
+        if (lane == 0) s_warp_arcs[warp] = arcs;
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned long long run = 0;
+            unsigned long long run = 0, run_arcs = 0;
             for (int w = 0; w < kNodeThreads / 32; ++w) {
                 const unsigned long long c = s_warp[w];
                 s_warp[w] = run;
                 run += c;
+                run_arcs += s_warp_arcs[w];
             }
             s_base = run ? atomicAdd(&as->rowctr, run) : 0ull;
+            if (run_arcs) atomicAdd(&as->arcctr, run_arcs);
         }
         __syncthreads();
         if (keep) {
@@ -967,9 +1002,12 @@ static __global__ void k_compact_decide(ActiveSet* as, const RoundState* st, Com
         as->do_copy = 0;
         return;
     }
+    // copy when the kept arcs fit the 32-bit destination offsets and the
+    // compaction buffers, and dropped to 3/4 of the current set or less
+    const uint64_t arcs = as->arcctr;
     const uint32_t nk = (uint32_t)(as->rowctr >> 32);
-    const uint32_t nm = (uint32_t)(as->rowctr & 0xffffffffull);
-    const bool copy = nk > 0 && (uint64_t)nm * 4ull <= as->m * 3ull;
+    const uint32_t nm = (uint32_t)arcs;
+    const bool copy = nk > 0 && arcs < (1ull << 32) && arcs <= as->dst_cap && arcs * 4ull <= as->m * 3ull;
     as->do_copy = copy ? 1u : 0u;
     as->new_K = nk;
     as->new_m = nm;
@@ -991,7 +1029,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
     const uint32_t nm = as->new_m;
     const uint32_t d = as->dst_arcs;
     const uint32_t* __restrict__ doff = bufs.off[d];
-    const uint32_t* __restrict__ dsrc = bufs.src[d];
+    const uint64_t* __restrict__ dsrc = bufs.src[d];
     const uint32_t* __restrict__ drows = bufs.rows[d];
     uint32_t* __restrict__ didx = bufs.idx[d];
     uint64_t* __restrict__ dwt = bufs.wt[d];
@@ -1009,7 +1047,8 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
         }
         const uint32_t k0 = lo;
         uint32_t k = k0;
-        uint32_t rb = doff[k], re = doff[k + 1], src = dsrc[k];
+        uint32_t rb = doff[k], re = doff[k + 1];
+        uint64_t src = dsrc[k];
         uint32_t bits = 0;
         for (uint32_t i = 0; i < 16u; ++i) {
             const uint32_t e = e0 + i;
@@ -1071,6 +1110,7 @@ static __global__ void k_compact_finalize(ActiveSet* as, RoundState* st, Compact
         as->do_copy = 0;
     }
     as->rowctr = 0;
+    as->arcctr = 0;
     as->splitctr = 0;
     const bool small = handoff_arcs > 0 && as->m <= handoff_arcs && as->nnodes <= handoff_nodes;
     st->handoff = small ? 1u : 0u;
