@@ -334,6 +334,7 @@ def run_ours(args, rank, world, local_rank):
 
     batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
     served = None if args.serve_requests <= 0 else run_served(args, world, dist, local_rank)
+    streamed = None if args.stream_scale <= 0 else run_streamed(args, ctx, local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -348,7 +349,7 @@ def run_ours(args, rank, world, local_rank):
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "batched": batched,
-                "served": served}
+                "served": served, "streamed": streamed}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -544,6 +545,81 @@ def run_served(args, world, dist, local_rank):
     return out
 
 
+def run_streamed(args, ctx, local_rank):
+    """Arcs in host memory (the out-of-HBM configuration): R-MAT scale
+    args.stream_scale, edge factor args.stream_ef, generated on the device in
+    source buckets into page-locked host memory; int64 offsets, int32 heads,
+    degree-bucket initial colours.  Each signature pass over the full arc set
+    streams it in batches of a quarter of the arcs through two device buffers,
+    the copy of the next batch beside the signature kernel of the current one.
+    The same graph refined from device memory gives the parity check (labels
+    equal) and the in-HBM time beside it."""
+    import torch
+    t0 = time.perf_counter()
+    pg = ctx.gen_rmat_pinned(args.stream_scale, args.stream_ef, seed=args.seed)
+    gen_s = time.perf_counter() - t0
+    n, m = pg.n, pg.m
+    # host-link reference: one page-locked 4 GiB host->device copy, best of 3
+    hbuf = torch.empty(1 << 30, dtype=torch.int32, pin_memory=True)
+    dbuf = torch.empty(1 << 30, dtype=torch.int32, device="cuda")
+    h2d = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dbuf.copy_(hbuf, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        h2d.append(4.0 * (1 << 30) / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del hbuf, dbuf
+    torch.cuda.empty_cache()
+    t0 = time.perf_counter()
+    g = ctx.upload_streamed(pg.off, pg.idx)
+    up_s = time.perf_counter() - t0
+    d_init = torch.empty(n, dtype=torch.int32, device="cuda")
+    d_out = torch.empty(n, dtype=torch.int32, device="cuda")
+    g.degree_colors_device(d_init.data_ptr())
+    torch.cuda.synchronize()
+    for _ in range(1):
+        g.refine_device(d_init.data_ptr(), d_out.data_ptr())
+    res = [g.refine_device(d_init.data_ptr(), d_out.data_ptr()) for _ in range(args.stream_steps)]
+    times, pr = g.profile(d_init.data_ptr())
+    labels_stream = d_out.cpu()
+    g.free()
+    ctx.trim()
+    ms = [r.device_ms for r in res]
+    rounds = res[0].rounds
+    p1 = times["per_pass"][0]
+    # the same graph from device memory
+    t0 = time.perf_counter()
+    g2 = ctx.upload(pg.off, pg.idx)
+    up2_s = time.perf_counter() - t0
+    g2.refine_device(d_init.data_ptr(), d_out.data_ptr())
+    res2 = [g2.refine_device(d_init.data_ptr(), d_out.data_ptr()) for _ in range(args.stream_steps)]
+    same = bool(torch.equal(labels_stream, d_out.cpu())) and res2[0].blocks == res[0].blocks and res2[0].rounds == rounds
+    assert same, "streamed and in-HBM refinements differ"
+    g2.free()
+    pg.free()
+    ctx.trim()
+    med = statistics.median(ms)
+    sig1 = p1["signature_ms"]
+    return {"workload": f"R-MAT scale {args.stream_scale}, edge factor {args.stream_ef} (a, b, c = 0.57, 0.19, 0.19), "
+                        "duplicates and self-loops removed; int64 offsets, int32 heads in page-locked host memory; "
+                        "initial colours floor(log2(out_degree+1)); batches of 25% of the arcs per streamed pass",
+            "nodes": n, "arcs": m, "rounds": rounds, "blocks": res[0].blocks,
+            "edge_rounds_per_s": m * rounds / (med / 1e3), "ms_to_fixpoint": med, "ms_all": ms,
+            "streamed_passes": res[0].streamed_passes, "streamed_bytes": res[0].streamed_bytes,
+            "first_pass_signature_ms": sig1, "first_pass_arcs": p1["arcs"],
+            "first_pass_h2d_gbs": 4.0 * p1["arcs"] / (sig1 / 1e3) / 1e9,
+            "h2d_copy_gbs_measured": max(h2d),
+            "host_link_frac": (4.0 * p1["arcs"] / (sig1 / 1e3) / 1e9) / max(h2d),
+            "per_pass": times["per_pass"][:6], "verify_ms": res[0].verify_ms,
+            "in_hbm": {"ms_to_fixpoint": statistics.median([r.device_ms for r in res2]),
+                       "upload_s": up2_s, "same_partition": same},
+            "generation_s": gen_s, "upload_streamed_s": up_s,
+            "path": "rbsc_graph_upload_streamed + rbsc_graph_refine_device; parity against rbsc_graph_upload of the "
+                    "same arrays (labels, blocks, rounds equal)"}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -560,6 +636,9 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-sample", type=int, default=1000, help="graphs refined one call each")
     ap.add_argument("--serve-requests", type=int, default=600, help="served stream length (0: skip)")
+    ap.add_argument("--stream-scale", type=int, default=28, help="R-MAT scale of the streamed graph (0: skip)")
+    ap.add_argument("--stream-ef", type=int, default=32)
+    ap.add_argument("--stream-steps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct graphs the requests draw from")
     ap.add_argument("--serve-slots", type=int, default=2)

@@ -263,6 +263,14 @@ rbsc_status rbsc_gen_rmat_device(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_fa
                                  double b, double c, uint64_t seed, rbsc_graph** out);
 rbsc_status rbsc_gen_rmat_host(uint32_t scale, uint32_t edge_factor, double a, double b, double c,
                                uint64_t seed, int32_t threads, rbsc_host_graph* out);
+/* The same graph generated on the device in source buckets (every bucket
+ * regenerates the arcs and keeps those whose source falls in it, sorts and
+ * deduplicates them) and written to page-locked host memory: for graphs
+ * larger than device memory (R-MAT scale 28, edge factor 32: 8.6e9 arcs,
+ * 34 GB of heads).  Free with rbsc_host_graph_free_pinned. */
+rbsc_status rbsc_gen_rmat_pinned(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                                 uint64_t seed, rbsc_host_graph* out);
+void rbsc_host_graph_free_pinned(rbsc_host_graph* g);
 
 /* Directed Erdos-Renyi G(n, p), p = mean_degree / (n - 1), no self-loops,
  * rows sorted; and its random lift: every node copied `lift` times, every

@@ -207,6 +207,15 @@ class Context:
         g._keep = keep
         return g
 
+    def gen_rmat_pinned(self, scale: int, edge_factor: int, a=RMAT_ABC[0], b=RMAT_ABC[1], c=RMAT_ABC[2],
+                        seed: int = 1) -> "PinnedGraph":
+        """R-MAT generated on the device in source buckets into page-locked host
+        memory (rbsc_gen_rmat_pinned): the same arcs as gen_rmat_host."""
+        hg = _lib.HostGraph()
+        _check(self._lib, self._lib.rbsc_gen_rmat_pinned(self._h, scale, edge_factor, a, b, c, seed, ctypes.byref(hg)),
+               self._h)
+        return PinnedGraph(self._lib, hg)
+
     def from_device(self, n: int, m: int, d_off: int, d_idx: int, d_wt: int | None = None,
                     offset_bytes: int = 8) -> "Graph":
         c = _lib.Csr()
@@ -297,6 +306,29 @@ class Graph:
         i = ctypes.c_void_p()
         _check(lib, lib.rbsc_graph_device_csr(self._h, ctypes.byref(o), ctypes.byref(i)), self.ctx._h)
         return o.value, i.value
+
+
+class PinnedGraph:
+    """A host CSR in page-locked memory owned by the library; `off` and `idx`
+    are numpy views of it (valid until free())."""
+
+    def __init__(self, lib, hg):
+        self._lib, self._hg = lib, hg
+        self.n, self.m = int(hg.n), int(hg.m)
+        self.off = np.ctypeslib.as_array(hg.offsets, shape=(self.n + 1,))
+        self.idx = np.ctypeslib.as_array(hg.indices, shape=(max(self.m, 1),))[: self.m]
+
+    def free(self):
+        if getattr(self, "_hg", None) is not None:
+            self.off = self.idx = None
+            self._lib.rbsc_host_graph_free_pinned(ctypes.byref(self._hg))
+            self._hg = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
 
 
 def _host_graph_to_numpy(lib, hg: _lib.HostGraph):

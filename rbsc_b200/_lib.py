@@ -39,6 +39,7 @@ EXPORTED = [
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
     "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches", "rbsc_graph_upload_streamed",
+    "rbsc_gen_rmat_pinned", "rbsc_host_graph_free_pinned",
     "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
     "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
@@ -262,6 +263,10 @@ def load():
                                          ctypes.c_double, ctypes.c_uint64, P(vp)]
     lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_gen_rmat_pinned.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                         ctypes.c_double, ctypes.c_uint64, P(HostGraph)]
+    lib.rbsc_host_graph_free_pinned.argtypes = [P(HostGraph)]
+    lib.rbsc_host_graph_free_pinned.restype = None
     lib.rbsc_gen_er_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
     lib.rbsc_gen_lift_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
                                        ctypes.c_int32, P(HostGraph)]
@@ -280,7 +285,7 @@ def load():
     lib.rbsc_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int64, P(ServeResult)]
     lib.rbsc_serve_stats_get.argtypes = [vp, P(ServeStats)]
     for name in EXPORTED:
-        if name not in ("rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_destroy",
+        if name not in ("rbsc_serve_opts_default", "rbsc_host_graph_free_pinned", "rbsc_serve_footprint", "rbsc_serve_destroy",
                         "rbsc_serve_last_error","rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
                         "rbsc_graph_batch_free",
                         "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):

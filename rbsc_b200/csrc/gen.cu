@@ -92,6 +92,66 @@ __global__ void k_rmat_emit(uint64_t m0, uint32_t scale, const unsigned long lon
     if (i < m0 && keep[i]) idx[pos[i]] = (uint32_t)(keys[i] & mask);
 }
 
+// The first `hb` levels of an arc's descent fix the top hb bits of its
+// source: the bucket an arc belongs to is known before the remaining levels.
+__device__ __forceinline__ uint32_t rmat_src_top(const RmatParams& p, uint64_t base, uint32_t hb)
+{
+    uint32_t u = 0;
+    for (uint32_t l = 0; l < hb; ++l) {
+        const uint32_t r = (uint32_t)(fmix64(base + (uint64_t)(l + 1) * 0xd1b54a32d192ed03ull) >> 32);
+        u = (u << 1) | (r >= p.tab ? 1u : 0u);
+    }
+    return u;
+}
+
+// Histogram of the arcs over the top hb bits of their source.
+__global__ void k_rmat_src_hist(RmatParams p, uint64_t m0, uint32_t hb, unsigned long long* __restrict__ hist)
+{
+    extern __shared__ unsigned int s_hist[];
+    const uint32_t bins = 1u << hb;
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x) s_hist[i] = 0;
+    __syncthreads();
+    for (uint64_t e = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; e < m0; e += (uint64_t)gridDim.x * blockDim.x)
+        atomicAdd(&s_hist[rmat_src_top(p, fmix64(p.seed ^ (e * kGolden)), hb)], 1u);
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < bins; i += blockDim.x)
+        if (s_hist[i]) atomicAdd(&hist[i], (unsigned long long)s_hist[i]);
+}
+
+// Keys of the arcs whose source's top bits fall in [lo, hi), appended.
+__global__ void __launch_bounds__(256) k_rmat_bucket_keys(RmatParams p, uint64_t m0, uint32_t hb, uint32_t lo, uint32_t hi,
+                                                          unsigned long long* __restrict__ keys, uint32_t* __restrict__ count)
+{
+    __shared__ BlockReserveSmem<256> sm;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base_e = (uint64_t)blockIdx.x * blockDim.x; base_e < m0; base_e += stride) {
+        const uint64_t e = base_e + threadIdx.x;
+        bool take = false;
+        if (e < m0) {
+            const uint32_t top = rmat_src_top(p, fmix64(p.seed ^ (e * kGolden)), hb);
+            take = top >= lo && top < hi;
+        }
+        const uint32_t pos = block_reserve<256>(take, count, sm);
+        if (take) keys[pos] = rmat_key(p, e);
+    }
+}
+
+// Heads of the kept arcs of a bucket (sorted keys) into idx, and the offsets
+// of the bucket's sources [s_lo, s_hi): off[x - s_lo] = arc_base + first kept
+// arc of source x.
+__global__ void k_rmat_bucket_emit(uint64_t mb, uint32_t scale, uint64_t s_lo, uint64_t s_hi, uint64_t arc_base,
+                                   const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ keep,
+                                   const uint32_t* __restrict__ pos, uint32_t* __restrict__ idx, uint64_t* __restrict__ off)
+{
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > mb) return;
+    const uint64_t mask = (1ull << scale) - 1ull;
+    const uint64_t u = i < mb ? (keys[i] >> scale) : s_hi;  // sentinel past the bucket's last source
+    const int64_t prev = i == 0 ? (int64_t)s_lo - 1 : (int64_t)(keys[i - 1] >> scale);
+    for (int64_t x = prev + 1; x <= (int64_t)u && x < (int64_t)s_hi; ++x) off[x - s_lo] = arc_base + pos[i];
+    if (i < mb && keep[i]) idx[pos[i]] = (uint32_t)(keys[i] & mask);
+}
+
 }  // namespace
 
 #define CKG(call)                                                                  \
@@ -168,6 +228,118 @@ done:
     dev_free(ctx, tmp);
     if (g) rbsc_graph_free(g);
     return st;
+}
+
+// ---------------------------------------------------------------------------
+// device generator into page-locked host memory, in source buckets
+// ---------------------------------------------------------------------------
+extern "C" rbsc_status rbsc_gen_rmat_pinned(rbsc_ctx* ctx, uint32_t scale, uint32_t edge_factor, double a, double b, double c,
+                                            uint64_t seed, rbsc_host_graph* out)
+{
+    if (!ctx || !out) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    std::memset(out, 0, sizeof *out);
+    if (scale < 1 || scale > 30) return rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "scale must be in [1, 30]");
+    const uint64_t n = 1ull << scale;
+    const uint64_t m0 = (uint64_t)edge_factor << scale;
+    const uint32_t hb = std::min<uint32_t>(scale, 12);
+    const uint32_t bins = 1u << hb;
+    const RmatParams p = make_params(scale, a, b, c, seed);
+    cudaStream_t s = ctx->stream;
+    rbsc_status st = RBSC_OK;
+    unsigned long long *hist = nullptr, *keys0 = nullptr, *keys1 = nullptr;
+    uint32_t *keep = nullptr, *pos = nullptr, *cnt = nullptr, *didx = nullptr;
+    uint64_t* doff = nullptr;
+    void* tmp = nullptr;
+    std::vector<unsigned long long> h(bins);
+    uint64_t cap = 0, arcs = 0;
+    const unsigned grid = (unsigned)ctx->sm_count * 16;
+    CKG(cudaSetDevice(ctx->device));
+    // page-locked output: offsets, and heads for up to m0 arcs (duplicates removed later)
+    CKG(cudaHostAlloc((void**)&out->offsets, 8 * (n + 1), cudaHostAllocDefault));
+    CKG(cudaHostAlloc((void**)&out->indices, 4 * std::max<uint64_t>(m0, 1), cudaHostAllocDefault));
+    out->n = (uint32_t)n;
+    CKGS(dev_alloc(ctx, (void**)&hist, 8 * bins));
+    CKG(cudaMemsetAsync(hist, 0, 8 * bins, s));
+    ++rbsc::launch_counter();
+    k_rmat_src_hist<<<grid, 256, 4 * bins, s>>>(p, m0, hb, hist);
+    CKG(cudaGetLastError());
+    CKG(cudaMemcpyAsync(h.data(), hist, 8 * bins, cudaMemcpyDeviceToHost, s));
+    CKG(cudaStreamSynchronize(s));
+    // buckets of consecutive bins with at most `cap` arcs (at least one bin)
+    cap = std::max<uint64_t>(*std::max_element(h.begin(), h.end()), std::min<uint64_t>(m0, 1ull << 29));
+    if (cap > (1ull << 31)) {
+        st = rbsc_fail(ctx, RBSC_ERR_TOO_LARGE, "R-MAT: %llu arcs share the top %u source bits (limit 2^31)",
+                       (unsigned long long)cap, hb);
+        goto done;
+    }
+    CKGS(dev_alloc(ctx, (void**)&keys0, 8 * cap));
+    CKGS(dev_alloc(ctx, (void**)&keys1, 8 * cap));
+    CKGS(dev_alloc(ctx, (void**)&keep, 4 * (cap + 1)));
+    CKGS(dev_alloc(ctx, (void**)&pos, 4 * (cap + 1)));
+    CKGS(dev_alloc(ctx, (void**)&didx, 4 * cap));
+    CKGS(dev_alloc(ctx, (void**)&doff, 8 * n));
+    CKGS(dev_alloc(ctx, (void**)&cnt, 16));
+    CKGS(dev_alloc(ctx, &tmp, std::max(radix_temp_bytes(cap), scan_temp_bytes<uint32_t>(cap + 1)) + 1024));
+    for (uint32_t lo = 0; lo < bins;) {
+        uint32_t hi = lo + 1;
+        uint64_t kb = h[lo];
+        while (hi < bins && kb + h[hi] <= cap) kb += h[hi++];
+        uint32_t mb = 0;
+        CKG(cudaMemsetAsync(cnt, 0, 4, s));
+        ++rbsc::launch_counter();
+        k_rmat_bucket_keys<<<grid, 256, 0, s>>>(p, m0, hb, lo, hi, keys0, cnt);
+        CKG(cudaGetLastError());
+        CKG(cudaMemcpyAsync(&mb, cnt, 4, cudaMemcpyDeviceToHost, s));
+        CKG(cudaStreamSynchronize(s));
+        bool alt = false;
+        CKG(radix_sort<uint32_t>(keys0, keys1, (uint32_t*)nullptr, (uint32_t*)nullptr, mb, 0, 2 * (int)scale, tmp, s, &alt));
+        const unsigned long long* sorted = alt ? keys1 : keys0;
+        uint32_t mu = 0;
+        if (mb) {
+            ++rbsc::launch_counter();
+            k_rmat_keep<<<(unsigned)ceil_div<uint64_t>(mb, 256), 256, 0, s>>>(mb, scale, sorted, keep);
+            CKG(cudaGetLastError());
+            CKG((exclusive_scan<uint32_t, uint32_t>(keep, pos, mb, pos + mb, tmp, s)));
+            CKG(cudaMemcpyAsync(&mu, pos + mb, 4, cudaMemcpyDeviceToHost, s));
+            CKG(cudaStreamSynchronize(s));
+        } else {
+            CKG(cudaMemsetAsync(pos, 0, 4, s));
+        }
+        const uint64_t s_lo = (uint64_t)lo << (scale - hb), s_hi = (uint64_t)hi << (scale - hb);
+        ++rbsc::launch_counter();
+        k_rmat_bucket_emit<<<(unsigned)ceil_div<uint64_t>((uint64_t)mb + 1, 256), 256, 0, s>>>(mb, scale, s_lo, s_hi, arcs, sorted,
+                                                                                              keep, pos, didx, doff);
+        CKG(cudaGetLastError());
+        if (mu) CKG(cudaMemcpyAsync(out->indices + arcs, didx, 4 * (size_t)mu, cudaMemcpyDeviceToHost, s));
+        CKG(cudaMemcpyAsync(out->offsets + s_lo, doff, 8 * (s_hi - s_lo), cudaMemcpyDeviceToHost, s));
+        CKG(cudaStreamSynchronize(s));
+        arcs += mu;
+        lo = hi;
+    }
+    out->offsets[n] = arcs;
+    out->m = arcs;
+done:
+    cudaStreamSynchronize(s);
+    dev_free(ctx, (void*&)hist);
+    dev_free(ctx, (void*&)keys0);
+    dev_free(ctx, (void*&)keys1);
+    dev_free(ctx, (void*&)keep);
+    dev_free(ctx, (void*&)pos);
+    dev_free(ctx, (void*&)didx);
+    dev_free(ctx, (void*&)doff);
+    dev_free(ctx, (void*&)cnt);
+    dev_free(ctx, tmp);
+    if (st != RBSC_OK) rbsc_host_graph_free_pinned(out);
+    return st;
+}
+
+extern "C" void rbsc_host_graph_free_pinned(rbsc_host_graph* g)
+{
+    if (!g) return;
+    if (g->offsets) cudaFreeHost(g->offsets);
+    if (g->indices) cudaFreeHost(g->indices);
+    if (g->weights) cudaFreeHost(g->weights);
+    std::memset(g, 0, sizeof *g);
 }
 
 // ---------------------------------------------------------------------------

@@ -693,7 +693,8 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     // compacted arc sets: as large as the graph's own (in device memory), or
     // the resident capacity of a streamed graph; k_compact_decide copies only
     // what fits (and what fits 32-bit offsets)
-    const size_t cap = g->host_arcs ? (size_t)std::max<uint64_t>(g->resident_cap, 1) : (size_t)std::max<uint64_t>(g->m, 1);
+    const size_t cap = g->host_arcs ? (size_t)std::max<uint64_t>(g->resident_cap, 1)
+                                    : (size_t)std::max<uint64_t>(ceil_div<uint64_t>(3 * g->m, 4), 1);
     const size_t ctiles = ceil_div<uint64_t>(std::min<uint64_t>(cap, 0xffffffffull), kTileEdges);
     const size_t cpad = ctiles * kTileEdges;
     for (int d = 0; d < 2; ++d) {
@@ -849,8 +850,16 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         k_compact_rows<<<kgrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb);
         ++rbsc::launch_counter();
         k_compact_decide<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb);
-        ++rbsc::launch_counter();
-        k_compact_arcs<<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig);
+        if (g->arcs_on_host) {
+            // source arcs in host memory: a coalesced copy, then the bookkeeping
+            ++rbsc::launch_counter();
+            k_compact_copy_tiles<<<persistent_grid(ctx, g->ntiles, kNodeThreads / 32), kNodeThreads, 0, s>>>(g->d_as, g->cb);
+            ++rbsc::launch_counter();
+            k_compact_arcs<false><<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig);
+        } else {
+            ++rbsc::launch_counter();
+            k_compact_arcs<true><<<agrid, kNodeThreads, 0, s>>>(g->d_as, g->cb, g->d_sig);
+        }
     }
     ++rbsc::launch_counter();
     // no hand-off to the persistent kernel from a pass over host arcs: the
@@ -1097,7 +1106,7 @@ static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
     a.nsplit = g->nsplit;
     a.nodes = g->cb.nodes[0];
     a.compact_arcs = g->compact_arcs ? 1u : 0u;
-    a.dst_cap = g->host_arcs ? g->resident_cap : std::max<uint64_t>(g->m, 1);
+    a.dst_cap = g->host_arcs ? g->resident_cap : std::max<uint64_t>(ceil_div<uint64_t>(3 * g->m, 4), 1);
     a.arcctr = 0;
     g->arcs_on_host = g->host_arcs;
     *g->h_as = a;

@@ -1020,7 +1020,9 @@ static __global__ void k_compact_decide(ActiveSet* as, const RoundState* st, Com
 
 // Copies the arcs of the kept rows (16 destination arcs per thread), and
 // builds the destination's row-head bitmap, tile rows and split list.  A row
-// entering the split list gets its signatures zeroed here.
+// entering the split list gets its signatures zeroed here.  COPY false: the
+// bookkeeping only (the arcs were copied by k_compact_copy_tiles).
+template <bool COPY>
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet* __restrict__ as, CompactBufs bufs,
                                                                       Sig* __restrict__ sig)
 {
@@ -1060,8 +1062,10 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
                 src = dsrc[k];
             }
             if (e == rb) bits |= 1u << i;
-            didx[e] = sidx[src + (e - rb)];
-            if (swt) dwt[e] = swt[src + (e - rb)];
+            if (COPY) {
+                didx[e] = sidx[src + (e - rb)];
+                if (swt) dwt[e] = swt[src + (e - rb)];
+            }
         }
         *reinterpret_cast<uint16_t*>(bufs.head8[d] + (e0 >> 3)) = (uint16_t)bits;
         if ((e0 & (kTileEdges - 1u)) == 0u) {
@@ -1071,6 +1075,62 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
                 const uint32_t p = atomicAdd(&as->splitctr, 1u);
                 bufs.split[d][p] = node;
                 sig_store(&sig[node], 0ull, 0u);
+            }
+        }
+    }
+}
+
+// The copy of k_compact_arcs for a source arc set in host memory (read over
+// the host link): one warp per 512-arc destination tile, lane l copying arcs
+// l, l+32, ... so that each load of the warp reads 32 consecutive arcs of one
+// row (one request) instead of 32 scattered ones.
+static __global__ void __launch_bounds__(kNodeThreads) k_compact_copy_tiles(const ActiveSet* __restrict__ as, CompactBufs bufs)
+{
+    if (!as->do_copy) return;
+    const uint32_t nk = as->new_K;
+    const uint32_t nm = as->new_m;
+    const uint32_t d = as->dst_arcs;
+    const uint32_t* __restrict__ doff = bufs.off[d];
+    const uint64_t* __restrict__ dsrc = bufs.src[d];
+    uint32_t* __restrict__ didx = bufs.idx[d];
+    uint64_t* __restrict__ dwt = bufs.wt[d];
+    const uint32_t* __restrict__ sidx = as->idx;
+    const uint64_t* __restrict__ swt = as->wt;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t tiles = (nm + kTileEdges - 1u) / kTileEdges;
+    const uint32_t warps = gridDim.x * (kNodeThreads / 32);
+    for (uint32_t t = blockIdx.x * (kNodeThreads / 32) + (threadIdx.x >> 5); t < tiles; t += warps) {
+        const uint32_t e0 = t * kTileEdges + lane;
+        if (e0 >= nm) continue;
+        uint32_t lo = 0, hi = nk - 1u;
+        while (lo < hi) {
+            const uint32_t mid = lo + ((hi - lo + 1u) >> 1);
+            if (doff[mid] <= e0) lo = mid; else hi = mid - 1u;
+        }
+        uint32_t k = lo, rb = doff[k], re = doff[k + 1];
+        uint64_t src = dsrc[k];
+        uint32_t v[kTileEdges / 32];
+        uint64_t w[kTileEdges / 32];
+#pragma unroll
+        for (uint32_t i = 0; i < kTileEdges / 32; ++i) {
+            const uint32_t e = e0 + 32u * i;
+            if (e < nm) {
+                while (e >= re) {
+                    ++k;
+                    rb = re;
+                    re = doff[k + 1];
+                    src = dsrc[k];
+                }
+                v[i] = sidx[src + (e - rb)];
+                if (swt) w[i] = swt[src + (e - rb)];
+            }
+        }
+#pragma unroll
+        for (uint32_t i = 0; i < kTileEdges / 32; ++i) {
+            const uint32_t e = e0 + 32u * i;
+            if (e < nm) {
+                didx[e] = v[i];
+                if (swt) dwt[e] = w[i];
             }
         }
     }

@@ -120,3 +120,22 @@ def test_streamed_graph_loop_and_host_loop(ctx):
         finally:
             ctx.set_opts(use_graph=True)
         assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
+
+
+def test_pinned_generator_matches_host_generator(ctx):
+    """rbsc_gen_rmat_pinned (device, source buckets, page-locked output) gives
+    the arcs of rbsc_gen_rmat_host; a streamed refinement of it equals the
+    in-HBM one."""
+    off, idx = R.gen_rmat_host(14, 16, seed=5)
+    pg = ctx.gen_rmat_pinned(14, 16, seed=5)
+    try:
+        assert pg.n == len(off) - 1 and pg.m == len(idx)
+        assert np.array_equal(pg.off, off) and np.array_equal(pg.idx, idx)
+        init = R.degree_bucket_colors(off)
+        ref = ctx.upload(off, idx).refine(init)
+        g = ctx.upload_streamed(pg.off, pg.idx)
+        r = g.refine(init)
+        g.free()
+        assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
+    finally:
+        pg.free()
