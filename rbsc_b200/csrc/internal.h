@@ -59,6 +59,7 @@ struct rbsc_graph {
     uint32_t* d_initlab = nullptr;
     rbsc::Sig* d_sig = nullptr;  // per-node signature (16 B)
     uint32_t* d_slot = nullptr;
+    uint32_t* d_joined = nullptr;    // per node: pass in which a member joined its representative's class
     uint32_t* d_out = nullptr;
     void* d_rank = nullptr;          // first pass: dense class ranks (uint8 / uint16)
     uint32_t* d_srank = nullptr;     // rank of the initial class claimed at each table slot

@@ -282,6 +282,7 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free(g->ctx, (void*&)g->d_initlab);
     dev_free(g->ctx, (void*&)g->d_sig);
     dev_free(g->ctx, (void*&)g->d_slot);
+    dev_free(g->ctx, (void*&)g->d_joined);
     dev_free(g->ctx, (void*&)g->d_tab);
     dev_free(g->ctx, (void*&)g->d_srank);
     dev_free(g->ctx, (void*&)g->d_st);
@@ -673,6 +674,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_initlab, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_sig, sizeof(Sig) * n));
     CKS(dev_alloc(ctx, (void**)&g->d_slot, 4 * n));
+    CKS(dev_alloc(ctx, (void**)&g->d_joined, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_out, 4 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_rank, 2 * n));
     CKS(dev_alloc(ctx, (void**)&g->d_small, 256));
@@ -830,10 +832,12 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         if (t) CK(cudaEventRecord(t->ev[3], s));
     } else {
         ++rbsc::launch_counter();
-        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab, g->log2tab, g->d_slot);
+        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab, g->log2tab, g->d_slot,
+                                                     g->d_joined);
         if (t) CK(cudaEventRecord(t->ev[3], s));
         ++rbsc::launch_counter();
-        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_tab, g->d_slot, g->d_sig);
+        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_tab, g->d_slot, g->d_sig,
+                                                      g->d_joined);
     }
     ++rbsc::launch_counter();
     k_follow<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_pairs, g->d_col[0]);
@@ -1001,6 +1005,7 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     a.tab_entries = 1ull << g->log2tab;
     a.slot = g->d_slot;
     a.pairs = g->d_pairs;
+    a.joined = g->d_joined;
     a.gs = g->d_gsync;
     a.weighted = g->weighted ? 1 : 0;
     void* args[] = {&a};
@@ -1263,6 +1268,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     g->first_sig_arcs = 0;
     g->streamed_bytes = 0;
     g->streamed_passes = 0;
+    CK(cudaMemsetAsync(g->d_joined, 0, 4 * (size_t)n, s));
     RoundState& hs = *g->h_st;
     std::memset(&hs, 0, sizeof hs);
     hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);

@@ -535,12 +535,26 @@ __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
     if ((threadIdx.x & 31) == 0 && nb) atomicAdd(counter, (uint32_t)__popc(nb));
 }
 
+// Slot of a listed node that keeps its block's label: the block's
+// representative r (its smallest node), or a node whose signature equals r's.
+constexpr uint32_t kRepSlot = 0xffffffffu;
+
 // Hashed pass over the node list (grid-stride by blocks); returns this
 // thread's count of new blocks.
+//
+// Representative fast path: the class of node u is (label, signature); the
+// block's representative r = label is its smallest node, so every node whose
+// signature equals r's lands in r's class, whose smallest member -- the new
+// label -- is r again.  Those nodes (and r itself) skip the relabel table:
+// they keep their colour, and mark joined[r] (= the pass tag) so that r knows
+// its class has another member.  Only the nodes that differ from their
+// representative go through the table, keyed by (label, signature) as before.
+// Late passes, where few blocks split, do almost no table work.
 __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                      const uint32_t* __restrict__ col,
                                                      const Sig* __restrict__ sig, Entry* __restrict__ tab,
-                                                     uint32_t log2size, uint32_t* __restrict__ slot)
+                                                     uint32_t log2size, uint32_t* __restrict__ slot,
+                                                     uint32_t* __restrict__ joined)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
@@ -551,6 +565,7 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
     // probe only the first 2^k entries, 2^k >= 2 * list length: the table of
     // a late pass with few active nodes stays in L2
     const uint32_t log2win = table_window(nn, log2size);
+    const uint32_t tag = st->round + 1u;
     uint32_t made = 0;
     for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
         const uint32_t i = base + (threadIdx.x & 31);
@@ -558,7 +573,8 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
         const uint32_t e = active ? nodes[i] : 0u;
         const uint32_t u = e & ~kRepFlag;
         const uint32_t c = active ? col[u] : kSingleton;
-        const bool need = active && !(c & kSingleton);
+        bool need = active && !(c & kSingleton);
+        bool is_rep = false;
         uint64_t k1 = 0;
         uint32_t k2 = stamp;
         if (need) {
@@ -570,10 +586,28 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
                 s1 = (hb >= 64) ? 0ull : (s1 & ((1ull << hb) - 1ull));
                 s2 = 0;
             }
-            k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
-            k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
+            bool keep = u == lab;
+            is_rep = keep;
+            if (!keep) {
+                uint64_t r1;
+                uint32_t r2;
+                sig_load(&sig[lab], r1, r2);
+                if (hb) {
+                    r1 = (hb >= 64) ? 0ull : (r1 & ((1ull << hb) - 1ull));
+                    r2 = 0;
+                }
+                keep = r1 == s1 && r2 == s2;
+                if (keep && joined[lab] != tag) joined[lab] = tag;
+            }
+            if (keep) {
+                slot[i] = kRepSlot;
+                need = false;
+            } else {
+                k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
+                k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
+            }
         }
-        bool nb = active && !need;
+        bool nb = (active && !need && !(active && !(c & kSingleton) && !is_rep)) || is_rep;
         insert_warp(need, u, i, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
         made += nb ? 1u : 0u;
     }
@@ -584,10 +618,10 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
                                                                      const uint32_t* __restrict__ col,
                                                                      const Sig* __restrict__ sig,
                                                                      Entry* __restrict__ tab, uint32_t log2size,
-                                                                     uint32_t* __restrict__ slot)
+                                                                     uint32_t* __restrict__ slot, uint32_t* __restrict__ joined)
 {
     __shared__ BlockReserveSmem<kNodeThreads> sm;
-    const uint32_t made = insert_list_body(as, st, col, sig, tab, log2size, slot);
+    const uint32_t made = insert_list_body(as, st, col, sig, tab, log2size, slot, joined);
     block_count<kNodeThreads>(made, &st->count, sm);
 }
 
@@ -751,8 +785,10 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 template <bool NC>
 __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                   uint32_t* __restrict__ col, const Entry* __restrict__ tab,
-                                                  const uint32_t* __restrict__ slot, Sig* __restrict__ sig)
+                                                  const uint32_t* __restrict__ slot, Sig* __restrict__ sig,
+                                                  const uint32_t* __restrict__ joined)
 {
+    const uint32_t tag = st->round + 1u;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
     const uint32_t stride = gridDim.x * kNodeThreads;
@@ -776,7 +812,16 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
 #pragma unroll
         for (int j = 0; j < U; ++j) {
             if (u[j] == 0xffffffffu) continue;
-            const uint32_t nc = relabel_one<NC>(c[j], tab, s[j]);
+            uint32_t nc = c[j];
+            if (s[j] == kRepSlot) {
+                // kept its block's label; the representative of a class that
+                // nobody joined (and that stands for no follower) is alone
+                if (!(c[j] & kSingleton) && (c[j] & kLabelMask) == u[j] && !rep[j] &&
+                    (NC ? __ldg(joined + u[j]) : __ldcg(joined + u[j])) != tag)
+                    nc = c[j] | kSingleton;
+            } else {
+                nc = relabel_one<NC>(c[j], tab, s[j]);
+            }
             if (nc != c[j]) {
                 col[u[j]] = nc;
                 if (rep[j]) st->rep_changed = 1u;
@@ -795,9 +840,9 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const Acti
                                                                       RoundState* __restrict__ st, uint32_t* __restrict__ col,
                                                                       const Entry* __restrict__ tab,
                                                                       const uint32_t* __restrict__ slot,
-                                                                      Sig* __restrict__ sig)
+                                                                      Sig* __restrict__ sig, const uint32_t* __restrict__ joined)
 {
-    relabel_list_body<true>(as, st, col, tab, slot, sig);
+    relabel_list_body<true>(as, st, col, tab, slot, sig, joined);
 }
 
 // New colours of all nodes (after k_insert_all), in place.
@@ -1404,6 +1449,7 @@ struct PersistArgs {
     const uint2* pairs;
     GridSync* gs;
     int weighted;
+    uint32_t* joined;
 };
 
 static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
@@ -1416,10 +1462,10 @@ static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(Pe
         if (a.weighted) signature_body<true, uint32_t, false>(a.as, a.st, a.col, a.sig);
         else signature_body<false, uint32_t, false>(a.as, a.st, a.col, a.sig);
         if (!grid_barrier(a.gs, a.st)) return;
-        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig, a.tab, a.log2tab, a.slot);
+        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined);
         block_count<kNodeThreads>(made, &a.st->count, sm);
         if (!grid_barrier(a.gs, a.st)) return;
-        relabel_list_body<false>(a.as, a.st, a.col, a.tab, a.slot, a.sig);
+        relabel_list_body<false>(a.as, a.st, a.col, a.tab, a.slot, a.sig, a.joined);
         if (!grid_barrier(a.gs, a.st)) return;
         follow_body(a.as, a.st, a.pairs, a.col);
         if (!grid_barrier(a.gs, a.st)) return;
