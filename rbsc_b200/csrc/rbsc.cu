@@ -278,6 +278,7 @@ static void graph_release_refine(rbsc_graph* g)
         dev_free(g->ctx, (void*&)g->cb.tile_row[d]);
         dev_free(g->ctx, (void*&)g->cb.split[d]);
         dev_free(g->ctx, (void*&)g->cb.nodes[d]);
+        dev_free(g->ctx, (void*&)g->cb.chunk_row[d]);
     }
     dev_free(g->ctx, (void*&)g->d_initlab);
     dev_free(g->ctx, (void*&)g->d_sig);
@@ -710,6 +711,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
         CKS(dev_alloc(ctx, (void**)&g->cb.head8[d], cpad / 8 + 16));
         CKS(dev_alloc(ctx, (void**)&g->cb.tile_row[d], 4 * (ctiles + 1)));
         CKS(dev_alloc(ctx, (void**)&g->cb.split[d], 4 * (ctiles + 1)));
+        CKS(dev_alloc(ctx, (void**)&g->cb.chunk_row[d], 4 * (cpad / 16 + 1)));
     }
     CK(cudaMemsetAsync(g->d_sig, 0, sizeof(Sig) * n, ctx->stream));
     CK(cudaMemsetAsync(g->d_tab, 0, sizeof(Entry) << g->log2tab, ctx->stream));

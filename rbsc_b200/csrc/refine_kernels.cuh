@@ -130,6 +130,7 @@ struct CompactBufs {
     uint32_t* tile_row[2];
     uint32_t* split[2];
     uint32_t* nodes[2];
+    uint32_t* chunk_row[2];  // row holding the first arc of each 16-arc destination chunk
 };
 
 // Pass modes of the exact (non-hashed) relabels over all nodes.
@@ -985,6 +986,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
     uint32_t* __restrict__ drows = bufs.rows[d];
     uint32_t* __restrict__ doff = bufs.off[d];
     uint64_t* __restrict__ dsrc = bufs.src[d];
+    uint32_t* __restrict__ chunk_row = bufs.chunk_row[d];
     const uint32_t stride = gridDim.x * kNodeThreads;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (uint32_t base = blockIdx.x * kNodeThreads; base < K; base += stride) {
@@ -1035,6 +1037,11 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
             drows[kn] = node;
             doff[kn] = (uint32_t)pos;
             dsrc[kn] = start;
+            // the 16-arc destination chunks that start in this row (within the
+            // buffers: past the capacity nothing is copied anyway)
+            const uint32_t p0 = (uint32_t)pos;
+            if (deg && (uint64_t)p0 + deg <= as->dst_cap)
+                for (uint32_t c = (p0 + 15u) >> 4; (c << 4) < p0 + deg; ++c) chunk_row[c] = kn;
         }
         __syncthreads();
     }
@@ -1084,15 +1091,11 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
     const uint64_t* __restrict__ swt = as->wt;
     const uint32_t chunks = (nm + 15u) / 16u;
     const uint32_t stride = gridDim.x * kNodeThreads;
+    const uint32_t* __restrict__ chunk_row = bufs.chunk_row[d];
     for (uint32_t ch = blockIdx.x * kNodeThreads + threadIdx.x; ch < chunks; ch += stride) {
         const uint32_t e0 = ch * 16u;
-        // row holding arc e0: largest k with doff[k] <= e0
-        uint32_t lo = 0, hi = nk - 1u;
-        while (lo < hi) {
-            const uint32_t mid = lo + ((hi - lo + 1u) >> 1);
-            if (doff[mid] <= e0) lo = mid; else hi = mid - 1u;
-        }
-        const uint32_t k0 = lo;
+        // row holding arc e0 (recorded by k_compact_rows)
+        const uint32_t k0 = chunk_row[ch];
         uint32_t k = k0;
         uint32_t rb = doff[k], re = doff[k + 1];
         uint64_t src = dsrc[k];
@@ -1141,18 +1144,21 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_copy_tiles(cons
     uint64_t* __restrict__ dwt = bufs.wt[d];
     const uint32_t* __restrict__ sidx = as->idx;
     const uint64_t* __restrict__ swt = as->wt;
+    const uint32_t* __restrict__ chunk_row = bufs.chunk_row[d];
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t tiles = (nm + kTileEdges - 1u) / kTileEdges;
     const uint32_t warps = gridDim.x * (kNodeThreads / 32);
+    (void)nk;
     for (uint32_t t = blockIdx.x * (kNodeThreads / 32) + (threadIdx.x >> 5); t < tiles; t += warps) {
         const uint32_t e0 = t * kTileEdges + lane;
         if (e0 >= nm) continue;
-        uint32_t lo = 0, hi = nk - 1u;
-        while (lo < hi) {
-            const uint32_t mid = lo + ((hi - lo + 1u) >> 1);
-            if (doff[mid] <= e0) lo = mid; else hi = mid - 1u;
+        // from the row of e0's 16-arc chunk, at most 15 arcs ahead
+        uint32_t k = chunk_row[e0 >> 4], rb = doff[k], re = doff[k + 1];
+        while (e0 >= re) {
+            ++k;
+            rb = re;
+            re = doff[k + 1];
         }
-        uint32_t k = lo, rb = doff[k], re = doff[k + 1];
         uint64_t src = dsrc[k];
         uint32_t v[kTileEdges / 32];
         uint64_t w[kTileEdges / 32];
