@@ -233,6 +233,14 @@ def run_ours(args, rank, world, local_rank):
 
     for _ in range(args.warmup):
         r = g.refine_device(d_init.data_ptr(), d_out.data_ptr())
+    # the pass kernels' knobs chosen by the library's autotuner on this graph
+    # (before the timed region; every candidate checked for the same result)
+    tune = None
+    if not args.no_autotune:
+        tune = g.autotune(d_init.data_ptr())
+        tune = {k: v for k, v in tune.items() if k != "table"}
+        for _ in range(args.warmup):
+            g.refine_device(d_init.data_ptr(), d_out.data_ptr())
     barrier()
     torch.cuda.synchronize()
     clocks = Clocks(local_rank)
@@ -348,7 +356,7 @@ def run_ours(args, rank, world, local_rank):
                 "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
-                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "batched": batched,
+                "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "autotune": tune, "batched": batched,
                 "served": served, "streamed": streamed}
         print(json.dumps(line))
     g.free()
@@ -384,6 +392,11 @@ def run_batched(args, ctx, world, dist):
     off_p, idx_p, lab_p = _pinned_copy(off), _pinned_copy(idx), _pinned_copy(lab)
     bufs = R.batch_buffers(n, G, alloc=lambda k, dt: _pinned(k, dt))
     rg = ctx.upload(off_p, idx_p)
+    tune = None
+    if not args.no_autotune:
+        d_lab = torch.from_numpy(lab.view(np.int32)).cuda()
+        tune = rg.autotune(d_lab.data_ptr())
+        tune = {k: v for k, v in tune.items() if k != "table"}
     for _ in range(2):
         rg.batch_refine(gn, lab_p, out=bufs)
     res_t, res_dev = [], []
@@ -435,7 +448,7 @@ def run_batched(args, ctx, world, dist):
             "resident_graphs_per_s": G * world / res_s, "resident_ms": 1000.0 * res_s,
             "device_ms": float(np.median(res_dev)),
             "per_launch_graphs_per_s": S * world / per_t, "per_launch_resident_graphs_per_s": S * world / per_res_t,
-            "per_launch_sample": S,
+            "per_launch_sample": S, "autotune": tune,
             "speedup": (G / one_s) / (S / per_t), "speedup_resident": (G / res_s) / (S / per_res_t),
             "paths": {"batched": "rbsc_batch_refine: host CSR + labels in (pinned), colours, local labels, "
                                  "histograms, fingerprints out",
@@ -642,6 +655,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct graphs the requests draw from")
     ap.add_argument("--serve-slots", type=int, default=2)
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default pass-kernel knobs")
     ap.add_argument("--no-persist", action="store_true",
                     help="every pass as separate launches (no persistent kernel for small active sets)")
     ap.add_argument("--profile-refine", action="store_true",

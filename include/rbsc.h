@@ -72,7 +72,11 @@ typedef struct {
                                  the exact check and repair path can be exercised.      */
     int32_t no_persist;       /* 1: never hand small active sets to the persistent
                                  kernel (every pass stays one launch per phase)         */
-    int32_t reserved[6];
+    int32_t persist_log2;     /* the persistent kernel takes over once the active arcs
+                                 and listed nodes are both <= 2^persist_log2
+                                 (0 = default 22)                                       */
+    int32_t grid_per_sm;      /* blocks per SM of the pass kernels' grids (0 = 16)      */
+    int32_t reserved[4];
 } rbsc_opts;
 
 typedef struct {
@@ -243,6 +247,39 @@ typedef struct {
 rbsc_status rbsc_refine_edge_batches(rbsc_ctx* ctx, const rbsc_csr* host_graph, uint64_t edge_batch_size,
                                      int32_t aggressive, uint32_t* out_labels, rbsc_stats* stats,
                                      rbsc_edge_batch_info* info);
+
+/* ---- autotuning (no reference counterpart) --------------------------------
+ * Times refinements of a resident graph (d_init_colors: device colours or
+ * NULL) under every combination of the candidate knobs below and returns the
+ * fastest as options (rbsc_ctx_set_opts applies them).  Every candidate must
+ * give the same blocks and rounds as the context's current options; a
+ * candidate that does not is reported as failed and never chosen.  A zero or
+ * empty list keeps the context's current value for that knob. */
+#define RBSC_TUNE_MAX 8
+typedef struct {
+    int32_t persist_log2[RBSC_TUNE_MAX];  /* hand-off thresholds to try (-1 = never hand off) */
+    uint32_t n_persist;
+    int32_t grid_per_sm[RBSC_TUNE_MAX];
+    uint32_t n_grid;
+    int32_t relabel[RBSC_TUNE_MAX];       /* RBSC_RELABEL_HASH / _SORT                      */
+    uint32_t n_relabel;
+    int32_t use_graph[RBSC_TUNE_MAX];     /* CUDA-graph loop 1 / host loop 0                */
+    uint32_t n_use_graph;
+    uint32_t reps;                        /* timed refinements per candidate (0 = 3)         */
+} rbsc_tune_space;
+
+typedef struct {
+    uint32_t candidates;      /* combinations timed                                   */
+    uint32_t failed;          /* candidates whose result differed (never chosen)      */
+    double best_ms;           /* median device time of the chosen candidate           */
+    double default_ms;        /* median device time under the context's options       */
+    double ms[64];            /* median device time of candidate i (first 64)         */
+    rbsc_opts opts[64];       /* the options of candidate i (first 64)               */
+} rbsc_tune_report;
+
+void rbsc_tune_space_default(rbsc_tune_space* space);
+rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init_colors,
+                                const rbsc_tune_space* space, rbsc_opts* best, rbsc_tune_report* report);
 
 /* ---- input formats (reference: read_graph, rbsc.cu:156-180) -------------- */
 

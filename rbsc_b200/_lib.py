@@ -39,7 +39,7 @@ EXPORTED = [
     "rbsc_gen_rmat_host", "rbsc_graph_profile", "rbsc_refine_noalloc", "rbsc_ctx_trim",
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
     "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches", "rbsc_graph_upload_streamed",
-    "rbsc_gen_rmat_pinned", "rbsc_host_graph_free_pinned",
+    "rbsc_gen_rmat_pinned", "rbsc_host_graph_free_pinned", "rbsc_tune_space_default", "rbsc_graph_autotune",
     "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
     "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
@@ -57,7 +57,9 @@ class Opts(ctypes.Structure):
         ("seed", ctypes.c_uint64),
         ("test_hash_bits", ctypes.c_int32),
         ("no_persist", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("persist_log2", ctypes.c_int32),
+        ("grid_per_sm", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 4),
     ]
 
 
@@ -154,6 +156,34 @@ class BatchResult(ctypes.Structure):
         ("hist_offsets", ctypes.c_void_p),
         ("hist_colors", ctypes.c_void_p),
         ("hist_counts", ctypes.c_void_p),
+    ]
+
+
+TUNE_MAX = 8
+
+
+class TuneSpace(ctypes.Structure):
+    _fields_ = [
+        ("persist_log2", ctypes.c_int32 * TUNE_MAX),
+        ("n_persist", ctypes.c_uint32),
+        ("grid_per_sm", ctypes.c_int32 * TUNE_MAX),
+        ("n_grid", ctypes.c_uint32),
+        ("relabel", ctypes.c_int32 * TUNE_MAX),
+        ("n_relabel", ctypes.c_uint32),
+        ("use_graph", ctypes.c_int32 * TUNE_MAX),
+        ("n_use_graph", ctypes.c_uint32),
+        ("reps", ctypes.c_uint32),
+    ]
+
+
+class TuneReport(ctypes.Structure):
+    _fields_ = [
+        ("candidates", ctypes.c_uint32),
+        ("failed", ctypes.c_uint32),
+        ("best_ms", ctypes.c_double),
+        ("default_ms", ctypes.c_double),
+        ("ms", ctypes.c_double * 64),
+        ("opts", Opts * 64),
     ]
 
 
@@ -263,6 +293,9 @@ def load():
                                          ctypes.c_double, ctypes.c_uint64, P(vp)]
     lib.rbsc_gen_rmat_host.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                        ctypes.c_double, ctypes.c_uint64, ctypes.c_int32, P(HostGraph)]
+    lib.rbsc_tune_space_default.argtypes = [P(TuneSpace)]
+    lib.rbsc_tune_space_default.restype = None
+    lib.rbsc_graph_autotune.argtypes = [vp, vp, vp, P(TuneSpace), P(Opts), P(TuneReport)]
     lib.rbsc_gen_rmat_pinned.argtypes = [vp, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
                                          ctypes.c_double, ctypes.c_uint64, P(HostGraph)]
     lib.rbsc_host_graph_free_pinned.argtypes = [P(HostGraph)]
@@ -285,7 +318,7 @@ def load():
     lib.rbsc_serve_wait.argtypes = [vp, ctypes.c_uint64, ctypes.c_int64, P(ServeResult)]
     lib.rbsc_serve_stats_get.argtypes = [vp, P(ServeStats)]
     for name in EXPORTED:
-        if name not in ("rbsc_serve_opts_default", "rbsc_host_graph_free_pinned", "rbsc_serve_footprint", "rbsc_serve_destroy",
+        if name not in ("rbsc_serve_opts_default", "rbsc_host_graph_free_pinned", "rbsc_tune_space_default", "rbsc_serve_footprint", "rbsc_serve_destroy",
                         "rbsc_serve_last_error","rbsc_abi_version", "rbsc_opts_default", "rbsc_ctx_create", "rbsc_ctx_destroy", "rbsc_ctx_trim",
                         "rbsc_graph_batch_free",
                         "rbsc_last_error", "rbsc_graph_free", "rbsc_host_graph_free"):

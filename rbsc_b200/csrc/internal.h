@@ -109,6 +109,8 @@ struct rbsc_graph {
     cudaGraphExec_t loop_exec = nullptr;
     int loop_relabel = -1;
     int loop_no_persist = -1;
+    int loop_persist_log2 = -2;
+    int loop_grid_per_sm = -1;
     float first_sig_ms = 0.f;       // the last refinement's first signature kernel
     uint64_t first_sig_arcs = 0;
     uint64_t body_kernels = 0;  // kernels in one iteration of the captured loop

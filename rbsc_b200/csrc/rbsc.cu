@@ -721,13 +721,20 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
 }
 
 // The persistent kernel takes over once both the active arcs and the listed
-// nodes are at most these.
-constexpr uint64_t kPersistArcs = 1ull << 22;
-constexpr uint32_t kPersistNodes = 1u << 22;
+// nodes are at most 2^persist_log2 (option; default 22).
+static uint64_t persist_limit(const rbsc_ctx* ctx)
+{
+    const int32_t l = ctx->opts.persist_log2;
+    if (l < 0) return 0;
+    return 1ull << (l == 0 ? 22 : std::min(l, 31));
+}
 
+// Grids of the pass kernels: one thread (or warp) per unit of work, at most
+// grid_per_sm blocks per SM (option; default 16), striding beyond.
 static unsigned persistent_grid(rbsc_ctx* ctx, uint64_t work, unsigned per_block)
 {
-    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(work, per_block), (uint64_t)ctx->sm_count * 16));
+    const uint64_t per_sm = ctx->opts.grid_per_sm > 0 ? (uint64_t)ctx->opts.grid_per_sm : 16ull;
+    return (unsigned)std::max<uint64_t>(1, std::min<uint64_t>(ceil_div<uint64_t>(work, per_block), (uint64_t)ctx->sm_count * per_sm));
 }
 
 // CUDA events around the kernels of one pass (profiling only).
@@ -871,7 +878,9 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     // no hand-off to the persistent kernel from a pass over host arcs: the
     // next pass sees whether the compaction brought them into device memory
     const bool persist = hash && !ctx->opts.no_persist && !g->arcs_on_host;
-    k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb, persist ? kPersistArcs : 0ull, kPersistNodes, h, use_handle);
+    const uint64_t plim = persist_limit(ctx);
+    k_compact_finalize<<<1, 1, 0, s>>>(g->d_as, g->d_st, g->cb, persist ? plim : 0ull, (uint32_t)std::min<uint64_t>(plim, 0xffffffffull),
+                                       h, use_handle);
     if (t) CK(cudaEventRecord(t->ev[5], s));
     CK(cudaGetLastError());
     return RBSC_OK;
@@ -879,7 +888,9 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
 
 static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
 {
-    if (g->loop_exec && g->loop_relabel == ctx->opts.relabel && g->loop_no_persist == ctx->opts.no_persist) return RBSC_OK;
+    if (g->loop_exec && g->loop_relabel == ctx->opts.relabel && g->loop_no_persist == ctx->opts.no_persist &&
+        g->loop_persist_log2 == ctx->opts.persist_log2 && g->loop_grid_per_sm == ctx->opts.grid_per_sm)
+        return RBSC_OK;
     if (g->loop_exec) cudaGraphExecDestroy(g->loop_exec);
     if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
     g->loop_exec = nullptr;
@@ -915,6 +926,8 @@ static rbsc_status build_loop_graph(rbsc_ctx* ctx, rbsc_graph* g)
     CK(cudaGraphInstantiate(&g->loop_exec, g->loop_graph, 0));
     g->loop_relabel = ctx->opts.relabel;
     g->loop_no_persist = ctx->opts.no_persist;
+    g->loop_persist_log2 = ctx->opts.persist_log2;
+    g->loop_grid_per_sm = ctx->opts.grid_per_sm;
     return RBSC_OK;
 }
 
@@ -1496,5 +1509,105 @@ extern "C" rbsc_status rbsc_graph_degree_colors(rbsc_ctx* ctx, rbsc_graph* g, ui
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(ctx->stream));
     }
+    return RBSC_OK;
+}
+
+// ---------------------------------------------------------------------------
+// autotuning
+// ---------------------------------------------------------------------------
+extern "C" void rbsc_tune_space_default(rbsc_tune_space* sp)
+{
+    std::memset(sp, 0, sizeof *sp);
+    const int32_t pl[] = {18, 20, 22, 24, -1};
+    for (int32_t v : pl) sp->persist_log2[sp->n_persist++] = v;
+    const int32_t gr[] = {4, 8, 16, 32};
+    for (int32_t v : gr) sp->grid_per_sm[sp->n_grid++] = v;
+    sp->relabel[sp->n_relabel++] = RBSC_RELABEL_HASH;
+    sp->use_graph[sp->n_use_graph++] = 1;
+    sp->use_graph[sp->n_use_graph++] = 0;
+    sp->reps = 3;
+}
+
+extern "C" rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init, const rbsc_tune_space* space,
+                                           rbsc_opts* best, rbsc_tune_report* report)
+{
+    if (!ctx || !g || !best) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null argument");
+    rbsc_tune_space sp;
+    if (space) sp = *space;
+    else rbsc_tune_space_default(&sp);
+    const rbsc_opts base = ctx->opts;
+    auto list = [](const int32_t* v, uint32_t n, int32_t cur) {
+        std::vector<int32_t> out(v, v + std::min<uint32_t>(n, RBSC_TUNE_MAX));
+        if (out.empty()) out.push_back(cur);
+        return out;
+    };
+    const auto pl = list(sp.persist_log2, sp.n_persist, base.persist_log2);
+    const auto gr = list(sp.grid_per_sm, sp.n_grid, base.grid_per_sm);
+    const auto rl = list(sp.relabel, sp.n_relabel, base.relabel);
+    const auto ug = list(sp.use_graph, sp.n_use_graph, base.use_graph);
+    const uint32_t reps = sp.reps ? sp.reps : 3;
+    rbsc_tune_report rep;
+    std::memset(&rep, 0, sizeof rep);
+    // one candidate: a warm-up refinement, then `reps` timed ones
+    auto time_opts = [&](const rbsc_opts& o, double* med, uint32_t* blocks, uint32_t* rounds) -> rbsc_status {
+        ctx->opts = o;
+        rbsc_stats st;
+        rbsc_status s = refine_resident(ctx, g, d_init, nullptr, &st, nullptr);
+        if (s != RBSC_OK) return s;
+        std::vector<double> t;
+        for (uint32_t r = 0; r < reps; ++r) {
+            s = refine_resident(ctx, g, d_init, nullptr, &st, nullptr);
+            if (s != RBSC_OK) return s;
+            t.push_back(st.device_ms);
+        }
+        std::sort(t.begin(), t.end());
+        *med = t[t.size() / 2];
+        *blocks = st.blocks;
+        *rounds = st.rounds;
+        return RBSC_OK;
+    };
+    uint32_t b0 = 0, r0 = 0;
+    rbsc_status s = time_opts(base, &rep.default_ms, &b0, &r0);
+    if (s != RBSC_OK) {
+        ctx->opts = base;
+        return s;
+    }
+    rbsc_opts chosen = base;
+    double best_ms = rep.default_ms;
+    for (int32_t p : pl)
+        for (int32_t gsm : gr)
+            for (int32_t r : rl)
+                for (int32_t u : ug) {
+                    rbsc_opts o = base;
+                    o.persist_log2 = p;
+                    o.no_persist = p < 0 ? 1 : base.no_persist;
+                    o.grid_per_sm = gsm;
+                    o.relabel = r;
+                    o.use_graph = u;
+                    double ms = 0;
+                    uint32_t b = 0, rd = 0;
+                    s = time_opts(o, &ms, &b, &rd);
+                    if (s != RBSC_OK) {
+                        ctx->opts = base;
+                        return s;
+                    }
+                    const uint32_t i = rep.candidates++;
+                    if (i < 64) {
+                        rep.ms[i] = ms;
+                        rep.opts[i] = o;
+                    }
+                    if (b != b0 || rd != r0) {
+                        ++rep.failed;
+                        continue;
+                    }
+                    if (ms < best_ms) {
+                        best_ms = ms;
+                        chosen = o;
+                    }
+                }
+    ctx->opts = base;
+    rep.best_ms = best_ms;
+    *best = chosen;
+    if (report) *report = rep;
     return RBSC_OK;
 }
