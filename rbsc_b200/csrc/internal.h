@@ -90,6 +90,7 @@ struct rbsc_graph {
     uint32_t* d_vl32 = nullptr;
     uint32_t* d_vllong = nullptr;
     uint64_t* d_vdeg = nullptr;
+    uint64_t* d_vstart = nullptr;    // exact check: row starts in the compacted active set
     uint32_t* d_fail = nullptr;
     unsigned long long* d_keys[2] = {nullptr, nullptr};
     unsigned long long* d_vals[2] = {nullptr, nullptr};

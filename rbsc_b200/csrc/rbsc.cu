@@ -296,6 +296,7 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free(g->ctx, (void*&)g->d_vl32);
     dev_free(g->ctx, (void*&)g->d_vllong);
     dev_free(g->ctx, (void*&)g->d_vdeg);
+    dev_free(g->ctx, (void*&)g->d_vstart);
     dev_free(g->ctx, (void*&)g->d_fail);
     dev_free(g->ctx, (void*&)g->d_keys[0]);
     dev_free(g->ctx, (void*&)g->d_keys[1]);
@@ -1170,15 +1171,33 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
     CK(cudaMemsetAsync(g->d_small, 0, 64, s));
     CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), s));
     CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
+    // the arc view: the graph's own arrays, or -- when those are in host
+    // memory and the active set was compacted into device memory -- the
+    // compacted rows (every row the check reads is among them)
+    const uint64_t* vstart = g->d_off;
+    const uint32_t* vidx = g->d_idx;
+    const uint64_t* vwt = g->d_wt;
+    if (g->host_arcs && !g->arcs_on_host) {
+        if (!g->d_vstart) CKS(dev_alloc(ctx, (void**)&g->d_vstart, 8 * ((size_t)n + 1)));
+        ActiveSet as;
+        CK(cudaMemcpyAsync(&as, g->d_as, sizeof as, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        ++rbsc::launch_counter();
+        k_verify_starts<<<persistent_grid(ctx, as.K, 256), 256, 0, s>>>(g->d_as, g->d_vstart);
+        CK(cudaGetLastError());
+        vstart = g->d_vstart;
+        vidx = as.idx;
+        vwt = as.wt;
+    }
     VerifyLists vl{g->d_vl8, g->d_vl32, g->d_vllong, counts};
     ++rbsc::launch_counter();
     k_verify_classify<<<grid_for(n, 256), 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->weighted ? 1 : 0, vl, g->d_vflag,
                                                       g->d_fail);
     const unsigned sgrid = persistent_grid(ctx, n, 256);
     ++rbsc::launch_counter();
-    k_verify_short<8><<<sgrid, 256, 0, s>>>(n, g->d_vl8, counts + 0, col, g->d_off, g->d_idx, g->d_fail, counts + 3);
+    k_verify_short<8><<<sgrid, 256, 0, s>>>(n, g->d_vl8, counts + 0, col, g->d_off, vstart, vidx, g->d_fail, counts + 3);
     ++rbsc::launch_counter();
-    k_verify_short<32><<<sgrid, 256, 0, s>>>(n, g->d_vl32, counts + 1, col, g->d_off, g->d_idx, g->d_fail, counts + 3);
+    k_verify_short<32><<<sgrid, 256, 0, s>>>(n, g->d_vl32, counts + 1, col, g->d_off, vstart, vidx, g->d_fail, counts + 3);
     CK(cudaGetLastError());
     uint32_t hc[4];
     CK(cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, s));
@@ -1216,8 +1235,8 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
         const unsigned long long* vals = g->weighted ? g->d_vals[0] : nullptr;
         if (nkeys > 0) {
             ++rbsc::launch_counter();
-            k_verify_keys<<<grid_for(n, 128), 128, 0, s>>>(n, col, g->d_off, g->d_idx, g->d_wt, g->d_vflag, g->d_vrow, g->d_vdeg,
-                                                          g->d_keys[0], g->weighted ? g->d_vals[0] : nullptr);
+            k_verify_keys<<<grid_for(n, 128), 128, 0, s>>>(n, col, g->d_off, vstart, vidx, vwt, g->d_vflag, g->d_vrow,
+                                                          g->d_vdeg, g->d_keys[0], g->weighted ? g->d_vals[0] : nullptr);
             CK(cudaGetLastError());
             CKS(ensure_temp(ctx, g, radix_temp_bytes(nkeys)));
             const int bits = 31 + (int)log2_ceil(std::max<uint32_t>(nrows, 1));

@@ -20,6 +20,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "common.cuh"
+#include "refine_kernels.cuh"
 
 namespace rbsc {
 
@@ -88,11 +89,15 @@ template <int G> __device__ __forceinline__ uint32_t group_sort(uint32_t v)
 
 // Groups of G lanes compare the sorted head colours of u and its block's
 // representative (rows of equal length <= G, unit weights).
+// Rows are read from an arc view: node u's row starts at vstart[u] in idx
+// (vstart = off for the graph's own arrays, or the start of u's row in the
+// compacted active set, which holds every row the check reads); its length
+// is always off[u+1] - off[u].
 template <int G>
 static __global__ void k_verify_short(uint32_t n, const uint32_t* __restrict__ list, const uint32_t* __restrict__ count,
                                       const uint32_t* __restrict__ col, const uint64_t* __restrict__ off,
-                                      const uint32_t* __restrict__ idx, uint32_t* __restrict__ fail,
-                                      uint32_t* __restrict__ nfail)
+                                      const uint64_t* __restrict__ vstart, const uint32_t* __restrict__ idx,
+                                      uint32_t* __restrict__ fail, uint32_t* __restrict__ nfail)
 {
     const uint32_t cnt = *count;
     const int gl = threadIdx.x & (G - 1);
@@ -111,8 +116,8 @@ static __global__ void k_verify_short(uint32_t n, const uint32_t* __restrict__ l
         if (valid) {
             u = list[gi];
             const uint32_t r = col[u] & kLabelMask;
-            const uint64_t ou = off[u], orr = off[r];
-            const uint32_t d = (uint32_t)(off[u + 1] - ou);
+            const uint64_t ou = vstart[u], orr = vstart[r];
+            const uint32_t d = (uint32_t)(off[u + 1] - off[u]);
             if ((uint32_t)gl < d) {
                 a = col[idx[ou + gl]] & kLabelMask;
                 b = col[idx[orr + gl]] & kLabelMask;
@@ -139,21 +144,32 @@ static __global__ void k_verify_mark(uint32_t n, const uint64_t* __restrict__ of
 
 // Keys of the needed rows: (row index << 31) | colour of the head.
 static __global__ void k_verify_keys(uint32_t n, const uint32_t* __restrict__ col, const uint64_t* __restrict__ off,
-                              const uint32_t* __restrict__ idx, const uint64_t* __restrict__ wt,
-                              const uint32_t* __restrict__ vflag, const uint32_t* __restrict__ vrow,
-                              const uint64_t* __restrict__ voff, unsigned long long* __restrict__ keys,
-                              unsigned long long* __restrict__ vals)
+                              const uint64_t* __restrict__ vstart, const uint32_t* __restrict__ idx,
+                              const uint64_t* __restrict__ wt, const uint32_t* __restrict__ vflag,
+                              const uint32_t* __restrict__ vrow, const uint64_t* __restrict__ voff,
+                              unsigned long long* __restrict__ keys, unsigned long long* __restrict__ vals)
 {
     const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
     if (u >= n) return;
-    const uint64_t b = off[u], e = off[u + 1];
-    if (e == b || !vflag[u]) return;
+    const uint64_t d = off[u + 1] - off[u];
+    if (d == 0 || !vflag[u]) return;
+    const uint64_t b = vstart[u];
     const uint64_t row = vrow[u];
     const uint64_t base = voff[u];
-    for (uint64_t k = b; k < e; ++k) {
-        keys[base + (k - b)] = (row << 31) | (uint64_t)(col[idx[k]] & kLabelMask);
-        if (vals) vals[base + (k - b)] = wt[k];
+    for (uint64_t k = 0; k < d; ++k) {
+        keys[base + k] = (row << 31) | (uint64_t)(col[idx[b + k]] & kLabelMask);
+        if (vals) vals[base + k] = wt[b + k];
     }
+}
+
+// Row starts of the compacted active set's rows (uint32 offsets): the arc
+// view of the exact check when the graph's own arcs are in host memory.
+static __global__ void k_verify_starts(const ActiveSet* __restrict__ as, uint64_t* __restrict__ vstart)
+{
+    const uint32_t K = as->K;
+    const uint32_t* __restrict__ rows = as->rows;
+    const uint32_t* __restrict__ roff = reinterpret_cast<const uint32_t*>(as->roff);
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < K; k += gridDim.x * blockDim.x) vstart[rows[k]] = roff[k];
 }
 
 // Walks the next run of equal colours in a sorted row segment; returns false
