@@ -142,8 +142,17 @@ def cpu_baseline_reference(steps: int = 1):
                 tot_t += t
                 tot_er += m * rounds
                 runs.append(dict(time_s=t, rounds=rounds, blocks=blocks, wall_s=round(wall, 3)))
+        law = None
+        g = oracle.load_law()
+        if g is not None:
+            with tempfile.TemporaryDirectory() as d:
+                path = os.path.join(d, "cnr.txt")
+                oracle.write_arcs_file(path, g[0], g[1])
+                t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
+            law = {"graph": "cnr-2000", "time_s": t, "rounds": rounds, "blocks": blocks, "wall_s": round(wall, 3),
+                   "edge_rounds_per_s": len(g[1]) * rounds / t}
         return {"value": tot_er / tot_t, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": sample, "runs": runs, "host_cores": os.cpu_count()}
+                "sample": sample, "runs": runs, "host_cores": os.cpu_count(), "law_cnr2000": law}
     t0 = time.perf_counter()
     r = oracle.refine_rsc(off, idx)
     t = time.perf_counter() - t0
@@ -342,6 +351,7 @@ def run_ours(args, rank, world, local_rank):
 
     batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
     served = None if args.serve_requests <= 0 else run_served(args, world, dist, local_rank)
+    law = None if args.law_steps <= 0 else run_law(args, ctx)
     streamed = None if args.stream_scale <= 0 else run_streamed(args, ctx, local_rank)
 
     cpu = None
@@ -357,7 +367,7 @@ def run_ours(args, rank, world, local_rank):
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "autotune": tune, "batched": batched,
-                "served": served, "streamed": streamed}
+                "served": served, "law_cnr2000": law, "streamed": streamed}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -558,6 +568,47 @@ def run_served(args, world, dist, local_rank):
     return out
 
 
+def run_law(args, ctx):
+    """The reference's own LAW sample, cnr-2000 (325,557 nodes, 3,216,152 arcs,
+    173 rounds), decoded from its BV files by rbsc_bv_load at build time
+    (oracle/_ref/cnr-2000.npz; absent -> section skipped).  Uniform initial
+    colours, as the reference programs run it.  Resident refinement (device
+    time) and the one-shot call from page-locked host arrays; the partition is
+    checked against the reference programs' (tests/golden/law_cnr2000.json),
+    whose recorded reference-GPU-program time on a B200 is quoted beside."""
+    import hashlib
+    from oracle import oracle  # the decoded graph only; nothing under oracle/ runs here
+    g0 = oracle.load_law()
+    if g0 is None:
+        return None
+    fx = json.load(open(os.path.join(ROOT, "tests", "golden", "law_cnr2000.json")))
+    off, idx = _pinned_copy(g0[0]), _pinned_copy(g0[1])
+    m = len(idx)
+    g = ctx.upload(off, idx)
+    for _ in range(3):
+        g.refine_device()
+    res = [g.refine_device() for _ in range(args.law_steps)]
+    g.free()
+    out_p = _pinned(len(off) - 1, np.uint32)
+    ctx.refine(off, idx, out=out_p)
+    one = [ctx.refine(off, idx, out=out_p) for _ in range(args.law_steps)]
+    lab = out_p[: len(off) - 1]
+    ok = (one[-1].blocks == fx["blocks"] and one[-1].rounds == fx["rounds"]
+          and hashlib.sha256(np.ascontiguousarray(lab).tobytes()).hexdigest() == fx["labels_sha256"])
+    assert ok, "cnr-2000 partition differs from the reference programs'"
+    dev = statistics.median([r.device_ms for r in res])
+    e2e = statistics.median([r.time_s for r in one]) * 1e3
+    ref_gpu = next((r["time_s"] for r in fx.get("ref_rbsc", {}).get("runs", []) if r["batch"] >= m), None)
+    return {"workload": "cnr-2000 (LAW; the reference's webgraph-rs/data sample), uniform initial colours",
+            "nodes": len(off) - 1, "arcs": m, "rounds": res[0].rounds, "blocks": res[0].blocks,
+            "ms_to_fixpoint": dev, "edge_rounds_per_s": m * res[0].rounds / (dev / 1e3),
+            "e2e_ms": e2e, "e2e_edge_rounds_per_s": m * res[0].rounds / (e2e / 1e3),
+            "same_partition_as_reference_programs": ok,
+            "reference_gpu_program_ms_recorded": None if ref_gpu is None else 1e3 * ref_gpu,
+            "reference_note": "reference GPU program time: its own timer (H2D + refinement), one batch, recorded on a "
+                              "B200 by tests/golden/make_law_golden.py --gpu; compare with e2e_ms"}
+
+
 def run_streamed(args, ctx, local_rank):
     """Arcs in host memory (the out-of-HBM configuration): R-MAT scale
     args.stream_scale, edge factor args.stream_ef, generated on the device in
@@ -649,6 +700,7 @@ def main():
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-sample", type=int, default=1000, help="graphs refined one call each")
     ap.add_argument("--serve-requests", type=int, default=600, help="served stream length (0: skip)")
+    ap.add_argument("--law-steps", type=int, default=5, help="refinements of the LAW sample cnr-2000 (0: skip)")
     ap.add_argument("--stream-scale", type=int, default=28, help="R-MAT scale of the streamed graph (0: skip)")
     ap.add_argument("--stream-ef", type=int, default=32)
     ap.add_argument("--stream-steps", type=int, default=2)

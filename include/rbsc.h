@@ -290,6 +290,23 @@ rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_
 rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_graph* out);
 void rbsc_host_graph_free(rbsc_host_graph* g);
 
+/* Reads a BV-compressed graph (the WebGraph format of the LAW datasets the
+ * reference benchmarks on, which its webgraph-rs decodes to arcs-cuda text,
+ * cli/src/to/arcscuda.rs:61-66): basename.properties, basename.graph and, if
+ * present, basename.offsets (used to check every list's start).  Default
+ * codes only (empty compressionflags).  Row u = the successors of u, sorted;
+ * no weights.  Free with rbsc_host_graph_free. */
+typedef struct {
+    uint64_t copied_arcs;     /* successors copied from a referenced list          */
+    uint64_t interval_arcs;   /* successors in intervals                           */
+    uint64_t residual_arcs;   /* successors coded as gaps                          */
+    uint64_t bits;            /* bits of the .graph stream decoded                 */
+    uint32_t offsets_checked; /* 1: every list started at its .offsets position     */
+    uint32_t pad;
+} rbsc_bv_stats;
+
+rbsc_status rbsc_bv_load(const char* basename, rbsc_host_graph* out, rbsc_bv_stats* stats);
+
 /* ---- synthetic workloads (stand-ins for the reference's LAW graphs) ------ */
 
 /* Directed R-MAT: 2^scale nodes, edge_factor * 2^scale generated arcs with

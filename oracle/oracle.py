@@ -30,6 +30,34 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_RSC = os.path.join(REF_DIR, "ref_rsc")
 REF_VALMARI = os.path.join(REF_DIR, "ref_valmari")
+REF_RBSC = os.path.join(REF_DIR, "ref_rbsc")
+# decoded copy of the reference's vendored LAW sample (webgraph-rs/data/cnr-2000),
+# made in this container by prepare_law() and carried with the tree
+LAW_CNR2000 = os.path.join(REF_DIR, "cnr-2000.npz")
+
+
+def prepare_law(ref: str | None) -> str | None:
+    """Decodes the reference's cnr-2000 BV graph (webgraph-rs/data) into
+    LAW_CNR2000, once; returns the path or None when the reference tree is
+    absent and no copy was made before."""
+    if os.path.exists(LAW_CNR2000):
+        return LAW_CNR2000
+    base = None if not ref else os.path.join(ref, "webgraph-rs", "data", "cnr-2000")
+    if not base or not os.path.exists(base + ".graph"):
+        return None
+    import rbsc_b200 as R
+    off, idx, _ = R.load_bvgraph(base)
+    os.makedirs(REF_DIR, exist_ok=True)
+    np.savez(LAW_CNR2000, off=off, idx=idx)
+    return LAW_CNR2000
+
+
+def load_law():
+    """(off, idx) of the decoded cnr-2000, or None."""
+    if not os.path.exists(LAW_CNR2000):
+        return None
+    z = np.load(LAW_CNR2000)
+    return z["off"], z["idx"]
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)

@@ -385,6 +385,17 @@ def parse_arcs(text: bytes):
     return _host_graph_to_numpy(lib, hg)
 
 
+def load_bvgraph(basename: str):
+    """A BV-compressed (WebGraph / LAW) graph: (offsets uint64, indices uint32,
+    stats dict) -- rbsc_bv_load."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    st = _lib.BvStats()
+    _check(lib, lib.rbsc_bv_load(basename.encode(), ctypes.byref(hg), ctypes.byref(st)), None)
+    off, idx, _ = _host_graph_to_numpy(lib, hg)
+    return off, idx, {k: int(getattr(st, k)) for k, _ in _lib.BvStats._fields_ if k != "pad"}
+
+
 def gen_rmat_host(scale: int, edge_factor: int, a=RMAT_ABC[0], b=RMAT_ABC[1], c=RMAT_ABC[2], seed: int = 1,
                   threads: int = 0):
     """The device generator's graph, built on the host: (offsets, indices)."""

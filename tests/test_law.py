@@ -1,0 +1,109 @@
+"""The reference's own LAW sample, cnr-2000 (325,557 nodes, 3,216,152 arcs;
+BV-compressed in the reference's webgraph-rs/data).
+
+tests/golden/law_cnr2000.json (made by tests/golden/make_law_golden.py)
+holds the reference programs' results on it: rsc and Valmari (partition,
+blocks, rounds) and the reference GPU program's `done` / `nodes` at its
+bench's batch sizes.  CPU: the BV reader against the format's own checks and
+the fixture's checksum.  GPU: the CUDA path against the fixture (zero
+tolerance), in one batch, in the reference's edge-batch mode, and streamed."""
+import hashlib
+import json
+import os
+
+import numpy as np
+import pytest
+
+import rbsc_b200 as R
+from conftest import GOLDEN
+from oracle import oracle
+
+FX = json.load(open(os.path.join(GOLDEN, "law_cnr2000.json")))
+BV = "/root/reference/webgraph-rs/data/cnr-2000"
+
+
+def _sha(*arrays):
+    h = hashlib.sha256()
+    for a in arrays:
+        h.update(np.ascontiguousarray(a).tobytes())
+    return h.hexdigest()
+
+
+@pytest.fixture(scope="module")
+def law():
+    g = oracle.load_law()
+    if g is None:
+        pytest.skip("decoded cnr-2000 not present (oracle/_ref/cnr-2000.npz is made by build() next to the reference)")
+    off, idx = g
+    assert _sha(off.astype(np.uint64), idx.astype(np.uint32)) == FX["csr_sha256"]
+    return off, idx
+
+
+@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+def test_bv_reader_on_the_reference_sample():
+    off, idx, st = R.load_bvgraph(BV)
+    assert len(off) - 1 == FX["n"] and len(idx) == FX["m"]
+    assert _sha(off.astype(np.uint64), idx.astype(np.uint32)) == FX["csr_sha256"]
+    # the compressor's own statistics (cnr-2000.properties) and list offsets
+    props = dict(l.strip().split("=", 1) for l in open(BV + ".properties") if "=" in l and not l.startswith("#"))
+    assert st["copied_arcs"] == int(props["copiedarcs"])
+    assert st["interval_arcs"] == int(props["intervalisedarcs"])
+    assert st["residual_arcs"] == int(props["residualarcs"])
+    assert st["offsets_checked"] == 1
+    # the transposed graph decodes to the transpose
+    offt, idxt, _ = R.load_bvgraph(BV + "-t")
+    n = len(off) - 1
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    order = np.lexsort((src, idx.astype(np.int64)))
+    assert np.array_equal(idx.astype(np.int64)[order], np.repeat(np.arange(n), np.diff(offt.astype(np.int64))))
+    assert np.array_equal(src[order], idxt.astype(np.int64))
+
+
+def test_bv_reader_rejects_bad_input(tmp_path):
+    base = str(tmp_path / "g")
+    with open(base + ".properties", "w") as f:
+        f.write("nodes=3\narcs=2\nwindowsize=7\nminintervallength=4\nzetak=3\ncompressionflags=OUTDEGREES_DELTA\n")
+    open(base + ".graph", "wb").write(b"\x00")
+    with pytest.raises(R.RbscError):
+        R.load_bvgraph(base)
+    with open(base + ".properties", "w") as f:
+        f.write("nodes=3\narcs=2\nwindowsize=7\nminintervallength=4\nzetak=3\ncompressionflags=\n")
+    open(base + ".graph", "wb").write(b"\xff")  # three empty lists: 0 arcs, not 2
+    with pytest.raises(R.RbscError):
+        R.load_bvgraph(base)
+
+
+@pytest.mark.gpu
+def test_gpu_partition_equals_the_reference_programs(law):
+    off, idx = law
+    with R.Context(0) as ctx:
+        r = ctx.refine(off, idx)
+        assert r.blocks == FX["blocks"] and r.rounds == FX["rounds"] and r.done == 1
+        assert _sha(r.labels.astype(np.uint32)) == FX["labels_sha256"]
+        g = ctx.upload(off, idx)
+        for _ in range(2):
+            r2 = g.refine()
+            assert r2.blocks == FX["blocks"] and r2.rounds == FX["rounds"]
+            assert _sha(r2.labels.astype(np.uint32)) == FX["labels_sha256"]
+        g.free()
+
+
+@pytest.mark.gpu
+def test_gpu_edge_batches_equal_the_reference_gpu_program(law):
+    off, idx = law
+    with R.Context(0) as ctx:
+        for run in FX["ref_rbsc"]["runs"]:
+            r, info = ctx.refine_edge_batches(off, idx, edge_batch_size=run["batch"], aggressive=run["aggressive"],
+                                              labels=False)
+            assert (r.done, r.blocks) == (run["done"], run["nodes"]), run
+
+
+@pytest.mark.gpu
+def test_gpu_streamed_equals_the_reference_programs(law):
+    off, idx = law
+    with R.Context(0) as ctx:
+        g = ctx.upload_streamed(off, idx, batch_arcs=len(idx) // 4 + 1)
+        r = g.refine()
+        g.free()
+    assert r.blocks == FX["blocks"] and r.rounds == FX["rounds"]
+    assert _sha(r.labels.astype(np.uint32)) == FX["labels_sha256"]
