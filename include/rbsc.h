@@ -76,7 +76,10 @@ typedef struct {
                                  and listed nodes are both <= 2^persist_log2
                                  (0 = default 22)                                       */
     int32_t grid_per_sm;      /* blocks per SM of the pass kernels' grids (0 = 16)      */
-    int32_t reserved[4];
+    int32_t sig_kernel;       /* signature kernel over device arcs: 0 = default (plain
+                                 loads), 1 = plain loads, 2 = staged (each warp's tiles
+                                 copied to shared memory by cp.async.bulk; unweighted) */
+    int32_t reserved[3];
 } rbsc_opts;
 
 typedef struct {
@@ -265,6 +268,8 @@ typedef struct {
     uint32_t n_relabel;
     int32_t use_graph[RBSC_TUNE_MAX];     /* CUDA-graph loop 1 / host loop 0                */
     uint32_t n_use_graph;
+    int32_t sig_kernel[RBSC_TUNE_MAX];    /* signature kernels to try (1 plain, 2 staged)   */
+    uint32_t n_sig_kernel;
     uint32_t reps;                        /* timed refinements per candidate (0 = 3)         */
 } rbsc_tune_space;
 

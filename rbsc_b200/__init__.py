@@ -102,7 +102,7 @@ class Context:
 
     def __init__(self, device: int = 0, relabel: int = RELABEL_HASH, verify: bool = True, max_rounds: int = 0,
                  use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0,
-                 persistent: bool = True, persist_log2: int = 0, grid_per_sm: int = 0):
+                 persistent: bool = True, persist_log2: int = 0, grid_per_sm: int = 0, sig_kernel: int = 0):
         self._lib = _lib.load()
         o = _lib.Opts()
         self._lib.rbsc_opts_default(ctypes.byref(o))
@@ -115,6 +115,7 @@ class Context:
         o.no_persist = 0 if persistent else 1
         o.persist_log2 = persist_log2
         o.grid_per_sm = grid_per_sm
+        o.sig_kernel = sig_kernel
         self._opts = o
         h = self._lib.rbsc_ctx_create(device, ctypes.byref(o))
         if not h:
@@ -303,7 +304,7 @@ class Graph:
         _check(lib, lib.rbsc_graph_degree_colors(self.ctx._h, self._h, d_out), self.ctx._h)
 
     def autotune(self, d_init: int | None = None, persist_log2=None, grid_per_sm=None, relabel=None, use_graph=None,
-                 reps: int = 3, apply: bool = True) -> dict:
+                 sig_kernel=None, reps: int = 3, apply: bool = True) -> dict:
         """Times refinements of this graph under combinations of the pass
         kernels' knobs (rbsc_graph_autotune) and, with apply, sets the fastest
         on the context.  Lists left at None take the library's default search
@@ -313,7 +314,8 @@ class Graph:
         sp = _lib.TuneSpace()
         lib.rbsc_tune_space_default(ctypes.byref(sp))
         for name, vals, cnt in (("persist_log2", persist_log2, "n_persist"), ("grid_per_sm", grid_per_sm, "n_grid"),
-                                ("relabel", relabel, "n_relabel"), ("use_graph", use_graph, "n_use_graph")):
+                                ("relabel", relabel, "n_relabel"), ("use_graph", use_graph, "n_use_graph"),
+                                ("sig_kernel", sig_kernel, "n_sig_kernel")):
             if vals is not None:
                 arr = getattr(sp, name)
                 for i, v in enumerate(vals[: _lib.TUNE_MAX]):
@@ -324,7 +326,7 @@ class Graph:
         rep = _lib.TuneReport()
         _check(lib, lib.rbsc_graph_autotune(self.ctx._h, self._h, d_init, ctypes.byref(sp), ctypes.byref(best),
                                             ctypes.byref(rep)), self.ctx._h)
-        knobs = ("persist_log2", "grid_per_sm", "relabel", "use_graph", "no_persist")
+        knobs = ("persist_log2", "grid_per_sm", "relabel", "use_graph", "no_persist", "sig_kernel")
         if apply:
             for k in knobs:
                 setattr(self.ctx._opts, k, getattr(best, k))

@@ -60,7 +60,8 @@ class Opts(ctypes.Structure):
         ("no_persist", ctypes.c_int32),
         ("persist_log2", ctypes.c_int32),
         ("grid_per_sm", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 4),
+        ("sig_kernel", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 3),
     ]
 
 
@@ -173,6 +174,8 @@ class TuneSpace(ctypes.Structure):
         ("n_relabel", ctypes.c_uint32),
         ("use_graph", ctypes.c_int32 * TUNE_MAX),
         ("n_use_graph", ctypes.c_uint32),
+        ("sig_kernel", ctypes.c_int32 * TUNE_MAX),
+        ("n_sig_kernel", ctypes.c_uint32),
         ("reps", ctypes.c_uint32),
     ]
 

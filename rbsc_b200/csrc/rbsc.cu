@@ -747,12 +747,20 @@ struct PassTimer {
 // First-pass gather variants (see k_signature / k_signature_uniform).
 enum FirstPass { kPassFull = 0, kPassUniform = 1, kPassRank8 = 2, kPassRank16 = 3 };
 
+// The signature kernel with tiles staged in shared memory by bulk copies
+// (k_signature_staged): unweighted arc sets, when the options ask for it.
+static bool staged_signature(const rbsc_ctx* ctx, const rbsc_graph* g)
+{
+    return !g->weighted && ctx->opts.sig_kernel == 2;
+}
+
 template <typename ColT>
-static void launch_signature_chunk(bool weighted, unsigned grid, cudaStream_t s, const ActiveSet* as, const RoundState* st,
+static void launch_signature_chunk(bool weighted, bool staged, unsigned grid, cudaStream_t s, ActiveSet* as, RoundState* st,
                                    const ColT* col, Sig* sig, TileRange r)
 {
     ++rbsc::launch_counter();
-    if (weighted) k_signature_chunk<true, ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r);
+    if (staged && !weighted) k_signature_staged<ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r, 1);
+    else if (weighted) k_signature_chunk<true, ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r);
     else k_signature_chunk<false, ColT><<<grid, kTileThreads, 0, s>>>(as, st, col, sig, r);
 }
 
@@ -776,14 +784,15 @@ static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s
         CK(cudaStreamWaitEvent(s, g->ev_copied[slot], 0));
         const TileRange r{t0, t1, g->d_chunk[slot], g->weighted ? g->d_chunk_wt[slot] : nullptr, a0};
         const unsigned grid = persistent_grid(ctx, t1 - t0, kTileThreads / 32);
+        const bool st = staged_signature(ctx, g);
         if (first == kPassRank8)
-            launch_signature_chunk<uint8_t>(g->weighted, grid, s, g->d_as, g->d_st, reinterpret_cast<const uint8_t*>(g->d_rank),
-                                            g->d_sig, r);
+            launch_signature_chunk<uint8_t>(g->weighted, st, grid, s, g->d_as, g->d_st,
+                                            reinterpret_cast<const uint8_t*>(g->d_rank), g->d_sig, r);
         else if (first == kPassRank16)
-            launch_signature_chunk<uint16_t>(g->weighted, grid, s, g->d_as, g->d_st,
+            launch_signature_chunk<uint16_t>(g->weighted, st, grid, s, g->d_as, g->d_st,
                                              reinterpret_cast<const uint16_t*>(g->d_rank), g->d_sig, r);
         else
-            launch_signature_chunk<uint32_t>(g->weighted, grid, s, g->d_as, g->d_st, g->d_col[0], g->d_sig, r);
+            launch_signature_chunk<uint32_t>(g->weighted, st, grid, s, g->d_as, g->d_st, g->d_col[0], g->d_sig, r);
         CK(cudaGetLastError());
         CK(cudaEventRecord(g->ev_used[slot], s));
         g->streamed_bytes += (a1 - a0) * (g->weighted ? 12 : 4);
@@ -817,6 +826,17 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
                 k_signature_uniform<true><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig);
             else
                 k_signature_uniform<false><<<ugrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_off, g->d_wt, c0, g->d_sig);
+        } else if (staged_signature(ctx, g)) {
+            const TileRange all{0u, 0u, nullptr, nullptr, 0ull};
+            if (first == kPassRank8)
+                k_signature_staged<uint8_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st,
+                                                                           reinterpret_cast<const uint8_t*>(g->d_rank), g->d_sig,
+                                                                           all, 0);
+            else if (first == kPassRank16)
+                k_signature_staged<uint16_t><<<blocks, kTileThreads, 0, s>>>(
+                    g->d_as, g->d_st, reinterpret_cast<const uint16_t*>(g->d_rank), g->d_sig, all, 0);
+            else
+                k_signature_staged<uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, all, 0);
         } else if (first == kPassRank8) {
             const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
             if (g->weighted)
@@ -1414,6 +1434,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     }
     g->next_stamp = hs.stamp;
     if (hs.error & kErrProbe) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "relabel table overflow");
+    if (hs.error & kErrStage) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "signature: a staged tile copy did not complete");
     if (hs.error & kErrRounds) return rbsc_fail(ctx, RBSC_ERR_NOT_CONVERGED, "no fixpoint after %u passes", hs.round);
     uint32_t* out = d_out ? d_out : g->d_out;
     ++rbsc::launch_counter();
@@ -1544,6 +1565,8 @@ extern "C" void rbsc_tune_space_default(rbsc_tune_space* sp)
     sp->relabel[sp->n_relabel++] = RBSC_RELABEL_HASH;
     sp->use_graph[sp->n_use_graph++] = 1;
     sp->use_graph[sp->n_use_graph++] = 0;
+    sp->sig_kernel[sp->n_sig_kernel++] = 1;
+    sp->sig_kernel[sp->n_sig_kernel++] = 2;
     sp->reps = 3;
 }
 
@@ -1564,6 +1587,7 @@ extern "C" rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const u
     const auto gr = list(sp.grid_per_sm, sp.n_grid, base.grid_per_sm);
     const auto rl = list(sp.relabel, sp.n_relabel, base.relabel);
     const auto ug = list(sp.use_graph, sp.n_use_graph, base.use_graph);
+    const auto sks = list(sp.sig_kernel, sp.n_sig_kernel, base.sig_kernel);
     const uint32_t reps = sp.reps ? sp.reps : 3;
     rbsc_tune_report rep;
     std::memset(&rep, 0, sizeof rep);
@@ -1596,8 +1620,10 @@ extern "C" rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const u
     for (int32_t p : pl)
         for (int32_t gsm : gr)
             for (int32_t r : rl)
-                for (int32_t u : ug) {
+                for (int32_t u : ug)
+                  for (int32_t sk : sks) {
                     rbsc_opts o = base;
+                    o.sig_kernel = sk;
                     o.persist_log2 = p;
                     o.no_persist = p < 0 ? 1 : base.no_persist;
                     o.grid_per_sm = gsm;

@@ -53,6 +53,7 @@ struct RoundState {
 constexpr uint32_t kErrProbe = 1u;   // relabel table full (cannot happen at load <= 1/2)
 constexpr uint32_t kErrRounds = 2u;  // max_rounds reached
 constexpr uint32_t kErrBarrier = 4u; // a grid barrier of the persistent kernel timed out
+constexpr uint32_t kErrStage = 8u;   // a staged (bulk async) copy of k_signature_staged did not complete
 
 // What the pass kernels work on; the compaction kernels shrink it.
 struct ActiveSet {
@@ -264,6 +265,113 @@ struct TileRange {
     uint64_t base;
 };
 
+// The fold of one tile, once the lane has its head bits (hb, bit j = arc
+// a + j starts a row), the colours c[] of its cnt heads and, weighted, their
+// weights: per-lane partial sums, a warp segmented scan across lanes, the
+// row signatures written (rows crossing a tile edge added atomically).
+template <bool WEIGHTED>
+__device__ __forceinline__ void signature_fold(uint32_t lane, uint32_t a, uint32_t cnt, uint32_t tlen, uint64_t tend, uint64_t m,
+                                               uint32_t k0, uint32_t h0, uint32_t hb, const uint32_t (&c)[kEdgesPerThread],
+                                               const uint64_t (&w)[kEdgesPerThread], uint64_t salt,
+                                               const uint32_t* __restrict__ rows, const uint8_t* __restrict__ head8,
+                                               Sig* __restrict__ sig)
+{
+    // row of arc a-1 (or of arc a when arc a does not start a row):
+    // k0 + (heads in tile arcs [0, a)) - h0
+    const uint32_t nheads = (uint32_t)__popc(hb);
+    uint32_t hs = nheads;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xffffffffu, hs, d);
+        if (lane >= (uint32_t)d) hs += o;
+    }
+    const uint32_t kbase = k0 + hs - nheads - h0;
+
+    // fold: `pre` = arcs before this lane's first head, `cur` = the row
+    // opened by the latest head; a row closed inside the lane is written
+    uint64_t pre1 = 0, cur1 = 0;
+    uint32_t pre2 = 0, cur2 = 0;
+    uint32_t nh = 0;
+#pragma unroll
+    for (int i = 0; i < kEdgesPerThread; ++i) {
+        if ((uint32_t)i < cnt) {
+            if ((hb >> i) & 1u) {
+                if (nh > 0) {
+                    const uint32_t node = rows[kbase + nh];
+                    sig_store(&sig[node], cur1, cur2);
+                }
+                ++nh;
+                cur1 = 0;
+                cur2 = 0;
+            }
+            uint64_t t1;
+            uint32_t t2;
+            arc_terms(c[i], salt, t1, t2);
+            if (WEIGHTED) {
+                t1 *= w[i];
+                t2 *= (uint32_t)w[i];
+            }
+            if (nh == 0) {
+                pre1 += t1;
+                pre2 += t2;
+            } else {
+                cur1 += t1;
+                cur2 += t2;
+            }
+        }
+    }
+
+    // warp inclusive segmented scan of the lanes' trailing parts (a
+    // segment starts at every lane with a head)
+    uint32_t f = nh > 0 ? 1u : 0u;
+    uint64_t c1 = f ? cur1 : pre1;
+    uint32_t c2 = f ? cur2 : pre2;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t fo = __shfl_up_sync(0xffffffffu, f, d);
+        const uint64_t vo1 = __shfl_up_sync(0xffffffffu, c1, d);
+        const uint32_t vo2 = __shfl_up_sync(0xffffffffu, c2, d);
+        if (lane >= (uint32_t)d) {
+            if (!f) {
+                c1 += vo1;
+                c2 += vo2;
+            }
+            f |= fo;
+        }
+    }
+    uint64_t cin1 = __shfl_up_sync(0xffffffffu, c1, 1);
+    uint32_t cin2 = __shfl_up_sync(0xffffffffu, c2, 1);
+    if (lane == 0) {
+        cin1 = 0;
+        cin2 = 0;
+    }
+    if (cnt == 0) return;
+
+    // the row continuing into this lane ends here when this lane has a head
+    if (nh > 0 && (a > 0 || !(hb & 1u))) {
+        const uint32_t node = rows[kbase];
+        const uint64_t tot1 = cin1 + pre1;
+        const uint32_t tot2 = cin2 + pre2;
+        if (kbase == k0 && !h0) {  // began in an earlier tile
+            sig_add(&sig[node], tot1, tot2);
+        } else {
+            sig_store(&sig[node], tot1, tot2);
+        }
+    }
+    // the last lane of the tile closes the tile's last row
+    if (a + cnt == tlen) {
+        const uint32_t klast = kbase + nh;
+        const bool ends = (tend == m) || (head8[tend >> 3] & 1u);
+        const bool began_before = (klast == k0 && !h0);
+        const uint32_t node = rows[klast];
+        if (ends && !began_before) {
+            sig_store(&sig[node], c1, c2);
+        } else {
+            sig_add(&sig[node], c1, c2);
+        }
+    }
+}
+
 template <bool WEIGHTED, typename ColT, bool NC = true, bool RANGE = false>
 __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                const ColT* __restrict__ col, Sig* __restrict__ sig,
@@ -318,100 +426,7 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
             for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + (tbeg - ebase) + a + i) : 0ull;
         }
 
-        // row of arc a-1 (or of arc a when arc a does not start a row):
-        // k0 + (heads in tile arcs [0, a)) - h0
-        const uint32_t nheads = (uint32_t)__popc(hb);
-        uint32_t hs = nheads;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t o = __shfl_up_sync(0xffffffffu, hs, d);
-            if (lane >= (uint32_t)d) hs += o;
-        }
-        const uint32_t kbase = k0 + hs - nheads - h0;
-
-        // fold: `pre` = arcs before this lane's first head, `cur` = the row
-        // opened by the latest head; a row closed inside the lane is written
-        uint64_t pre1 = 0, cur1 = 0;
-        uint32_t pre2 = 0, cur2 = 0;
-        uint32_t nh = 0;
-#pragma unroll
-        for (int i = 0; i < kEdgesPerThread; ++i) {
-            if ((uint32_t)i < cnt) {
-                if ((hb >> i) & 1u) {
-                    if (nh > 0) {
-                        const uint32_t node = rows[kbase + nh];
-                        sig_store(&sig[node], cur1, cur2);
-                    }
-                    ++nh;
-                    cur1 = 0;
-                    cur2 = 0;
-                }
-                uint64_t t1;
-                uint32_t t2;
-                arc_terms(c[i], salt, t1, t2);
-                if (WEIGHTED) {
-                    t1 *= w[i];
-                    t2 *= (uint32_t)w[i];
-                }
-                if (nh == 0) {
-                    pre1 += t1;
-                    pre2 += t2;
-                } else {
-                    cur1 += t1;
-                    cur2 += t2;
-                }
-            }
-        }
-
-        // warp inclusive segmented scan of the lanes' trailing parts (a
-        // segment starts at every lane with a head)
-        uint32_t f = nh > 0 ? 1u : 0u;
-        uint64_t c1 = f ? cur1 : pre1;
-        uint32_t c2 = f ? cur2 : pre2;
-#pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t fo = __shfl_up_sync(0xffffffffu, f, d);
-            const uint64_t vo1 = __shfl_up_sync(0xffffffffu, c1, d);
-            const uint32_t vo2 = __shfl_up_sync(0xffffffffu, c2, d);
-            if (lane >= (uint32_t)d) {
-                if (!f) {
-                    c1 += vo1;
-                    c2 += vo2;
-                }
-                f |= fo;
-            }
-        }
-        uint64_t cin1 = __shfl_up_sync(0xffffffffu, c1, 1);
-        uint32_t cin2 = __shfl_up_sync(0xffffffffu, c2, 1);
-        if (lane == 0) {
-            cin1 = 0;
-            cin2 = 0;
-        }
-        if (cnt == 0) continue;
-
-        // the row continuing into this lane ends here when this lane has a head
-        if (nh > 0 && (a > 0 || !(hb & 1u))) {
-            const uint32_t node = rows[kbase];
-            const uint64_t tot1 = cin1 + pre1;
-            const uint32_t tot2 = cin2 + pre2;
-            if (kbase == k0 && !h0) {  // began in an earlier tile
-                sig_add(&sig[node], tot1, tot2);
-            } else {
-                sig_store(&sig[node], tot1, tot2);
-            }
-        }
-        // the last lane of the tile closes the tile's last row
-        if (a + cnt == tlen) {
-            const uint32_t klast = kbase + nh;
-            const bool ends = (tend == m) || (head8[tend >> 3] & 1u);
-            const bool began_before = (klast == k0 && !h0);
-            const uint32_t node = rows[klast];
-            if (ends && !began_before) {
-                sig_store(&sig[node], c1, c2);
-            } else {
-                sig_add(&sig[node], c1, c2);
-            }
-        }
+        signature_fold<WEIGHTED>(lane, a, cnt, tlen, tend, m, k0, h0, hb, c, w, salt, rows, head8, sig);
     }
 }
 
@@ -422,6 +437,167 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature(const ActiveS
                                                                    Sig* __restrict__ sig)
 {
     signature_body<WEIGHTED, ColT>(as, st, col, sig);
+}
+
+// ---------------------------------------------------------------------------
+// k_signature_staged: the same fold, with each warp's tiles staged in shared
+// memory by the bulk copy engine (cp.async.bulk, completion counted on an
+// mbarrier) two tiles deep: while the warp folds tile i, the heads and
+// row-head bits of its next tile are already on their way.  The staged heads
+// never pass through L1, which keeps L1 for the gathered colours.  Measured
+// on R-MAT-24's first pass it is slower than the plain loads (1.13 vs 0.96
+// ms: the pass is bound by the L2->L1 colour gathers, and the per-tile wait
+// and lower occupancy -- 64 registers, 34 KB of shared memory a block -- cost
+// more than the staged head stream saves), so it is an option
+// (rbsc_opts.sig_kernel = 2) and an autotuner candidate, not the default.  Every
+// array it reads is padded to whole tiles, so a tile's copy is 2 KB of heads
+// (the last one rounded up to 16 B) and 64 B of head bits, 16-B aligned.
+// Waits are bounded: a copy that does not complete sets kErrStage, the warp
+// waits (bounded again) for its other copy in flight and stops.
+// ---------------------------------------------------------------------------
+constexpr int kStageWarps = kTileThreads / 32;
+constexpr uint32_t kStageSpins = 1u << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(ok)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity)
+{
+    for (uint32_t i = 0; i < kStageSpins; ++i) {
+        if (mbar_try_wait(bar, parity)) return true;
+        __nanosleep(32);
+    }
+    return false;
+}
+
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+template <typename ColT>
+static __global__ void __launch_bounds__(kTileThreads) k_signature_staged(const ActiveSet* __restrict__ as,
+                                                                          RoundState* __restrict__ st,
+                                                                          const ColT* __restrict__ col, Sig* __restrict__ sig,
+                                                                          TileRange rng, int use_range)
+{
+    __shared__ __align__(128) uint32_t s_idx[kStageWarps][2][kTileEdges];
+    __shared__ __align__(16) uint8_t s_hd[kStageWarps][2][kTileEdges / 8];
+    __shared__ __align__(8) uint64_t s_bar[kStageWarps][2];
+    const uint32_t lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const uint32_t ntiles = use_range ? rng.hi : as->ntiles;
+    const uint64_t m = as->m;
+    const uint32_t* __restrict__ rows = as->rows;
+    const uint32_t* __restrict__ tile_row = as->tile_row;
+    const uint8_t* __restrict__ head8 = as->head8;
+    const uint32_t* __restrict__ idx = use_range ? rng.idx : as->idx;
+    const uint64_t ebase = use_range ? rng.base : 0ull;
+    const uint64_t salt = pass_salt1(st->seed, st->round);
+    const uint32_t warps = gridDim.x * kStageWarps;
+    uint64_t* bar = s_bar[wi];
+    if (lane == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncwarp();
+    // lane 0 asks for tile t in buffer b
+    auto issue = [&](uint32_t t, int b) {
+        const uint64_t tb = (uint64_t)t * kTileEdges;
+        const uint32_t tl = (uint32_t)min((uint64_t)kTileEdges, m - tb);
+        const uint32_t bytes = (tl * 4u + 15u) & ~15u;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(&bar[b], bytes + kTileEdges / 8);
+        bulk_copy_g2s(s_idx[wi][b], idx + (tb - ebase), bytes, &bar[b]);
+        bulk_copy_g2s(s_hd[wi][b], head8 + (tb >> 3), kTileEdges / 8, &bar[b]);
+    };
+    uint32_t tile = (use_range ? rng.lo : 0u) + blockIdx.x * kStageWarps + wi;
+    // bit b of `phases`: the parity buffer b waits for next; bit b of
+    // `inflight`: a copy into buffer b is issued and not yet waited for
+    uint32_t phases = 0u, inflight = 0u;
+    if (tile < ntiles) {
+        if (lane == 0) issue(tile, 0);
+        inflight = 1u;
+    }
+    bool failed = false;
+    for (uint32_t i = 0; tile < ntiles; tile += warps, ++i) {
+        const int b = (int)(i & 1u);
+        const uint32_t next = tile + warps;
+        if (next < ntiles) {
+            if (lane == 0) issue(next, b ^ 1);
+            inflight |= 1u << (b ^ 1);
+        }
+        const bool ok = mbar_wait_bounded(&bar[b], (phases >> b) & 1u);
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) atomicOr(&st->error, kErrStage);
+            failed = true;
+            break;
+        }
+        phases ^= 1u << b;
+        inflight &= ~(1u << b);
+        const uint64_t tbeg = (uint64_t)tile * kTileEdges;
+        const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
+        const uint64_t tend = tbeg + tlen;
+        const uint32_t k0 = tile_row[tile];
+        const uint8_t* hd = s_hd[wi][b];
+        const uint32_t h0 = hd[0] & 1u;
+        const uint32_t a = lane * kEdgesPerThread;
+        const uint32_t cnt = a < tlen ? min((uint32_t)kEdgesPerThread, tlen - a) : 0u;
+        uint32_t hb = cnt ? (uint32_t)*reinterpret_cast<const uint16_t*>(hd + (a >> 3)) : 0u;
+        if (cnt < (uint32_t)kEdgesPerThread) hb &= (1u << cnt) - 1u;
+        uint32_t c[kEdgesPerThread];
+        uint64_t w[kEdgesPerThread];
+        if (cnt == kEdgesPerThread) {
+            // the lane's four 16-B quarters, read in a lane-rotated order so
+            // that eight lanes of a phase hit distinct banks
+            const uint4* p = reinterpret_cast<const uint4*>(&s_idx[wi][b][a]);
+            const uint32_t r = lane & 3u;
+            const uint4 v0 = p[(0u + r) & 3u], v1 = p[(1u + r) & 3u], v2 = p[(2u + r) & 3u], v3 = p[(3u + r) & 3u];
+            // quarter q was read by load (q - r) & 3
+            const uint4 q0 = r == 0 ? v0 : r == 1 ? v3 : r == 2 ? v2 : v1;
+            const uint4 q1 = r == 0 ? v1 : r == 1 ? v0 : r == 2 ? v3 : v2;
+            const uint4 q2 = r == 0 ? v2 : r == 1 ? v1 : r == 2 ? v0 : v3;
+            const uint4 q3 = r == 0 ? v3 : r == 1 ? v2 : r == 2 ? v1 : v0;
+            c[0] = gather_col<true>(col + q0.x); c[1] = gather_col<true>(col + q0.y);
+            c[2] = gather_col<true>(col + q0.z); c[3] = gather_col<true>(col + q0.w);
+            c[4] = gather_col<true>(col + q1.x); c[5] = gather_col<true>(col + q1.y);
+            c[6] = gather_col<true>(col + q1.z); c[7] = gather_col<true>(col + q1.w);
+            c[8] = gather_col<true>(col + q2.x); c[9] = gather_col<true>(col + q2.y);
+            c[10] = gather_col<true>(col + q2.z); c[11] = gather_col<true>(col + q2.w);
+            c[12] = gather_col<true>(col + q3.x); c[13] = gather_col<true>(col + q3.y);
+            c[14] = gather_col<true>(col + q3.z); c[15] = gather_col<true>(col + q3.w);
+        } else {
+#pragma unroll
+            for (int j = 0; j < kEdgesPerThread; ++j) c[j] = (uint32_t)j < cnt ? gather_col<true>(col + s_idx[wi][b][a + j]) : 0u;
+        }
+        signature_fold<false>(lane, a, cnt, tlen, tend, m, k0, h0, hb, c, w, salt, rows, head8, sig);
+        __syncwarp();
+    }
+    // copies still in flight (the loop stopped early): wait for them, bounded
+    if (failed)
+        for (int b = 0; b < 2; ++b)
+            if ((inflight >> b) & 1u) mbar_wait_bounded(&bar[b], (phases >> b) & 1u);
 }
 
 // The same over the tiles of one streamed chunk (see TileRange).

@@ -25,12 +25,14 @@ def test_opts_layout_unchanged():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("sig_kernel", [1, 2])
 @pytest.mark.parametrize("persist_log2,grid", [(-1, 4), (10, 8), (16, 32), (31, 2)])
-def test_knobs_keep_the_partition(persist_log2, grid):
+def test_knobs_keep_the_partition(persist_log2, grid, sig_kernel):
     off, idx = G.rmat(12, 8, seed=4)
     init = R.degree_bucket_colors(off)
     ex = oracle.refine_exact(off, idx, init=init)
-    with R.Context(0, persistent=persist_log2 >= 0, persist_log2=persist_log2, grid_per_sm=grid) as ctx:
+    with R.Context(0, persistent=persist_log2 >= 0, persist_log2=persist_log2, grid_per_sm=grid,
+                   sig_kernel=sig_kernel) as ctx:
         g = ctx.upload(off, idx)
         for _ in range(2):
             r = g.refine(init)
@@ -46,10 +48,11 @@ def test_autotune_chooses_an_equivalent_setting():
     with R.Context(0) as ctx:
         g = ctx.upload(off, idx)
         ref = g.refine(lab)
-        t = g.autotune(d_init.data_ptr(), persist_log2=[14, 22, -1], grid_per_sm=[4, 16], use_graph=[1, 0], reps=2)
-        assert t["candidates"] == 12 and t["failed"] == 0
+        t = g.autotune(d_init.data_ptr(), persist_log2=[14, 22, -1], grid_per_sm=[4, 16], use_graph=[1, 0],
+                       sig_kernel=[1, 2], reps=2)
+        assert t["candidates"] == 24 and t["failed"] == 0
         assert t["best_ms"] <= t["default_ms"] + 1e-9
-        assert len(t["table"]) == 12
+        assert len(t["table"]) == 24
         r = g.refine(lab)  # under the chosen setting
         assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
         g.free()
