@@ -49,6 +49,26 @@ def env_rank():
             int(os.environ.get("LOCAL_RANK", 0)))
 
 
+def max_over_ranks(values, dist):
+    """Element-wise maximum of every rank's values (the slowest rank's times);
+    the values themselves with one rank.  NCCL reduces on the GPU, gloo on the
+    host."""
+    vals = [float(v) for v in values]
+    if dist is None:
+        return vals
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(vals, dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_value(world: int, arcs: int, rounds: int, steps: int, slowest_ms: float) -> float:
+    """Whole-job edge-rounds/s of N replicas: every rank refines its own copy
+    of the graph `steps` times; the job takes the slowest rank's time."""
+    return world * arcs * rounds * steps / (slowest_ms / 1000.0)
+
+
 def measured_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -266,11 +286,8 @@ def run_ours(args, rank, world, local_rank):
     rounds = results[0].rounds
     assert all(r.rounds == rounds and r.blocks == results[0].blocks and r.verified == 1 for r in results)
     launches = sum(r.kernel_launches for r in results)
-    if dist is not None:
-        t = torch.tensor([dev_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        dev_ms = float(t.item())
-    value = world * m * rounds * args.steps / (dev_ms / 1000.0)
+    dev_ms = max_over_ranks([dev_ms], dist)[0]
+    value = replica_value(world, m, rounds, args.steps, dev_ms)
 
     # per-kernel times: one refinement with CUDA events around every launch
     # (host-driven loop, same kernels and work as the timed graph-driven loop)
@@ -337,10 +354,7 @@ def run_ours(args, rank, world, local_rank):
         e2e_res.append(ctx.refine(off_np, idx_np, init=init_np, out=out_np))
     e2e_wall = time.perf_counter() - t0
     e2e_s = sum(r.time_s for r in e2e_res)
-    if dist is not None:
-        t = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks([e2e_s], dist)[0]
     assert all(r.rounds == rounds and r.blocks == results[0].blocks for r in e2e_res)
     assert np.array_equal(out_np, d_out.cpu().numpy().view(np.uint32))
     e2e = {"value": world * m * rounds * args.e2e_steps / e2e_s, "unit": UNIT,
@@ -350,9 +364,12 @@ def run_ours(args, rank, world, local_rank):
            "path": "rbsc_refine (C ABI): pinned host CSR + colours in, labels out"}
 
     batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
-    served = None if args.serve_requests <= 0 else run_served(args, world, dist, local_rank)
-    law = None if args.law_steps <= 0 else run_law(args, ctx)
-    streamed = None if args.stream_scale <= 0 else run_streamed(args, ctx, local_rank)
+    # the served, LAW and streamed sections describe one GPU (the streamed one
+    # alone pins 36 GB of host memory): they run at N = 1 only
+    single = world == 1
+    served = None if args.serve_requests <= 0 or not single else run_served(args, world, dist, local_rank)
+    law = None if args.law_steps <= 0 or not single else run_law(args, ctx)
+    streamed = None if args.stream_scale <= 0 or not single else run_streamed(args, ctx, local_rank)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -445,11 +462,7 @@ def run_batched(args, ctx, world, dist):
     per_res_t = time.perf_counter() - t0
     for gg in gs:
         gg.free()
-    ts = [float(np.median(one_t)), float(np.median(res_t)), per_t, per_res_t]
-    if dist is not None:
-        t = torch.tensor(ts, dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ts = t.tolist()
+    ts = max_over_ranks([float(np.median(one_t)), float(np.median(res_t)), per_t, per_res_t], dist)
     one_s, res_s, per_t, per_res_t = ts
     return {"workload": f"{G} graphs: n ~ U[10, 500]; even: Erdos-Renyi p = 4/(n-1), odd: random 3-regular; "
                         "symmetric arcs; labels U{1..8}",
