@@ -295,6 +295,14 @@ rbsc_status rbsc_graph_autotune(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_
 rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_graph* out);
 void rbsc_host_graph_free(rbsc_host_graph* g);
 
+/* A binary cache of a host CSR (8-byte offsets): rbsc_csr_save writes it,
+ * rbsc_csr_load reads it back (checksum, size and offsets checked), so a graph
+ * parsed once from text loads again without the parse.  No reference
+ * counterpart: the reference parses its text input on every run
+ * (rbsc.cu:156-180).  Free with rbsc_host_graph_free. */
+rbsc_status rbsc_csr_save(const char* path, const rbsc_csr* host_graph);
+rbsc_status rbsc_csr_load(const char* path, rbsc_host_graph* out);
+
 /* Reads a BV-compressed graph (the WebGraph format of the LAW datasets the
  * reference benchmarks on, which its webgraph-rs decodes to arcs-cuda text,
  * cli/src/to/arcscuda.rs:61-66): basename.properties, basename.graph and, if

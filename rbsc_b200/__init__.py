@@ -387,6 +387,21 @@ def parse_arcs(text: bytes):
     return _host_graph_to_numpy(lib, hg)
 
 
+def save_csr(path: str, off, idx, wt=None) -> None:
+    """Binary CSR cache file (rbsc_csr_save)."""
+    lib = _lib.load()
+    c, keep = _csr(np.ascontiguousarray(off, dtype=np.uint64), idx, wt)
+    _check(lib, lib.rbsc_csr_save(path.encode(), ctypes.byref(c)), None)
+
+
+def load_csr(path: str):
+    """(offsets, indices, weights | None) from a binary CSR cache file (rbsc_csr_load)."""
+    lib = _lib.load()
+    hg = _lib.HostGraph()
+    _check(lib, lib.rbsc_csr_load(path.encode(), ctypes.byref(hg)), None)
+    return _host_graph_to_numpy(lib, hg)
+
+
 def load_bvgraph(basename: str):
     """A BV-compressed (WebGraph / LAW) graph: (offsets uint64, indices uint32,
     stats dict) -- rbsc_bv_load."""

@@ -23,6 +23,9 @@
 //   --aggressive            the stop test of the reference's rbsc_aggressive
 //                           program (rbsc_aggressive.cu:487) in edge-batch mode
 //   --exact                 the coarsest partition whatever edge_batch_size is
+//   --csr-cache FILE        read the graph from this binary CSR cache when it
+//                           exists (stdin is not read); otherwise parse stdin
+//                           and write the cache
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -44,6 +47,7 @@ int main(int argc, char** argv)
 {
     const char* dump = nullptr;
     const char* init_path = nullptr;
+    const char* cache_path = nullptr;
     bool want_stats = false, aggressive = false, exact = false;
     int relabel = RBSC_RELABEL_HASH;
     std::vector<const char*> pos;
@@ -53,6 +57,7 @@ int main(int argc, char** argv)
         else if (!std::strcmp(argv[i], "--stats")) want_stats = true;
         else if (!std::strcmp(argv[i], "--aggressive")) aggressive = true;
         else if (!std::strcmp(argv[i], "--exact")) exact = true;
+        else if (!std::strcmp(argv[i], "--csr-cache") && i + 1 < argc) cache_path = argv[++i];
         else if (!std::strcmp(argv[i], "--relabel") && i + 1 < argc) relabel = !std::strcmp(argv[++i], "sort") ? RBSC_RELABEL_SORT : RBSC_RELABEL_HASH;
         else pos.push_back(argv[i]);
     }
@@ -61,18 +66,32 @@ int main(int argc, char** argv)
     unsigned long long gpus = pos.size() >= 2 ? std::strtoull(pos[1], nullptr, 10) : 1;
     (void)gpus;
 
-    std::string text;
-    if (!read_all(stdin, text)) {
-        std::printf("failed to read standard input\n");
-        return EXIT_FAILURE;
-    }
     rbsc_host_graph hg;
-    if (rbsc_parse_arcs(text.data(), text.size(), &hg) != RBSC_OK) {
-        std::printf("input error: %s\n", rbsc_last_error(nullptr));
-        return EXIT_FAILURE;
+    FILE* cached = cache_path ? std::fopen(cache_path, "rb") : nullptr;
+    if (cached) {
+        std::fclose(cached);
+        if (rbsc_csr_load(cache_path, &hg) != RBSC_OK) {
+            std::printf("input error: %s\n", rbsc_last_error(nullptr));
+            return EXIT_FAILURE;
+        }
+    } else {
+        std::string text;
+        if (!read_all(stdin, text)) {
+            std::printf("failed to read standard input\n");
+            return EXIT_FAILURE;
+        }
+        if (rbsc_parse_arcs(text.data(), text.size(), &hg) != RBSC_OK) {
+            std::printf("input error: %s\n", rbsc_last_error(nullptr));
+            return EXIT_FAILURE;
+        }
+        if (cache_path) {
+            rbsc_csr c{hg.n, hg.m, hg.offsets, 8, hg.indices, hg.weights};
+            if (rbsc_csr_save(cache_path, &c) != RBSC_OK) {
+                std::printf("cache error: %s\n", rbsc_last_error(nullptr));
+                return EXIT_FAILURE;
+            }
+        }
     }
-    text.clear();
-    text.shrink_to_fit();
 
     std::vector<uint32_t> init;
     if (init_path) {

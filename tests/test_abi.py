@@ -98,3 +98,25 @@ def test_cli_fails_loudly_without_device():
 def test_cli_parse_error_on_stdout():
     r = subprocess.run([_lib.CLI_PATH], input=b"2\n3\n0 1 1\n", capture_output=True, timeout=60)
     assert r.returncode != 0 and b"input error" in r.stdout
+
+
+def test_csr_cache_roundtrip_and_checks(tmp_path):
+    import rbsc_b200 as R
+    from rbsc_b200 import graphs as G
+    off, idx = G.rmat(10, 8, seed=2)
+    wt = np.arange(len(idx), dtype=np.uint64) % 5 + 1
+    for w in (None, wt):
+        p = str(tmp_path / ("g_w.csr" if w is not None else "g.csr"))
+        R.save_csr(p, off, idx, w)
+        o2, i2, w2 = R.load_csr(p)
+        assert np.array_equal(o2, off) and np.array_equal(i2, idx)
+        assert (w2 is None) if w is None else np.array_equal(w2, w)
+    # a flipped byte, a truncated file, a foreign file
+    raw = bytearray(open(str(tmp_path / "g.csr"), "rb").read())
+    raw[-1] ^= 0x40
+    open(str(tmp_path / "bad.csr"), "wb").write(bytes(raw))
+    open(str(tmp_path / "short.csr"), "wb").write(bytes(raw[:-3]))
+    open(str(tmp_path / "text.csr"), "wb").write(b"3\n1\n0 1 2\n")
+    for name in ("bad.csr", "short.csr", "text.csr"):
+        with pytest.raises(R.RbscError):
+            R.load_csr(str(tmp_path / name))

@@ -326,6 +326,22 @@ def test_cli_three_lines_and_partition(tmp_path):
     assert np.array_equal(got, labels)
 
 
+def test_cli_csr_cache(tmp_path):
+    """--csr-cache: the first run parses stdin and writes the cache, the second
+    reads the cache (stdin empty) and prints the same `done` / `nodes`."""
+    off, idx, wt, init, labels, meta = load_case("rmat10", INDEX["rmat10"])
+    text = oracle.arcs_cuda_text(off, idx, wt)
+    cache = tmp_path / "g.csr"
+    outs = []
+    for inp in (text, b""):
+        r = subprocess.run([_lib.CLI_PATH, str(int(off[-1])), "1", "--csr-cache", str(cache)], input=inp,
+                           capture_output=True, timeout=120)
+        assert r.returncode == 0, r.stdout
+        outs.append(r.stdout.decode().strip().split("\n")[1:])
+    assert cache.exists()
+    assert outs[0] == outs[1] == ["1", str(meta["blocks"])]
+
+
 def test_run_api():
     off, idx, wt, init, labels, meta = load_case("lift64x8", INDEX["lift64x8"])
     t, done, nodes = R.run(oracle.arcs_cuda_text(off, idx))
