@@ -134,6 +134,11 @@ struct rbsc_graph {
     uint64_t resident_cap = 0;      // arcs the compacted (device) arc sets hold
     uint64_t streamed_bytes = 0;    // copied by the streamed passes of the last refinement
     uint32_t streamed_passes = 0;
+    // one-shot upload that overlaps the refinement: the heads arrive in
+    // chunks (copied into d_idx on copy_stream) during the first pass that
+    // reads them; until then d_idx is only partly filled
+    bool stream_upload = false;
+    const uint32_t* h_upload = nullptr;
 };
 
 rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);

@@ -24,8 +24,9 @@ static __global__ void k_validate(uint32_t n, uint64_t m, const uint64_t* __rest
         if (off[i] > off[i + 1]) atomicOr(err, 1u);
     }
     if (i == 0 && (off[0] != 0 || off[n] != m)) atomicOr(err, 2u);
-    for (uint64_t k = i; k < m; k += (uint64_t)gridDim.x * blockDim.x)
-        if (idx[k] >= n) atomicOr(err, 4u);
+    if (idx)  // null: the heads are checked as they arrive (k_validate_heads)
+        for (uint64_t k = i; k < m; k += (uint64_t)gridDim.x * blockDim.x)
+            if (idx[k] >= n) atomicOr(err, 4u);
 }
 
 template <typename OffIn>

@@ -319,15 +319,15 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
     cudaStreamSynchronize(g->ctx->stream);
     graph_release_refine(g);
     dev_free(g->ctx, (void*&)g->d_off);
+    if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
+    for (int i = 0; i < 2; ++i) {
+        dev_free(g->ctx, (void*&)g->d_chunk[i]);
+        dev_free(g->ctx, (void*&)g->d_chunk_wt[i]);
+        if (g->ev_copied[i]) cudaEventDestroy(g->ev_copied[i]);
+        if (g->ev_used[i]) cudaEventDestroy(g->ev_used[i]);
+    }
+    if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     if (g->host_arcs) {
-        if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
-        for (int i = 0; i < 2; ++i) {
-            dev_free(g->ctx, (void*&)g->d_chunk[i]);
-            dev_free(g->ctx, (void*&)g->d_chunk_wt[i]);
-            if (g->ev_copied[i]) cudaEventDestroy(g->ev_copied[i]);
-            if (g->ev_used[i]) cudaEventDestroy(g->ev_used[i]);
-        }
-        if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
         if (g->reg_idx) cudaHostUnregister(g->reg_idx);
         if (g->reg_wt) cudaHostUnregister(g->reg_wt);
         g->d_idx = nullptr;  // host memory of the caller
@@ -372,7 +372,8 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g)
     struct Guard { rbsc_ctx* c; uint32_t*& p; ~Guard() { dev_free(c, (void*&)p); } } guard{ctx, d_err};
     CK(cudaMemsetAsync(d_err, 0, sizeof(uint32_t) * 4, s));
     ++rbsc::launch_counter();
-    k_validate<<<grid_for(std::max<uint64_t>(n, 1), 256) > 65535u * 16 ? 65535u * 16 : grid_for(std::max<uint64_t>(n, 1), 256), 256, 0, s>>>(n, m, g->d_off, g->d_idx, d_err);
+    k_validate<<<grid_for(std::max<uint64_t>(n, 1), 256) > 65535u * 16 ? 65535u * 16 : grid_for(std::max<uint64_t>(n, 1), 256), 256, 0, s>>>(
+        n, m, g->d_off, g->stream_upload ? nullptr : g->d_idx, d_err);
     CK(cudaGetLastError());
     uint32_t herr = 0;
     CK(cudaMemcpyAsync(&herr, d_err, sizeof herr, cudaMemcpyDeviceToHost, s));
@@ -495,8 +496,11 @@ rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted)
     return RBSC_OK;
 }
 
+// defer_heads: the heads are not copied here; they arrive in chunks during
+// the first pass that reads them (stream_signature's upload mode), which
+// overlaps their copy with the initial colours, the setup and that pass.
 static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device, rbsc_graph** out, double* h2d_ms,
-                              uint64_t* h2d_bytes)
+                              uint64_t* h2d_bytes, bool defer_heads = false)
 {
     *out = nullptr;
     CKS(check_csr_args(ctx, c));
@@ -536,7 +540,16 @@ static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device
         cudaStreamSynchronize(s);
         dev_free(ctx, tmp);
     }
-    if (e == cudaSuccess && c->m) e = cudaMemcpyAsync(g->d_idx, c->indices, sizeof(uint32_t) * c->m, kind, s);
+    defer_heads = defer_heads && !from_device && !c->weights && c->m > 0;
+    if (defer_heads) {
+        g->stream_upload = true;
+        g->h_upload = c->indices;
+        g->chunk_tiles = (uint32_t)std::max<uint64_t>(1, ceil_div<uint64_t>(ceil_div<uint64_t>(c->m, kTileEdges), 8));
+        if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking);
+        for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->ev_copied[i], cudaEventDisableTiming);
+    } else if (e == cudaSuccess && c->m) {
+        e = cudaMemcpyAsync(g->d_idx, c->indices, sizeof(uint32_t) * c->m, kind, s);
+    }
     if (e == cudaSuccess && c->weights && c->m) e = cudaMemcpyAsync(g->d_wt, c->weights, sizeof(uint64_t) * c->m, kind, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     auto t1 = std::chrono::steady_clock::now();
@@ -768,21 +781,38 @@ static void launch_signature_chunk(bool weighted, bool staged, unsigned grid, cu
 // are copied into two device buffers on copy_stream; chunk c's copy waits
 // until the kernel that read its buffer (chunk c-2) is done, and its kernel
 // waits for the copy, so copies run beside the kernels of earlier chunks.
+//
+// Upload mode (g->stream_upload, the one-shot refinement of an unweighted
+// graph): the chunks go straight to their final place in d_idx, each checked
+// by k_validate_heads before its signature kernel reads it; after the pass
+// the arcs are resident.
 static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, int first)
 {
     const uint64_t m = g->m;
     const uint32_t ntiles = g->ntiles;
+    const bool upload = g->stream_upload;
     for (uint32_t t0 = 0, c = 0; t0 < ntiles; t0 += g->chunk_tiles, ++c) {
         const uint32_t t1 = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)t0 + g->chunk_tiles);
         const uint64_t a0 = (uint64_t)t0 * kTileEdges, a1 = std::min<uint64_t>(m, (uint64_t)t1 * kTileEdges);
         const int slot = (int)(c & 1u);
-        CK(cudaStreamWaitEvent(g->copy_stream, g->ev_used[slot], 0));
-        CK(cudaMemcpyAsync(g->d_chunk[slot], g->d_idx + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
-        if (g->weighted)
-            CK(cudaMemcpyAsync(g->d_chunk_wt[slot], g->d_wt + a0, 8 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        if (upload) {
+            CK(cudaMemcpyAsync(g->d_idx + a0, g->h_upload + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        } else {
+            CK(cudaStreamWaitEvent(g->copy_stream, g->ev_used[slot], 0));
+            CK(cudaMemcpyAsync(g->d_chunk[slot], g->d_idx + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+            if (g->weighted)
+                CK(cudaMemcpyAsync(g->d_chunk_wt[slot], g->d_wt + a0, 8 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        }
         CK(cudaEventRecord(g->ev_copied[slot], g->copy_stream));
         CK(cudaStreamWaitEvent(s, g->ev_copied[slot], 0));
-        const TileRange r{t0, t1, g->d_chunk[slot], g->weighted ? g->d_chunk_wt[slot] : nullptr, a0};
+        if (upload) {
+            ++rbsc::launch_counter();
+            k_validate_heads<<<persistent_grid(ctx, ceil_div<uint64_t>(a1 - a0, 256), 1), 256, 0, s>>>(a0, a1, g->n, g->d_idx,
+                                                                                                      g->d_st);
+            CK(cudaGetLastError());
+        }
+        const TileRange r = upload ? TileRange{t0, t1, g->d_idx + a0, nullptr, a0}
+                                   : TileRange{t0, t1, g->d_chunk[slot], g->weighted ? g->d_chunk_wt[slot] : nullptr, a0};
         const unsigned grid = persistent_grid(ctx, t1 - t0, kTileThreads / 32);
         const bool st = staged_signature(ctx, g);
         if (first == kPassRank8)
@@ -794,10 +824,25 @@ static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s
         else
             launch_signature_chunk<uint32_t>(g->weighted, st, grid, s, g->d_as, g->d_st, g->d_col[0], g->d_sig, r);
         CK(cudaGetLastError());
-        CK(cudaEventRecord(g->ev_used[slot], s));
+        if (!upload) CK(cudaEventRecord(g->ev_used[slot], s));
         g->streamed_bytes += (a1 - a0) * (g->weighted ? 12 : 4);
     }
     ++g->streamed_passes;
+    g->stream_upload = false;
+    return RBSC_OK;
+}
+
+// An upload still pending when a pass that reads no arcs (the uniform first
+// pass) would be followed by kernels that do: copy and check the rest now.
+static rbsc_status finish_upload(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
+{
+    if (g->m) {
+        CK(cudaMemcpyAsync(g->d_idx, g->h_upload, 4 * g->m, cudaMemcpyHostToDevice, s));
+        ++rbsc::launch_counter();
+        k_validate_heads<<<persistent_grid(ctx, ceil_div<uint64_t>(g->m, 256), 1), 256, 0, s>>>(0, g->m, g->n, g->d_idx, g->d_st);
+        CK(cudaGetLastError());
+    }
+    g->stream_upload = false;
     return RBSC_OK;
 }
 
@@ -814,7 +859,8 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (t) CK(cudaEventRecord(t->ev[1], s));
     // the host-launched first pass is never captured: time its signature kernel
     if (first != kPassFull) CK(cudaEventRecord(ctx->ev_sig[0], s));
-    const bool streamed = g->arcs_on_host && g->m > 0 && first != kPassUniform;
+    const bool streamed = (g->arcs_on_host || g->stream_upload) && g->m > 0 && first != kPassUniform;
+    if (g->stream_upload && !streamed) CKS(finish_upload(ctx, g, s));
     if (streamed) {
         CKS(stream_signature(ctx, g, s, first));
     } else if (g->m > 0) {
@@ -1435,6 +1481,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     g->next_stamp = hs.stamp;
     if (hs.error & kErrProbe) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "relabel table overflow");
     if (hs.error & kErrStage) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "signature: a staged tile copy did not complete");
+    if (hs.error & kErrInput) return rbsc_fail(ctx, RBSC_ERR_INVALID, "an arc head is >= N");
     if (hs.error & kErrRounds) return rbsc_fail(ctx, RBSC_ERR_NOT_CONVERGED, "no fixpoint after %u passes", hs.round);
     uint32_t* out = d_out ? d_out : g->d_out;
     ++rbsc::launch_counter();
@@ -1527,7 +1574,9 @@ extern "C" rbsc_status rbsc_refine(rbsc_ctx* ctx, const rbsc_csr* host_graph, co
     rbsc_graph* g = nullptr;
     double up_ms = 0;
     uint64_t up_bytes = 0;
-    CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes));
+    // large unweighted graphs: the heads' copy overlaps the refinement
+    const bool defer = host_graph && !host_graph->weights && host_graph->m >= (1ull << 22);
+    CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes, defer));
     g->oneshot = true;
     rbsc_status st = rbsc_graph_refine(ctx, g, init_colors, out_labels, stats);
     rbsc_graph_free(g);

@@ -54,6 +54,19 @@ constexpr uint32_t kErrProbe = 1u;   // relabel table full (cannot happen at loa
 constexpr uint32_t kErrRounds = 2u;  // max_rounds reached
 constexpr uint32_t kErrBarrier = 4u; // a grid barrier of the persistent kernel timed out
 constexpr uint32_t kErrStage = 8u;   // a staged (bulk async) copy of k_signature_staged did not complete
+constexpr uint32_t kErrInput = 16u;  // an uploaded head is >= N (k_validate_heads)
+
+// Heads [a0, a1) of an upload that arrives during the first pass: any head
+// >= n sets kErrInput, and the signature kernels that would gather it return
+// without reading (they check the error word first).
+static __global__ void k_validate_heads(uint64_t a0, uint64_t a1, uint32_t n, const uint32_t* __restrict__ idx,
+                                        RoundState* __restrict__ st)
+{
+    bool bad = false;
+    for (uint64_t k = a0 + (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < a1; k += (uint64_t)gridDim.x * blockDim.x)
+        bad |= idx[k] >= n;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(&st->error, kErrInput);
+}
 
 // What the pass kernels work on; the compaction kernels shrink it.
 struct ActiveSet {
@@ -505,6 +518,7 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature_staged(const 
     __shared__ __align__(128) uint32_t s_idx[kStageWarps][2][kTileEdges];
     __shared__ __align__(16) uint8_t s_hd[kStageWarps][2][kTileEdges / 8];
     __shared__ __align__(8) uint64_t s_bar[kStageWarps][2];
+    if (*(const volatile uint32_t*)&st->error) return;
     const uint32_t lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
     const uint32_t ntiles = use_range ? rng.hi : as->ntiles;
     const uint64_t m = as->m;
@@ -607,6 +621,7 @@ static __global__ void __launch_bounds__(kTileThreads) k_signature_chunk(const A
                                                                          const ColT* __restrict__ col,
                                                                          Sig* __restrict__ sig, TileRange rng)
 {
+    if (*(const volatile uint32_t*)&st->error) return;  // e.g. a bad head in this chunk
     signature_body<WEIGHTED, ColT, true, true>(as, st, col, sig, rng);
 }
 

@@ -139,3 +139,27 @@ def test_pinned_generator_matches_host_generator(ctx):
         assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
     finally:
         pg.free()
+
+
+def test_one_shot_upload_overlapped_with_the_first_pass(ctx):
+    """rbsc_refine of a large unweighted graph copies the heads in chunks during
+    the first pass: same result as the resident graph, with and without
+    initial colours (a uniform first pass reads no arc: the upload finishes
+    before the kernels that do)."""
+    off, idx = R.gen_rmat_host(18, 20, seed=6)
+    assert len(idx) >= (1 << 22)
+    for init in (R.degree_bucket_colors(off), None):
+        ref = ctx.upload(off, idx).refine(init)
+        r = ctx.refine(off, idx, init=init)
+        assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
+
+
+def test_one_shot_upload_rejects_a_bad_head(ctx):
+    off, idx = R.gen_rmat_host(18, 20, seed=7)
+    bad = idx.copy()
+    bad[len(bad) * 3 // 4] = len(off) - 1 + 5  # a head >= N in the fourth chunk
+    with pytest.raises(R.RbscError) as e:
+        ctx.refine(off, bad, init=R.degree_bucket_colors(off))
+    assert e.value.status == -1
+    r = ctx.refine(off, idx)  # the context is still usable
+    assert r.done == 1
