@@ -78,10 +78,11 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def signature_traffic_per_arc():
-    """DRAM bytes per arc of k_signature from the committed ncu summary
-    (profiles/k_signature_rmat24.md, line 'traffic_bytes_per_arc: X'), or None."""
-    p = os.path.join(ROOT, "profiles", "k_signature_rmat24.md")
+def signature_traffic_per_arc(kernel: str = "k_signature"):
+    """DRAM bytes per arc of the first-pass signature kernel from its committed
+    ncu summary (profiles/<kernel>_rmat24.md, line 'traffic_bytes_per_arc: X'),
+    or None."""
+    p = os.path.join(ROOT, "profiles", f"{kernel}_rmat24.md")
     try:
         for ln in open(p):
             if ln.startswith("traffic_bytes_per_arc:"):
@@ -308,10 +309,14 @@ def run_ours(args, rank, world, local_rank):
     sig_bytes_p1 = 8 * arcs1 + n * (ob + 8)
     sig_bytes_all = sum(8 * p["arcs"] for p in per_pass) + len(per_pass) * n * (ob + 8)
     sig_ms_all = sum(p["signature_ms"] for p in per_pass)
-    tpa = signature_traffic_per_arc()
+    hot = results[0].first_signature_hot
+    kname = "k_signature_hot" if hot else "k_signature"
+    tpa = signature_traffic_per_arc(kname)
     round_bytes = 8 * m + n * (ob + 28)
     ach = sig_bytes_p1 / (sig_ms1 / 1e3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "k_signature (first pass: every arc)",
+    kdesc = (f"{kname} (first pass: every arc; the class ranks of the {hot} most pointed-to nodes "
+             "read from shared memory)" if hot else f"{kname} (first pass: every arc)")
+    roofline = {"bound": "hbm", "kernel": kdesc,
                 "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                 "traffic": None if tpa is None else tpa * arcs1,
                 "algorithmic_bytes_per_launch": sig_bytes_p1, "arcs_per_launch": arcs1, "launch_ms": sig_ms1,

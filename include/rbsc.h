@@ -76,10 +76,16 @@ typedef struct {
                                  and listed nodes are both <= 2^persist_log2
                                  (0 = default 22)                                       */
     int32_t grid_per_sm;      /* blocks per SM of the pass kernels' grids (0 = 16)      */
-    int32_t sig_kernel;       /* signature kernel over device arcs: 0 = default (plain
-                                 loads), 1 = plain loads, 2 = staged (each warp's tiles
-                                 copied to shared memory by cp.async.bulk; unweighted) */
-    int32_t reserved[3];
+    int32_t sig_kernel;       /* signature kernel over device arcs: 0 = default (hot
+                                 heads where they apply, else plain loads), 1 = plain
+                                 loads, 2 = staged (each warp's tiles copied to shared
+                                 memory by cp.async.bulk; unweighted), 3 = hot heads:
+                                 the first pass of a resident graph with >= 2^22 arcs
+                                 and <= 256 initial classes reads the class ranks of
+                                 the most pointed-to nodes from shared memory          */
+    int32_t hot_log2;         /* hot heads: at most 2^hot_log2 nodes, those with the
+                                 most in-arcs (0 = default 17; 10..17)                  */
+    int32_t reserved[2];
 } rbsc_opts;
 
 typedef struct {
@@ -108,7 +114,8 @@ typedef struct {
     uint64_t streamed_bytes;  /* host->device bytes of the streamed signature passes
                                  (graphs from rbsc_graph_upload_streamed)                */
     uint32_t streamed_passes; /* signature passes that streamed the arcs                */
-    uint32_t pad;
+    uint32_t first_signature_hot; /* hot heads the first signature kernel read from shared
+                                     memory (0: it gathered every rank from global memory) */
 } rbsc_stats;
 
 /* Per-kernel device time of one refinement, measured with CUDA events around
@@ -268,7 +275,8 @@ typedef struct {
     uint32_t n_relabel;
     int32_t use_graph[RBSC_TUNE_MAX];     /* CUDA-graph loop 1 / host loop 0                */
     uint32_t n_use_graph;
-    int32_t sig_kernel[RBSC_TUNE_MAX];    /* signature kernels to try (1 plain, 2 staged)   */
+    int32_t sig_kernel[RBSC_TUNE_MAX];    /* signature kernels to try (1 plain, 2 staged,
+                                             3 hot heads)                              */
     uint32_t n_sig_kernel;
     uint32_t reps;                        /* timed refinements per candidate (0 = 3)         */
 } rbsc_tune_space;

@@ -60,6 +60,7 @@ class Result:
     first_signature_arcs: int = 0
     streamed_bytes: int = 0
     streamed_passes: int = 0
+    first_signature_hot: int = 0
 
 
 def _result(st: _lib.Stats, labels) -> Result:
@@ -68,7 +69,8 @@ def _result(st: _lib.Stats, labels) -> Result:
                   int(st.initial_blocks), float(st.time_s), float(st.device_ms), float(st.verify_ms),
                   float(st.h2d_ms), float(st.d2h_ms), int(st.h2d_bytes), int(st.d2h_bytes), rb,
                   int(st.kernel_launches), float(st.init_ms), float(st.loop_ms), float(st.first_signature_ms),
-                  int(st.first_signature_arcs), int(st.streamed_bytes), int(st.streamed_passes))
+                  int(st.first_signature_arcs), int(st.streamed_bytes), int(st.streamed_passes),
+                  int(st.first_signature_hot))
 
 
 def _check(lib, status: int, ctx=None):
@@ -102,7 +104,8 @@ class Context:
 
     def __init__(self, device: int = 0, relabel: int = RELABEL_HASH, verify: bool = True, max_rounds: int = 0,
                  use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0,
-                 persistent: bool = True, persist_log2: int = 0, grid_per_sm: int = 0, sig_kernel: int = 0):
+                 persistent: bool = True, persist_log2: int = 0, grid_per_sm: int = 0, sig_kernel: int = 0,
+                 hot_log2: int = 0):
         self._lib = _lib.load()
         o = _lib.Opts()
         self._lib.rbsc_opts_default(ctypes.byref(o))
@@ -116,6 +119,7 @@ class Context:
         o.persist_log2 = persist_log2
         o.grid_per_sm = grid_per_sm
         o.sig_kernel = sig_kernel
+        o.hot_log2 = hot_log2
         self._opts = o
         h = self._lib.rbsc_ctx_create(device, ctypes.byref(o))
         if not h:

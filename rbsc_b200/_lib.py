@@ -61,7 +61,8 @@ class Opts(ctypes.Structure):
         ("persist_log2", ctypes.c_int32),
         ("grid_per_sm", ctypes.c_int32),
         ("sig_kernel", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 3),
+        ("hot_log2", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 2),
     ]
 
 
@@ -88,7 +89,7 @@ class Stats(ctypes.Structure):
         ("first_signature_arcs", ctypes.c_uint64),
         ("streamed_bytes", ctypes.c_uint64),
         ("streamed_passes", ctypes.c_uint32),
-        ("pad", ctypes.c_uint32),
+        ("first_signature_hot", ctypes.c_uint32),
     ]
 
 

@@ -62,6 +62,15 @@ struct rbsc_graph {
     uint32_t* d_joined = nullptr;    // per node: pass in which a member joined its representative's class
     uint32_t* d_out = nullptr;
     void* d_rank = nullptr;          // first pass: dense class ranks (uint8 / uint16)
+    // hot heads of the first pass (hot_kernels.cuh), built once per graph
+    uint32_t* d_hot_idx = nullptr;   // heads, hot ones as kHotFlag | slot
+    uint32_t* d_hot_node = nullptr;  // node of each hot slot
+    uint8_t* d_hot_rank = nullptr;   // per refinement: class rank of each hot slot
+    uint32_t hot_n = 0;              // hot slots
+    uint32_t hot_bytes = 0;          // staged table: hot_n rounded up to 16
+    int hot_state = 0;               // 0 not built, 1 built, -1 not applicable (no skew, no memory)
+    uint32_t hot_log2 = 0;           // the size limit it was built (or rejected) for
+    bool hot_active = false;         // the running refinement's first pass uses it
     uint32_t* d_srank = nullptr;     // rank of the initial class claimed at each table slot
     uint32_t* d_init = nullptr;
     rbsc::Entry* d_tab = nullptr;

@@ -17,6 +17,7 @@
 #include "prep_kernels.cuh"
 #include "radix.cuh"
 #include "refine_kernels.cuh"
+#include "hot_kernels.cuh"
 #include "scan.cuh"
 #include "verify_kernels.cuh"
 #include "internal.h"
@@ -289,6 +290,10 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free(g->ctx, (void*&)g->d_st);
     dev_free(g->ctx, (void*&)g->d_out);
     dev_free(g->ctx, (void*&)g->d_rank);
+    dev_free(g->ctx, (void*&)g->d_hot_idx);
+    dev_free(g->ctx, (void*&)g->d_hot_node);
+    dev_free(g->ctx, (void*&)g->d_hot_rank);
+    g->hot_state = 0;
     dev_free(g->ctx, (void*&)g->d_init);
     dev_free(g->ctx, (void*&)g->d_vflag);
     dev_free(g->ctx, (void*&)g->d_vrow);
@@ -734,6 +739,119 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     return RBSC_OK;
 }
 
+// Hot heads of the first pass (hot_kernels.cuh): for a resident graph with
+// >= 2^22 arcs in device memory, unless the options choose another
+// signature kernel.
+static uint32_t hot_limit_log2(const rbsc_ctx* ctx)
+{
+    const int32_t l = ctx->opts.hot_log2;
+    if (l == 0) return kHotMaxLog2;
+    return (uint32_t)std::min<int32_t>(std::max<int32_t>(l, (int32_t)kHotMinLog2), (int32_t)kHotMaxLog2);
+}
+
+static bool hot_wanted(const rbsc_ctx* ctx, const rbsc_graph* g)
+{
+    const int32_t k = ctx->opts.sig_kernel;
+    return (k == 0 || k == 3) && !g->host_arcs && !g->oneshot && !g->stream_upload && g->m >= (1ull << 22) && g->n > 1;
+}
+
+// In-degree threshold that at most `limit` nodes reach, from the binned
+// in-degrees (in-degree >= 2 only); 0 when no node qualifies.
+static uint32_t hot_threshold(const uint32_t* bins, uint64_t limit)
+{
+    uint64_t above = 0;
+    uint32_t thr = 0;
+    for (uint32_t b = kHotBins; b-- > 2;) {
+        if (above + bins[b] > limit) break;
+        above += bins[b];
+        if (above) thr = hot_bin_floor(b);
+    }
+    return thr;
+}
+
+// Builds the hot heads of a graph once per size limit: in-degrees, the
+// threshold, the slots, the encoded copy of the heads.  false (nothing kept)
+// when no node qualifies or device memory is short: the plain kernel runs.
+static rbsc_status build_hot(rbsc_ctx* ctx, rbsc_graph* g, bool* ready)
+{
+    const uint32_t lim = hot_limit_log2(ctx);
+    *ready = false;
+    if (g->hot_state != 0 && g->hot_log2 == lim) {
+        *ready = g->hot_state > 0;
+        return RBSC_OK;
+    }
+    cudaStream_t s = ctx->stream;
+    dev_free(ctx, (void*&)g->d_hot_idx);
+    dev_free(ctx, (void*&)g->d_hot_node);
+    dev_free(ctx, (void*&)g->d_hot_rank);
+    g->hot_state = -1;
+    g->hot_log2 = lim;
+    g->hot_n = g->hot_bytes = 0;
+    const uint32_t n = g->n;
+    const uint64_t mpad = (uint64_t)g->ntiles * kTileEdges;
+    uint32_t* deg = nullptr;
+    uint32_t* slot = nullptr;
+    uint32_t* bins = nullptr;
+    void* tmp = nullptr;
+    auto drop = [&]() {
+        dev_free(ctx, (void*&)deg);
+        dev_free(ctx, (void*&)slot);
+        dev_free(ctx, (void*&)bins);
+        dev_free(ctx, tmp);
+    };
+    const size_t tbytes = scan_temp_bytes<uint32_t>((uint64_t)n) + 256;
+    if (dev_alloc(ctx, (void**)&deg, 4ull * n) != RBSC_OK || dev_alloc(ctx, (void**)&slot, 4ull * n + 16) != RBSC_OK ||
+        dev_alloc(ctx, (void**)&bins, 4 * kHotBins) != RBSC_OK || dev_alloc(ctx, &tmp, tbytes) != RBSC_OK) {
+        drop();
+        return RBSC_OK;
+    }
+    const unsigned agrid = (unsigned)ctx->sm_count * 16;
+    CK(cudaMemsetAsync(deg, 0, 4ull * n, s));
+    CK(cudaMemsetAsync(bins, 0, 4 * kHotBins, s));
+    ++rbsc::launch_counter();
+    k_hot_indeg<<<agrid, 256, 0, s>>>(g->d_idx, g->m, deg);
+    ++rbsc::launch_counter();
+    k_hot_hist<<<(unsigned)ctx->sm_count * 4, 256, 0, s>>>(n, deg, bins);
+    CK(cudaGetLastError());
+    uint32_t hb[kHotBins];
+    CK(cudaMemcpyAsync(hb, bins, sizeof hb, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const uint32_t thr = hot_threshold(hb, 1ull << lim);
+    if (thr < 2) {
+        drop();
+        return RBSC_OK;
+    }
+    ++rbsc::launch_counter();
+    k_hot_flags<<<grid_for(n, 256), 256, 0, s>>>(n, deg, thr);
+    uint32_t* total = slot + n;
+    CK((exclusive_scan<uint32_t, uint32_t>(deg, slot, n, total, tmp, s)));
+    uint32_t hot_n = 0;
+    CK(cudaMemcpyAsync(&hot_n, total, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const uint32_t hot_bytes = (uint32_t)ceil_div<uint64_t>(hot_n, 16) * 16;
+    if (hot_n == 0 || hot_n > (1u << lim) || dev_alloc(ctx, (void**)&g->d_hot_node, 4ull * hot_n) != RBSC_OK ||
+        dev_alloc(ctx, (void**)&g->d_hot_rank, hot_bytes) != RBSC_OK || dev_alloc(ctx, (void**)&g->d_hot_idx, 4 * mpad) != RBSC_OK) {
+        dev_free(ctx, (void*&)g->d_hot_node);
+        dev_free(ctx, (void*&)g->d_hot_rank);
+        drop();
+        return RBSC_OK;
+    }
+    ++rbsc::launch_counter();
+    k_hot_assign<<<grid_for(n, 256), 256, 0, s>>>(n, deg, slot, g->d_hot_node);
+    ++rbsc::launch_counter();
+    k_hot_encode<<<agrid, 256, 0, s>>>(g->d_idx, g->m, deg, g->d_hot_idx);
+    CK(cudaGetLastError());
+    CK(cudaFuncSetAttribute(k_signature_hot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1 << kHotMaxLog2));
+    CK(cudaFuncSetAttribute(k_signature_hot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1 << kHotMaxLog2));
+    CK(cudaStreamSynchronize(s));
+    drop();
+    g->hot_n = hot_n;
+    g->hot_bytes = hot_bytes;
+    g->hot_state = 1;
+    *ready = true;
+    return RBSC_OK;
+}
+
 // The persistent kernel takes over once both the active arcs and the listed
 // nodes are at most 2^persist_log2 (option; default 22).
 static uint64_t persist_limit(const rbsc_ctx* ctx)
@@ -883,6 +1001,15 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
                     g->d_as, g->d_st, reinterpret_cast<const uint16_t*>(g->d_rank), g->d_sig, all, 0);
             else
                 k_signature_staged<uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, all, 0);
+        } else if (first == kPassRank8 && g->hot_active) {
+            const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
+            const unsigned hgrid = std::min<unsigned>((unsigned)ctx->sm_count, ceil_div<uint32_t>(g->ntiles, kHotThreads / 32));
+            if (g->weighted)
+                k_signature_hot<true><<<hgrid, kHotThreads, g->hot_bytes, s>>>(g->d_as, g->d_st, cr, g->d_hot_idx, g->d_hot_rank,
+                                                                              g->hot_bytes, g->d_sig);
+            else
+                k_signature_hot<false><<<hgrid, kHotThreads, g->hot_bytes, s>>>(g->d_as, g->d_st, cr, g->d_hot_idx,
+                                                                               g->d_hot_rank, g->hot_bytes, g->d_sig);
         } else if (first == kPassRank8) {
             const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
             if (g->weighted)
@@ -1448,6 +1575,20 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
             CK(cudaGetLastError());
         }
     }
+    // hot heads: the first pass reads the ranks of the most pointed-to nodes
+    // from shared memory
+    g->hot_active = false;
+    if (first == kPassRank8 && hot_wanted(ctx, g)) {
+        bool ready = false;
+        CKS(build_hot(ctx, g, &ready));
+        if (ready) {
+            ++rbsc::launch_counter();
+            k_hot_ranks<<<grid_for(g->hot_bytes, 256), 256, 0, s>>>(g->hot_n, g->hot_bytes, g->d_hot_node,
+                                                                   reinterpret_cast<const uint8_t*>(g->d_rank), g->d_hot_rank);
+            CK(cudaGetLastError());
+            g->hot_active = true;
+        }
+    }
 
     float verify_ms = 0.f, loop_ms = 0.f;
     uint32_t repairs = 0;
@@ -1508,6 +1649,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         stats->first_signature_arcs = g->first_sig_arcs;
         stats->streamed_bytes = g->streamed_bytes;
         stats->streamed_passes = g->streamed_passes;
+        stats->first_signature_hot = g->hot_active ? g->hot_n : 0u;
     }
     if (kt) kt->total_ms = total_ms;
     return RBSC_OK;
@@ -1616,6 +1758,7 @@ extern "C" void rbsc_tune_space_default(rbsc_tune_space* sp)
     sp->use_graph[sp->n_use_graph++] = 0;
     sp->sig_kernel[sp->n_sig_kernel++] = 1;
     sp->sig_kernel[sp->n_sig_kernel++] = 2;
+    sp->sig_kernel[sp->n_sig_kernel++] = 3;
     sp->reps = 3;
 }
 

@@ -268,6 +268,20 @@ __device__ __forceinline__ uint32_t gather_col(const ColT* p)
     else return (uint32_t)__ldcg(p);
 }
 
+// Hot heads (first pass, 1-byte class ranks): a head with bit 31 set is the
+// slot of one of the most pointed-to nodes, whose rank sits in shared memory
+// (s_hot); any other head is a node id.  Node ids are < 2^31.
+constexpr uint32_t kHotFlag = 0x80000000u;
+
+template <bool NC, typename ColT, bool HOT>
+__device__ __forceinline__ uint32_t gather_head(const ColT* col, const uint8_t* s_hot, uint32_t h)
+{
+    if constexpr (HOT) {
+        if (h & kHotFlag) return (uint32_t)s_hot[h & ~kHotFlag];
+    }
+    return gather_col<NC>(col + h);
+}
+
 // A range of tiles [lo, hi) whose heads (and weights) were copied to a chunk
 // buffer that starts at arc `base` (streamed arc sets); the default range is
 // every tile, read from the active set's own arrays.
@@ -385,11 +399,18 @@ __device__ __forceinline__ void signature_fold(uint32_t lane, uint32_t a, uint32
     }
 }
 
-template <bool WEIGHTED, typename ColT, bool NC = true, bool RANGE = false>
+// HOT: the heads come from hot_idx (same positions as the active set's
+// heads, hot ones encoded as kHotFlag | slot) and ColT is the 1-byte rank.
+// WPB: warps per block.
+template <bool WEIGHTED, typename ColT, bool NC = true, bool RANGE = false, bool HOT = false,
+          uint32_t WPB = kTileThreads / 32>
 __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                const ColT* __restrict__ col, Sig* __restrict__ sig,
-                                               TileRange rng = TileRange{0u, 0u, nullptr, nullptr, 0ull})
+                                               TileRange rng = TileRange{0u, 0u, nullptr, nullptr, 0ull},
+                                               const uint32_t* __restrict__ hot_idx = nullptr,
+                                               const uint8_t* __restrict__ s_hot = nullptr)
 {
+    static_assert(!HOT || (sizeof(ColT) == 1 && !RANGE), "hot heads: resident arcs, 1-byte ranks");
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t ntiles = RANGE ? rng.hi : as->ntiles;
     const uint64_t m = as->m;
@@ -397,13 +418,13 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
     const uint32_t* __restrict__ tile_row = as->tile_row;
     const uint8_t* __restrict__ head8 = as->head8;
     // RANGE: idx[e - base] / wt[e - base] hold arc e of the chunk
-    const uint32_t* __restrict__ idx = RANGE ? rng.idx : as->idx;
+    const uint32_t* __restrict__ idx = HOT ? hot_idx : (RANGE ? rng.idx : as->idx);
     const uint64_t* __restrict__ wt = RANGE ? rng.wt : as->wt;
     const uint64_t ebase = RANGE ? rng.base : 0ull;
     const uint64_t salt = pass_salt1(st->seed, st->round);
-    const uint32_t warps = gridDim.x * (kTileThreads / 32);
+    const uint32_t warps = gridDim.x * WPB;
 
-    for (uint32_t tile = (RANGE ? rng.lo : 0u) + blockIdx.x * (kTileThreads / 32) + (threadIdx.x >> 5); tile < ntiles;
+    for (uint32_t tile = (RANGE ? rng.lo : 0u) + blockIdx.x * WPB + (threadIdx.x >> 5); tile < ntiles;
          tile += warps) {
         const uint64_t tbeg = (uint64_t)tile * kTileEdges;
         const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
@@ -421,18 +442,19 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
             hb = *reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3));
             const uint4* p = reinterpret_cast<const uint4*>(idx + (tbeg - ebase) + a);
             const uint4 q0 = __ldcs(p), q1 = __ldcs(p + 1), q2 = __ldcs(p + 2), q3 = __ldcs(p + 3);
-            c[0] = gather_col<NC>(col + q0.x); c[1] = gather_col<NC>(col + q0.y);
-            c[2] = gather_col<NC>(col + q0.z); c[3] = gather_col<NC>(col + q0.w);
-            c[4] = gather_col<NC>(col + q1.x); c[5] = gather_col<NC>(col + q1.y);
-            c[6] = gather_col<NC>(col + q1.z); c[7] = gather_col<NC>(col + q1.w);
-            c[8] = gather_col<NC>(col + q2.x); c[9] = gather_col<NC>(col + q2.y);
-            c[10] = gather_col<NC>(col + q2.z); c[11] = gather_col<NC>(col + q2.w);
-            c[12] = gather_col<NC>(col + q3.x); c[13] = gather_col<NC>(col + q3.y);
-            c[14] = gather_col<NC>(col + q3.z); c[15] = gather_col<NC>(col + q3.w);
+            c[0] = gather_head<NC, ColT, HOT>(col, s_hot, q0.x); c[1] = gather_head<NC, ColT, HOT>(col, s_hot, q0.y);
+            c[2] = gather_head<NC, ColT, HOT>(col, s_hot, q0.z); c[3] = gather_head<NC, ColT, HOT>(col, s_hot, q0.w);
+            c[4] = gather_head<NC, ColT, HOT>(col, s_hot, q1.x); c[5] = gather_head<NC, ColT, HOT>(col, s_hot, q1.y);
+            c[6] = gather_head<NC, ColT, HOT>(col, s_hot, q1.z); c[7] = gather_head<NC, ColT, HOT>(col, s_hot, q1.w);
+            c[8] = gather_head<NC, ColT, HOT>(col, s_hot, q2.x); c[9] = gather_head<NC, ColT, HOT>(col, s_hot, q2.y);
+            c[10] = gather_head<NC, ColT, HOT>(col, s_hot, q2.z); c[11] = gather_head<NC, ColT, HOT>(col, s_hot, q2.w);
+            c[12] = gather_head<NC, ColT, HOT>(col, s_hot, q3.x); c[13] = gather_head<NC, ColT, HOT>(col, s_hot, q3.y);
+            c[14] = gather_head<NC, ColT, HOT>(col, s_hot, q3.z); c[15] = gather_head<NC, ColT, HOT>(col, s_hot, q3.w);
         } else {
             if (cnt) hb = (uint32_t)(*reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3))) & ((1u << cnt) - 1u);
 #pragma unroll
-            for (int i = 0; i < kEdgesPerThread; ++i) c[i] = (uint32_t)i < cnt ? gather_col<NC>(col + __ldcs(idx + (tbeg - ebase) + a + i)) : 0u;
+            for (int i = 0; i < kEdgesPerThread; ++i)
+                c[i] = (uint32_t)i < cnt ? gather_head<NC, ColT, HOT>(col, s_hot, __ldcs(idx + (tbeg - ebase) + a + i)) : 0u;
         }
         if (WEIGHTED) {
 #pragma unroll
