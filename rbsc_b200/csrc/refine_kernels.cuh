@@ -132,6 +132,7 @@ __device__ __forceinline__ void sig_load(const Sig* p, uint64_t& s1, uint32_t& s
 // Node-list flag: the node represents a group of arc-less nodes with the same
 // initial colour, so its block is never a singleton.
 constexpr uint32_t kRepFlag = 0x80000000u;
+constexpr int kListBuf = 2048;  // shared-memory buffer of the buffered list appends (BlockAppend)
 
 // Static pointers of the ping-pong compaction buffers.
 struct CompactBufs {
@@ -1158,9 +1159,11 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
 
 // Keeps the non-singleton entries of the node list (order is not kept: the
 // relabel does not depend on it); dropped nodes are singleton blocks for good.
+// Appends are buffered per block (one reservation per kListBuf kept nodes).
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                        const uint32_t* __restrict__ col, CompactBufs bufs)
 {
+    __shared__ BlockAppend<uint32_t, kListBuf, kNodeThreads> sa;
     __shared__ BlockReserveSmem<kNodeThreads> sm;
     if (st->done || st->error) return;
     const uint32_t nn = as->nnodes;
@@ -1168,21 +1171,29 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet
     uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
     const uint32_t stride = gridDim.x * kNodeThreads;
     uint32_t dropped = 0;
+    block_append_begin(sa);
     for (uint32_t base = blockIdx.x * kNodeThreads; base < nn; base += stride) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < nn;
         const uint32_t e = valid ? src[i] : 0u;
         const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
-        const uint32_t pos = block_reserve<kNodeThreads>(keep, &as->nodectr, sm);
-        if (keep) dst[pos] = e;
+        block_append(sa, keep, e, &as->nodectr, dst);
         dropped += (valid && !keep) ? 1u : 0u;
     }
+    block_append_flush(sa, &as->nodectr, dst);
     block_count<kNodeThreads>(dropped, &as->retired, sm);
 }
 
 // Counts and places the rows of non-singleton nodes of the current arc set in
-// the destination arc set.  One 64-bit atomic per block reserves (rows, arcs)
-// together, so row order and arc order agree in the destination.
+// the destination arc set.  Each thread takes kCompactRows rows per block
+// iteration; one 64-bit atomic per iteration reserves (rows, arcs) together
+// for the block, so row order and arc order agree in the destination (a
+// counter that every block hits once per 256 rows serialises in L2).  The
+// packed arcs are exact while the kept arcs stay below 2^32, which arcctr
+// (64-bit) tells k_compact_decide; beyond that the positions are unused,
+// and a row position past the current set's row count is not written.
+constexpr int kCompactRows = 8;
+
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
@@ -1196,33 +1207,40 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
     const uint64_t* __restrict__ roff64 = reinterpret_cast<const uint64_t*>(as->roff);
     const uint32_t* __restrict__ roff32 = reinterpret_cast<const uint32_t*>(as->roff);
     const uint32_t d = as->dst_arcs;
+    const uint64_t dst_cap = as->dst_cap;
     uint32_t* __restrict__ drows = bufs.rows[d];
     uint32_t* __restrict__ doff = bufs.off[d];
     uint64_t* __restrict__ dsrc = bufs.src[d];
     uint32_t* __restrict__ chunk_row = bufs.chunk_row[d];
-    const uint32_t stride = gridDim.x * kNodeThreads;
+    const uint64_t span = (uint64_t)kNodeThreads * kCompactRows;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (uint32_t base = blockIdx.x * kNodeThreads; base < K; base += stride) {
-        const uint32_t k = base + threadIdx.x;
-        uint32_t node = 0, deg = 0;
-        uint64_t start = 0;
-        bool keep = false;
-        if (k < K) {
-            node = rows[k];
-            keep = !(col[node] & kSingleton);
-            if (keep) {
-                const uint64_t b = r64 ? roff64[k] : roff32[k];
-                const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
-                start = b;
-                deg = (uint32_t)(e - b);
+    for (uint64_t base = (uint64_t)blockIdx.x * span; base < K; base += (uint64_t)gridDim.x * span) {
+        // every row of an arc set has at least one arc: deg 0 = not kept
+        uint32_t node[kCompactRows], deg[kCompactRows];
+        uint64_t start[kCompactRows];
+        uint32_t nrows = 0;
+        uint64_t narcs = 0;
+#pragma unroll
+        for (int j = 0; j < kCompactRows; ++j) {
+            const uint64_t k = base + (uint64_t)j * kNodeThreads + threadIdx.x;
+            node[j] = 0u;
+            deg[j] = 0u;
+            start[j] = 0ull;
+            if (k < K) {
+                node[j] = rows[k];
+                if (!(col[node[j]] & kSingleton)) {
+                    const uint64_t b = r64 ? roff64[k] : roff32[k];
+                    const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
+                    start[j] = b;
+                    deg[j] = (uint32_t)(e - b);
+                    nrows += 1u;
+                    narcs += e - b;
+                }
             }
         }
-        // per-thread (rows, arcs) packed: rows in the high half; the packed
-        // arcs are exact while the kept arcs stay below 2^32, which arcctr
-        // (64-bit) tells k_compact_decide
-        unsigned long long v = keep ? ((1ull << 32) | deg) : 0ull;
+        const unsigned long long v = ((unsigned long long)nrows << 32) + (uint32_t)narcs;
         unsigned long long incl = v;
-        unsigned long long arcs = deg;
+        unsigned long long arcs = narcs;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
@@ -1244,17 +1262,23 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
             if (run_arcs) atomicAdd(&as->arcctr, run_arcs);
         }
         __syncthreads();
-        if (keep) {
-            const unsigned long long pos = s_base + s_warp[warp] + incl - v;
-            const uint32_t kn = (uint32_t)(pos >> 32);
-            drows[kn] = node;
-            doff[kn] = (uint32_t)pos;
-            dsrc[kn] = start;
-            // the 16-arc destination chunks that start in this row (within the
-            // buffers: past the capacity nothing is copied anyway)
-            const uint32_t p0 = (uint32_t)pos;
-            if (deg && (uint64_t)p0 + deg <= as->dst_cap)
-                for (uint32_t c = (p0 + 15u) >> 4; (c << 4) < p0 + deg; ++c) chunk_row[c] = kn;
+        unsigned long long pos = s_base + s_warp[warp] + incl - v;
+#pragma unroll
+        for (int j = 0; j < kCompactRows; ++j) {
+            if (deg[j]) {
+                const uint32_t kn = (uint32_t)(pos >> 32);
+                const uint32_t p0 = (uint32_t)pos;
+                if (kn < K) {
+                    drows[kn] = node[j];
+                    doff[kn] = p0;
+                    dsrc[kn] = start[j];
+                    // the 16-arc destination chunks that start in this row
+                    // (within the buffers: past the capacity nothing is copied)
+                    if ((uint64_t)p0 + deg[j] <= dst_cap)
+                        for (uint32_t c = (p0 + 15u) >> 4; (c << 4) < p0 + deg[j]; ++c) chunk_row[c] = kn;
+                }
+                pos += (1ull << 32) + deg[j];
+            }
         }
         __syncthreads();
     }
@@ -1307,25 +1331,50 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet*
     const uint32_t* __restrict__ chunk_row = bufs.chunk_row[d];
     for (uint32_t ch = blockIdx.x * kNodeThreads + threadIdx.x; ch < chunks; ch += stride) {
         const uint32_t e0 = ch * 16u;
-        // row holding arc e0 (recorded by k_compact_rows)
+        const uint32_t cnt = min(16u, nm - e0);
+        // row holding arc e0 (recorded by k_compact_rows); the row walk finds
+        // each arc's source position first, so the 16 source loads below are
+        // independent of one another
         const uint32_t k0 = chunk_row[ch];
         uint32_t k = k0;
         uint32_t rb = doff[k], re = doff[k + 1];
         uint64_t src = dsrc[k];
         uint32_t bits = 0;
+        uint64_t from[16];
+#pragma unroll
         for (uint32_t i = 0; i < 16u; ++i) {
             const uint32_t e = e0 + i;
-            if (e >= nm) break;
-            while (e >= re) {
-                ++k;
-                rb = re;
-                re = doff[k + 1];
-                src = dsrc[k];
+            from[i] = 0ull;
+            if (i < cnt) {
+                while (e >= re) {
+                    ++k;
+                    rb = re;
+                    re = doff[k + 1];
+                    src = dsrc[k];
+                }
+                if (e == rb) bits |= 1u << i;
+                from[i] = src + (e - rb);
             }
-            if (e == rb) bits |= 1u << i;
-            if (COPY) {
-                didx[e] = sidx[src + (e - rb)];
-                if (swt) dwt[e] = swt[src + (e - rb)];
+        }
+        if (COPY) {
+            uint32_t h[16];
+#pragma unroll
+            for (uint32_t i = 0; i < 16u; ++i) h[i] = i < cnt ? sidx[from[i]] : 0u;
+            if (cnt == 16u) {
+                uint4* q = reinterpret_cast<uint4*>(didx + e0);
+                q[0] = make_uint4(h[0], h[1], h[2], h[3]);
+                q[1] = make_uint4(h[4], h[5], h[6], h[7]);
+                q[2] = make_uint4(h[8], h[9], h[10], h[11]);
+                q[3] = make_uint4(h[12], h[13], h[14], h[15]);
+            } else {
+#pragma unroll
+                for (uint32_t i = 0; i < 16u; ++i)
+                    if (i < cnt) didx[e0 + i] = h[i];
+            }
+            if (swt) {
+#pragma unroll
+                for (uint32_t i = 0; i < 16u; ++i)
+                    if (i < cnt) dwt[e0 + i] = swt[from[i]];
             }
         }
         *reinterpret_cast<uint16_t*>(bufs.head8[d] + (e0 >> 3)) = (uint16_t)bits;
@@ -1518,7 +1567,6 @@ static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uin
 // Node list = non-singleton nodes that are not followers (representatives
 // flagged); follower pairs; singleton count.  Grid-stride, both lists written
 // through shared-memory buffers (few reservations on the two counters).
-constexpr int kListBuf = 2048;
 struct BuildListsSmem {
     BlockAppend<uint32_t, kListBuf, kNodeThreads> nodes;
     BlockAppend<uint2, kListBuf, kNodeThreads> pairs;
