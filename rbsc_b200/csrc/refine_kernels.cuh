@@ -753,6 +753,7 @@ __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
 // Slot of a listed node that keeps its block's label: the block's
 // representative r (its smallest node), or a node whose signature equals r's.
 constexpr uint32_t kRepSlot = 0xffffffffu;
+constexpr int kInsertU = 1;  // list entries per thread and iteration of the hashed insert (2 measured slower)
 
 // Hashed pass over the node list (grid-stride by blocks); returns this
 // thread's count of new blocks.
@@ -781,50 +782,69 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
     // a late pass with few active nodes stays in L2
     const uint32_t log2win = table_window(nn, log2size);
     const uint32_t tag = st->round + 1u;
+    const uint32_t lane = threadIdx.x & 31;
     uint32_t made = 0;
-    for (uint32_t base = blockIdx.x * kNodeThreads + (threadIdx.x & ~31u); base < nn; base += stride) {
-        const uint32_t i = base + (threadIdx.x & 31);
-        const bool active = i < nn;
-        const uint32_t e = active ? nodes[i] : 0u;
-        const uint32_t u = e & ~kRepFlag;
-        const uint32_t c = active ? col[u] : kSingleton;
-        bool need = active && !(c & kSingleton);
-        bool is_rep = false;
-        uint64_t k1 = 0;
-        uint32_t k2 = stamp;
-        if (need) {
-            const uint32_t lab = c & kLabelMask;
-            uint64_t s1;
-            uint32_t s2;
-            sig_load(&sig[u], s1, s2);
-            if (hb) {  // test hook: truncated (or, from 64 bits on, no) signatures
-                s1 = (hb >= 64) ? 0ull : (s1 & ((1ull << hb) - 1ull));
-                s2 = 0;
-            }
-            bool keep = u == lab;
-            is_rep = keep;
-            if (!keep) {
-                uint64_t r1;
-                uint32_t r2;
-                sig_load(&sig[lab], r1, r2);
-                if (hb) {
-                    r1 = (hb >= 64) ? 0ull : (r1 & ((1ull << hb) - 1ull));
-                    r2 = 0;
-                }
-                keep = r1 == s1 && r2 == s2;
-                if (keep && joined[lab] != tag) joined[lab] = tag;
-            }
-            if (keep) {
-                slot[i] = kRepSlot;
-                need = false;
-            } else {
-                k1 = s1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
-                k2 = ((s2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
+    // each warp takes kInsertU x 32 consecutive list entries per iteration and
+    // issues their loads (colour, then both signatures) side by side, so the
+    // dependent chains of kInsertU nodes per thread overlap
+    for (uint32_t base = (blockIdx.x * kNodeThreads + (threadIdx.x & ~31u)) * kInsertU; base < nn; base += stride * kInsertU) {
+        uint32_t idx[kInsertU], e[kInsertU], u[kInsertU], c[kInsertU];
+        uint64_t s1[kInsertU], r1[kInsertU];
+        uint32_t s2[kInsertU], r2[kInsertU];
+#pragma unroll
+        for (int j = 0; j < kInsertU; ++j) {
+            idx[j] = base + 32u * j + lane;
+            e[j] = idx[j] < nn ? nodes[idx[j]] : 0u;
+            u[j] = e[j] & ~kRepFlag;
+        }
+#pragma unroll
+        for (int j = 0; j < kInsertU; ++j) c[j] = idx[j] < nn ? col[u[j]] : kSingleton;
+#pragma unroll
+        for (int j = 0; j < kInsertU; ++j) {
+            s1[j] = r1[j] = 0ull;
+            s2[j] = r2[j] = 0u;
+            if (!(c[j] & kSingleton)) {
+                const uint32_t lab = c[j] & kLabelMask;
+                sig_load(&sig[u[j]], s1[j], s2[j]);
+                if (u[j] != lab) sig_load(&sig[lab], r1[j], r2[j]);
             }
         }
-        bool nb = (active && !need && !(active && !(c & kSingleton) && !is_rep)) || is_rep;
-        insert_warp(need, u, i, (e & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
-        made += nb ? 1u : 0u;
+#pragma unroll
+        for (int j = 0; j < kInsertU; ++j) {
+            const bool active = idx[j] < nn;
+            bool need = active && !(c[j] & kSingleton);
+            bool is_rep = false;
+            uint64_t k1 = 0;
+            uint32_t k2 = stamp;
+            if (need) {
+                const uint32_t lab = c[j] & kLabelMask;
+                uint64_t a1 = s1[j], b1 = r1[j];
+                uint32_t a2 = s2[j], b2 = r2[j];
+                if (hb) {  // test hook: truncated (or, from 64 bits on, no) signatures
+                    a1 = (hb >= 64) ? 0ull : (a1 & ((1ull << hb) - 1ull));
+                    b1 = (hb >= 64) ? 0ull : (b1 & ((1ull << hb) - 1ull));
+                    a2 = b2 = 0;
+                }
+                bool keep = u[j] == lab;
+                is_rep = keep;
+                if (!keep) {
+                    keep = b1 == a1 && b2 == a2;
+                    if (keep && joined[lab] != tag) joined[lab] = tag;
+                }
+                if (keep) {
+                    slot[idx[j]] = kRepSlot;
+                    need = false;
+                } else {
+                    k1 = a1 ^ fmix64(((uint64_t)lab << 1 | 1ull) * kGolden ^ seed);
+                    k2 = ((a2 ^ fmix32(lab * 0x9e3779b1u + (uint32_t)seed)) & 0xffffff00u) | stamp;
+                }
+            }
+            // a singleton or a representative stands for a block of its own
+            // so far; the others count only when they open a class
+            bool nb = (active && (c[j] & kSingleton)) || is_rep;
+            insert_warp(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
+            made += nb ? 1u : 0u;
+        }
     }
     return made;
 }
@@ -1719,7 +1739,7 @@ struct PersistArgs {
     uint32_t* joined;
 };
 
-static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
+static __global__ void __launch_bounds__(kNodeThreads, 4) k_refine_persistent(PersistArgs a)
 {
     static_assert(kNodeThreads == kTileThreads, "the signature phase runs one tile per warp");
     __shared__ BlockReserveSmem<kNodeThreads> sm;
