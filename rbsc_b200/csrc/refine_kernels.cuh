@@ -1205,20 +1205,24 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet
 }
 
 // Counts and places the rows of non-singleton nodes of the current arc set in
-// the destination arc set.  Each thread takes kCompactRows rows per block
-// iteration; one 64-bit atomic per iteration reserves (rows, arcs) together
-// for the block, so row order and arc order agree in the destination (a
-// counter that every block hits once per 256 rows serialises in L2).  The
-// packed arcs are exact while the kept arcs stay below 2^32, which arcctr
-// (64-bit) tells k_compact_decide; beyond that the positions are unused,
-// and a row position past the current set's row count is not written.
+// the destination arc set.  A block iteration takes kCompactRows x 256
+// consecutive rows (row base + j*256 + thread, so every load is coalesced);
+// one 64-bit atomic per iteration reserves (rows, arcs) together for the
+// block, so row order and arc order agree in the destination (a counter that
+// every block hits once per 256 rows serialises in L2).  Positions inside the
+// iteration follow the source order (j, then warp, then lane), so the kept
+// rows of one warp and item are written side by side.  The packed arcs are
+// exact while the kept arcs stay below 2^32, which arcctr (64-bit) tells
+// k_compact_decide; beyond that the positions are unused, and a row position
+// past the current set's row count is not written.
 constexpr int kCompactRows = 8;
 
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
-    __shared__ unsigned long long s_warp[kNodeThreads / 32];
-    __shared__ unsigned long long s_warp_arcs[kNodeThreads / 32];
+    constexpr int W = kNodeThreads / 32;
+    __shared__ unsigned long long s_pre[kCompactRows][W];  // per (item, warp): packed total, then its exclusive offset
+    __shared__ unsigned long long s_arcs[W];
     __shared__ unsigned long long s_base;
     if (st->done || st->error || !as->compact_arcs) return;
     const uint32_t K = as->K;
@@ -1238,66 +1242,70 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet*
         // every row of an arc set has at least one arc: deg 0 = not kept
         uint32_t node[kCompactRows], deg[kCompactRows];
         uint64_t start[kCompactRows];
-        uint32_t nrows = 0;
-        uint64_t narcs = 0;
+        unsigned long long incl[kCompactRows];
 #pragma unroll
         for (int j = 0; j < kCompactRows; ++j) {
             const uint64_t k = base + (uint64_t)j * kNodeThreads + threadIdx.x;
             node[j] = 0u;
             deg[j] = 0u;
             start[j] = 0ull;
-            if (k < K) {
-                node[j] = rows[k];
-                if (!(col[node[j]] & kSingleton)) {
-                    const uint64_t b = r64 ? roff64[k] : roff32[k];
-                    const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
-                    start[j] = b;
-                    deg[j] = (uint32_t)(e - b);
-                    nrows += 1u;
-                    narcs += e - b;
-                }
+            if (k < K) node[j] = rows[k];
+        }
+#pragma unroll
+        for (int j = 0; j < kCompactRows; ++j) {
+            const uint64_t k = base + (uint64_t)j * kNodeThreads + threadIdx.x;
+            if (k < K && !(col[node[j]] & kSingleton)) {
+                const uint64_t b = r64 ? roff64[k] : roff32[k];
+                const uint64_t e = r64 ? roff64[k + 1] : roff32[k + 1];
+                start[j] = b;
+                deg[j] = (uint32_t)(e - b);
             }
         }
-        const unsigned long long v = ((unsigned long long)nrows << 32) + (uint32_t)narcs;
-        unsigned long long incl = v;
-        unsigned long long arcs = narcs;
+        unsigned long long arcs = 0;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const unsigned long long t = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += t;
-            arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+        for (int j = 0; j < kCompactRows; ++j) {
+            const unsigned long long v = deg[j] ? ((1ull << 32) | deg[j]) : 0ull;
+            unsigned long long x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const unsigned long long t = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += t;
+            }
+            incl[j] = x;
+            if (lane == 31) s_pre[j][warp] = x;
+            arcs += deg[j];
         }
-        if (lane == 31) s_warp[warp] = incl;
-        if (lane == 0) s_warp_arcs[warp] = arcs;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) arcs += __shfl_xor_sync(0xffffffffu, arcs, o);
+        if (lane == 0) s_arcs[warp] = arcs;
         __syncthreads();
         if (threadIdx.x == 0) {
             unsigned long long run = 0, run_arcs = 0;
-            for (int w = 0; w < kNodeThreads / 32; ++w) {
-                const unsigned long long c = s_warp[w];
-                s_warp[w] = run;
-                run += c;
-                run_arcs += s_warp_arcs[w];
-            }
+            for (int j = 0; j < kCompactRows; ++j)
+                for (int w = 0; w < W; ++w) {
+                    const unsigned long long c = s_pre[j][w];
+                    s_pre[j][w] = run;
+                    run += c;
+                }
+            for (int w = 0; w < W; ++w) run_arcs += s_arcs[w];
             s_base = run ? atomicAdd(&as->rowctr, run) : 0ull;
             if (run_arcs) atomicAdd(&as->arcctr, run_arcs);
         }
         __syncthreads();
-        unsigned long long pos = s_base + s_warp[warp] + incl - v;
 #pragma unroll
         for (int j = 0; j < kCompactRows; ++j) {
-            if (deg[j]) {
-                const uint32_t kn = (uint32_t)(pos >> 32);
-                const uint32_t p0 = (uint32_t)pos;
-                if (kn < K) {
-                    drows[kn] = node[j];
-                    doff[kn] = p0;
-                    dsrc[kn] = start[j];
-                    // the 16-arc destination chunks that start in this row
-                    // (within the buffers: past the capacity nothing is copied)
-                    if ((uint64_t)p0 + deg[j] <= dst_cap)
-                        for (uint32_t c = (p0 + 15u) >> 4; (c << 4) < p0 + deg[j]; ++c) chunk_row[c] = kn;
-                }
-                pos += (1ull << 32) + deg[j];
+            if (!deg[j]) continue;
+            const unsigned long long pos = s_base + s_pre[j][warp] + incl[j] - ((1ull << 32) | deg[j]);
+            const uint32_t kn = (uint32_t)(pos >> 32);
+            const uint32_t p0 = (uint32_t)pos;
+            if (kn < K) {
+                drows[kn] = node[j];
+                doff[kn] = p0;
+                dsrc[kn] = start[j];
+                // the 16-arc destination chunks that start in this row
+                // (within the buffers: past the capacity nothing is copied)
+                if ((uint64_t)p0 + deg[j] <= dst_cap)
+                    for (uint32_t c = (p0 + 15u) >> 4; (c << 4) < p0 + deg[j]; ++c) chunk_row[c] = kn;
             }
         }
         __syncthreads();
@@ -1739,7 +1747,7 @@ struct PersistArgs {
     uint32_t* joined;
 };
 
-static __global__ void __launch_bounds__(kNodeThreads, 4) k_refine_persistent(PersistArgs a)
+static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
 {
     static_assert(kNodeThreads == kTileThreads, "the signature phase runs one tile per warp");
     __shared__ BlockReserveSmem<kNodeThreads> sm;
