@@ -37,6 +37,7 @@
  * colours.  rsc.cpp:104-144 starts its count at N instead; orc_refine_rsc
  * reports both.
  */
+#include <pthread.h>
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -333,11 +334,274 @@ int orc_refine_rsc(uint32_t n, const uint64_t* off, const uint32_t* idx, const u
      * confirm it */
     if (!gpu_done) *rounds_gpu = (uint32_t)it + 1;
     *rounds_cpu = (uint32_t)it;
+    if (it == 0)  /* no pass ran: the initial colours */
+        for (uint32_t u = 0; u < n; ++u) lab[u] = (uint32_t)w[u];
     *blocks_out = orc_canonicalize(n, lab, labels_out);
     free(w); free(z); free(ord); free(tmp); free(lab);
     return status;
 }
 
+
+/* ------------------------------------------------------------------ */
+/* rsc.cpp:71-144 restated again, multi-threaded (pthreads), u64        */
+/* counters throughout: the same arithmetic and the same dense ranks    */
+/* as orc_refine_rsc, for graphs whose arcs do not fit in 32 bits       */
+/* (R-MAT-28: 8.5 G arcs) and a single thread would take too long.      */
+/*                                                                      */
+/* Dense ranks in (z, w) order without one global sort: every node goes */
+/* to a bucket by a key that is monotone in (z, w) -- z = 0 by the      */
+/* range of w, z != 0 by the top bits of z -- buckets are sorted in     */
+/* parallel, and a bucket's ranks start after all earlier buckets'.     */
+/* ------------------------------------------------------------------ */
+#define ORC_WBUCKETS 1024u
+#define ORC_ZBITS 12u
+#define ORC_BUCKETS (ORC_WBUCKETS + (1u << ORC_ZBITS))
+
+typedef struct {
+    uint32_t n, threads;
+    const uint64_t* off;
+    const uint32_t* idx;
+    const uint64_t* wt;
+    uint64_t* w;
+    uint64_t* z;
+    uint32_t* ord;
+    uint32_t* tmp;
+    uint32_t* lab;
+    uint64_t it, wmax;
+    uint64_t* cnt;        /* [threads][ORC_BUCKETS]: counts, then scatter cursors */
+    uint64_t* bstart;     /* [ORC_BUCKETS + 1] */
+    uint64_t* bdist;      /* [ORC_BUCKETS]: distinct pairs, then the bucket's first rank */
+    uint32_t* sig_lo;     /* [threads + 1]: signature ranges with equal arc counts */
+    uint32_t next;        /* bucket work counter */
+} mt_ctx;
+
+typedef struct {
+    mt_ctx* c;
+    uint32_t t;
+} mt_arg;
+
+static uint32_t mt_bucket(const mt_ctx* c, uint32_t u)
+{
+    if (c->z[u] == 0) return (uint32_t)((c->w[u] * (uint64_t)ORC_WBUCKETS) / (c->wmax + 1u));
+    return ORC_WBUCKETS + (uint32_t)(c->z[u] >> (64u - ORC_ZBITS));
+}
+
+static void mt_range(const mt_ctx* c, uint32_t t, uint32_t* lo, uint32_t* hi)
+{
+    *lo = (uint32_t)((uint64_t)c->n * t / c->threads);
+    *hi = (uint32_t)((uint64_t)c->n * (t + 1) / c->threads);
+}
+
+static void* mt_signatures(void* p)
+{
+    const mt_arg* a = (const mt_arg*)p;
+    const mt_ctx* c = a->c;
+    for (uint32_t u = c->sig_lo[a->t]; u < c->sig_lo[a->t + 1]; ++u) {
+        if (c->off[u] == c->off[u + 1]) continue; /* z stays as it was */
+        uint64_t s = 0;
+        for (uint64_t k = c->off[u]; k < c->off[u + 1]; ++k)
+            s += orc_rsc_randomize(c->w[c->idx[k]] + c->it) * (c->wt ? c->wt[k] : 1u);
+        c->z[u] = s;
+    }
+    return NULL;
+}
+
+static void* mt_count(void* p)
+{
+    const mt_arg* a = (const mt_arg*)p;
+    const mt_ctx* c = a->c;
+    uint64_t* cnt = c->cnt + (size_t)a->t * ORC_BUCKETS;
+    uint32_t lo, hi;
+    mt_range(c, a->t, &lo, &hi);
+    memset(cnt, 0, sizeof(uint64_t) * ORC_BUCKETS);
+    for (uint32_t u = lo; u < hi; ++u) ++cnt[mt_bucket(c, u)];
+    return NULL;
+}
+
+static void* mt_scatter(void* p)
+{
+    const mt_arg* a = (const mt_arg*)p;
+    const mt_ctx* c = a->c;
+    uint64_t* cur = c->cnt + (size_t)a->t * ORC_BUCKETS;
+    uint32_t lo, hi;
+    mt_range(c, a->t, &lo, &hi);
+    for (uint32_t u = lo; u < hi; ++u) c->ord[cur[mt_bucket(c, u)]++] = u;
+    return NULL;
+}
+
+static void* mt_sort_buckets(void* p)
+{
+    mt_ctx* c = ((const mt_arg*)p)->c;
+    const rsc_ctx rc = { c->z, c->w };
+    for (;;) {
+        const uint32_t b = __atomic_fetch_add(&c->next, 1u, __ATOMIC_RELAXED);
+        if (b >= ORC_BUCKETS) break;
+        const uint64_t s = c->bstart[b], e = c->bstart[b + 1];
+        if (s == e) {
+            c->bdist[b] = 0;
+            continue;
+        }
+        msort_idx(c->ord + s, c->tmp + s, (size_t)(e - s), cmp_rsc, &rc);
+        uint64_t r = 0;
+        for (uint64_t i = s; i < e; ++i) {
+            if (i > s && cmp_rsc(c->ord[i - 1], c->ord[i], &rc) != 0) ++r;
+            c->lab[c->ord[i]] = (uint32_t)r;
+        }
+        c->bdist[b] = r + 1;
+    }
+    return NULL;
+}
+
+static void* mt_apply(void* p)
+{
+    mt_ctx* c = ((const mt_arg*)p)->c;
+    for (;;) {
+        const uint32_t b = __atomic_fetch_add(&c->next, 1u, __ATOMIC_RELAXED);
+        if (b >= ORC_BUCKETS) break;
+        for (uint64_t i = c->bstart[b]; i < c->bstart[b + 1]; ++i) {
+            const uint32_t v = c->ord[i];
+            c->lab[v] += (uint32_t)c->bdist[b];
+            c->w[v] = c->lab[v];
+        }
+    }
+    return NULL;
+}
+
+/* Runs fn for every thread index; a thread that cannot be created runs
+ * inline. */
+static void mt_run(mt_ctx* c, void* (*fn)(void*))
+{
+    pthread_t th[256];
+    mt_arg args[256];
+    int made[256];
+    for (uint32_t t = 0; t < c->threads; ++t) {
+        args[t].c = c;
+        args[t].t = t;
+        made[t] = pthread_create(&th[t], NULL, fn, &args[t]) == 0;
+        if (!made[t]) fn(&args[t]);
+    }
+    for (uint32_t t = 0; t < c->threads; ++t)
+        if (made[t]) pthread_join(th[t], NULL);
+}
+
+/* Same contract and results as orc_refine_rsc (labels, rounds in both
+ * conventions, blocks); threads in 1..256.  Returns -1 when max_rounds ran
+ * out, -2 when memory is short. */
+int orc_refine_rsc_mt(uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt,
+                      const uint32_t* init, uint32_t* labels_out, uint32_t* rounds_gpu,
+                      uint32_t* rounds_cpu, uint32_t* blocks_out, uint32_t max_rounds, uint32_t threads)
+{
+    *rounds_gpu = *rounds_cpu = *blocks_out = 0;
+    if (n == 0) return 0;
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    mt_ctx c;
+    memset(&c, 0, sizeof c);
+    c.n = n;
+    c.threads = threads;
+    c.off = off;
+    c.idx = idx;
+    c.wt = wt;
+    c.w = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    c.z = (uint64_t*)calloc(n, sizeof(uint64_t));
+    c.ord = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    c.tmp = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    c.lab = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    c.cnt = (uint64_t*)malloc(sizeof(uint64_t) * ORC_BUCKETS * threads);
+    c.bstart = (uint64_t*)malloc(sizeof(uint64_t) * (ORC_BUCKETS + 1));
+    c.bdist = (uint64_t*)malloc(sizeof(uint64_t) * ORC_BUCKETS);
+    c.sig_lo = (uint32_t*)malloc(sizeof(uint32_t) * (threads + 1));
+    int status = -1;
+    if (!c.w || !c.z || !c.ord || !c.tmp || !c.lab || !c.cnt || !c.bstart || !c.bdist || !c.sig_lo) {
+        status = -2;
+        goto out;
+    }
+    /* signature ranges: equal shares of the arcs (first node whose offset
+     * reaches t * m / threads) */
+    {
+        const uint64_t m = off[n];
+        uint32_t u = 0;
+        for (uint32_t t = 0; t <= threads; ++t) {
+            const uint64_t target = t == threads ? m + 1 : m / threads * t;
+            while (u < n && off[u] < target) ++u;
+            c.sig_lo[t] = t == threads ? n : u;
+        }
+        c.sig_lo[0] = 0;
+    }
+    uint32_t count0 = 1;
+    if (init) {
+        /* dense rank of the initial colour, in increasing colour order */
+        for (uint32_t i = 0; i < n; ++i) c.ord[i] = i;
+        const uint32_t* ic = init;
+        msort_idx(c.ord, c.tmp, n, cmp_lab, &ic);
+        uint64_t rank = 1;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i && init[c.ord[i]] != init[c.ord[i - 1]]) ++rank;
+            c.w[c.ord[i]] = rank;
+        }
+        count0 = (uint32_t)rank;
+        c.wmax = rank;
+    } else {
+        for (uint32_t i = 0; i < n; ++i) c.w[i] = 1;
+        c.wmax = 1;
+    }
+    uint32_t prev_cpu = n, prev_gpu = count0, count = count0;
+    int gpu_done = 0;
+    while (c.it < max_rounds) {
+        mt_run(&c, mt_signatures);
+        mt_run(&c, mt_count);
+        uint64_t pos = 0;
+        for (uint32_t b = 0; b < ORC_BUCKETS; ++b) {
+            c.bstart[b] = pos;
+            for (uint32_t t = 0; t < threads; ++t) {
+                const uint64_t k = c.cnt[(size_t)t * ORC_BUCKETS + b];
+                c.cnt[(size_t)t * ORC_BUCKETS + b] = pos;
+                pos += k;
+            }
+        }
+        c.bstart[ORC_BUCKETS] = pos;
+        mt_run(&c, mt_scatter);
+        c.next = 0;
+        mt_run(&c, mt_sort_buckets);
+        uint64_t total = 0;
+        for (uint32_t b = 0; b < ORC_BUCKETS; ++b) {
+            const uint64_t d = c.bdist[b];
+            c.bdist[b] = total;
+            total += d;
+        }
+        c.next = 0;
+        mt_run(&c, mt_apply);
+        count = (uint32_t)total;
+        c.wmax = total ? total - 1 : 0;
+        ++c.it;
+        if (!gpu_done) {
+            if (count == prev_gpu) { *rounds_gpu = (uint32_t)c.it; gpu_done = 1; }
+            prev_gpu = count;
+        }
+        if (count == prev_cpu) { status = 0; break; }
+        prev_cpu = count;
+    }
+    if (!gpu_done) *rounds_gpu = (uint32_t)c.it + 1;
+    *rounds_cpu = (uint32_t)c.it;
+    /* the ranks are dense (0..count-1): canonical label = first node of
+     * each rank, in one pass (c.tmp holds first[rank]) */
+    if (c.it == 0) {  /* no pass ran: the initial colours */
+        for (uint32_t u = 0; u < n; ++u) c.lab[u] = (uint32_t)c.w[u];
+        *blocks_out = orc_canonicalize(n, c.lab, labels_out);
+    } else {
+        for (uint32_t r = 0; r < count; ++r) c.tmp[r] = UINT32_MAX;
+        for (uint32_t u = 0; u < n; ++u) {
+            const uint32_t r = c.lab[u];
+            if (c.tmp[r] == UINT32_MAX) c.tmp[r] = u;
+            labels_out[u] = c.tmp[r];
+        }
+        *blocks_out = count;
+    }
+out:
+    free(c.w); free(c.z); free(c.ord); free(c.tmp); free(c.lab);
+    free(c.cnt); free(c.bstart); free(c.bdist); free(c.sig_lo);
+    return status;
+}
 
 /* batches = ceil((double)edge_n / max_batch_edge_n) (rbsc.cu:295) */
 static double ceil_u64_div_double(uint64_t a, uint64_t b)

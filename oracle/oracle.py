@@ -87,6 +87,9 @@ def _load():
         lib.orc_refine_rsc.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p, _u32p,
                                        _u32p, _u32p, _u32p, ctypes.c_uint32]
         lib.orc_refine_rsc.restype = ctypes.c_int
+        lib.orc_refine_rsc_mt.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p, _u32p,
+                                          _u32p, _u32p, _u32p, ctypes.c_uint32, ctypes.c_uint32]
+        lib.orc_refine_rsc_mt.restype = ctypes.c_int
         lib.orc_canonicalize.argtypes = [ctypes.c_uint32, _u32p, _u32p]
         lib.orc_canonicalize.restype = ctypes.c_uint32
         lib.orc_rsc_randomize.argtypes = [ctypes.c_uint64]
@@ -168,18 +171,24 @@ def refine_edge_batches(off, idx, wt=None, batch: int = 0, aggressive: bool = Fa
     return EdgeBatchResult(labels[:n].copy(), bl.value, dn.value, it.value)
 
 
-def refine_rsc(off, idx, wt=None, init=None, max_rounds: int | None = None) -> OracleResult:
-    """The reference CPU loop restated (oracle.c: orc_refine_rsc)."""
+def refine_rsc(off, idx, wt=None, init=None, max_rounds: int | None = None, threads: int | None = None) -> OracleResult:
+    """The reference CPU loop restated (oracle.c: orc_refine_rsc); with
+    `threads`, the multi-threaded restatement (orc_refine_rsc_mt: the same
+    ranks and results, for graphs of billions of arcs)."""
     lib = _load()
     n = len(off) - 1
     off, idx, wt = _csr(off, idx, wt)
     init = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
     if max_rounds is None:
-        max_rounds = n + 2
+        max_rounds = min(n + 2, 0xFFFFFFFF)
     labels = np.zeros(max(n, 1), dtype=np.uint32)
     rg, rc, bl = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
-    st = lib.orc_refine_rsc(n, _p64(off), _p32(idx), _p64(wt), _p32(init), _p32(labels),
-                            ctypes.byref(rg), ctypes.byref(rc), ctypes.byref(bl), max_rounds)
+    if threads:
+        st = lib.orc_refine_rsc_mt(n, _p64(off), _p32(idx), _p64(wt), _p32(init), _p32(labels),
+                                   ctypes.byref(rg), ctypes.byref(rc), ctypes.byref(bl), max_rounds, int(threads))
+    else:
+        st = lib.orc_refine_rsc(n, _p64(off), _p32(idx), _p64(wt), _p32(init), _p32(labels),
+                                ctypes.byref(rg), ctypes.byref(rc), ctypes.byref(bl), max_rounds)
     return OracleResult(labels[:n].copy(), bl.value, rg.value, rc.value, None, st)
 
 

@@ -58,3 +58,36 @@ def test_valmari_with_initial_blocks():
 def test_empty_graph():
     r = oracle.refine_exact(np.zeros(1, dtype=np.uint64), np.zeros(0, dtype=np.uint32))
     assert r.blocks == 0 and r.rounds == 0
+
+
+def _mt_cases():
+    import rbsc_b200 as R
+    yield "er", *G.er_directed(300, 1200, seed=11), None, None
+    off, idx = G.rmat(13, 8, seed=12)
+    yield "rmat13_degree_colours", off, idx, None, R.degree_bucket_colors(off)
+    off, idx = G.random_lift(64, 256, 8, seed=13)
+    yield "lift_weighted", off, idx, np.random.default_rng(13).integers(1, 5, len(idx)).astype(np.uint64), None
+    off, idx = G.er_undirected(500, 3.0, seed=14)
+    yield "labels", off, idx, None, np.random.default_rng(14).integers(0, 6, 500).astype(np.uint32)
+    yield "isolated", np.zeros(11, dtype=np.uint64), np.zeros(0, dtype=np.uint32), None, None
+    yield "empty", np.zeros(1, dtype=np.uint64), np.zeros(0, dtype=np.uint32), None, None
+
+
+@pytest.mark.parametrize("threads", [1, 3, 8])
+@pytest.mark.parametrize("case", list(_mt_cases()), ids=lambda c: c[0])
+def test_multithreaded_rsc_restatement_is_the_same(case, threads):
+    """orc_refine_rsc_mt (for graphs of billions of arcs) gives the serial
+    restatement's labels, blocks, rounds in both conventions and status."""
+    _, off, idx, wt, init = case
+    a = oracle.refine_rsc(off, idx, wt, init)
+    b = oracle.refine_rsc(off, idx, wt, init, threads=threads)
+    assert np.array_equal(a.labels, b.labels)
+    assert (a.blocks, a.rounds, a.rounds_cpu, a.status) == (b.blocks, b.rounds, b.rounds_cpu, b.status)
+
+
+@pytest.mark.parametrize("max_rounds", [0, 1, 2])
+def test_multithreaded_rsc_restatement_stopped_early(max_rounds):
+    off, idx = G.rmat(10, 8, seed=15)
+    a = oracle.refine_rsc(off, idx, max_rounds=max_rounds)
+    b = oracle.refine_rsc(off, idx, max_rounds=max_rounds, threads=4)
+    assert np.array_equal(a.labels, b.labels) and a.blocks == b.blocks and a.status == b.status == -1
