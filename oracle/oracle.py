@@ -225,16 +225,27 @@ def arcs_cuda_text(off, idx, wt=None) -> bytes:
     return "".join(lines).encode()
 
 
-def mdp_text(off, idx, wt=None, init=None) -> bytes:
+def mdp_text(off, idx, wt=None, init=None, merge: bool = False) -> bytes:
     """Valmari MDP text (src/part_ref/MDP_read.cc:51-63), the conversion that
-    valmari-adapter:9-16 performs, extended with <blocks> for initial colours."""
+    valmari-adapter:9-16 performs, extended with <blocks> for initial colours.
+    merge: parallel arcs become one transition carrying their summed weight
+    (the same weight sum into every block, so the same lumping); the reader
+    refuses more transitions than states squared."""
     off = np.asarray(off, dtype=np.uint64)
     idx = np.asarray(idx, dtype=np.uint32)
     n = len(off) - 1
     m = int(off[-1])
     deg = np.diff(off.astype(np.int64))
     src = np.repeat(np.arange(n, dtype=np.int64), deg)
-    w = np.ones(m, dtype=np.uint64) if wt is None else np.asarray(wt, dtype=np.uint64)
+    w = np.ones(m, dtype=np.uint64) if wt is None else np.asarray(wt, dtype=np.uint64)[:m]
+    if merge and m:
+        key = src * n + idx[:m].astype(np.int64)
+        uk, inv = np.unique(key, return_inverse=True)
+        wsum = np.zeros(len(uk), dtype=np.uint64)
+        np.add.at(wsum, inv, w)  # exact (modulo 2^64)
+        w = wsum
+        src, idx = uk // n, (uk % n).astype(np.uint32)
+        m = len(uk)
     blocks = []
     if init is not None:
         init = np.asarray(init, dtype=np.uint32)
@@ -331,7 +342,9 @@ def run_ref_valmari(off, idx, wt=None, init=None, timeout: float = 600.0) -> Ora
     colours go in as MDP <blocks>."""
     if not os.path.exists(REF_VALMARI):
         raise FileNotFoundError(REF_VALMARI)
-    txt = subprocess.run([REF_VALMARI], input=mdp_text(off, idx, wt, init), capture_output=True,
+    n = len(off) - 1
+    merge = int(off[-1]) > n * n  # more arcs than the reader takes: merge parallel ones
+    txt = subprocess.run([REF_VALMARI], input=mdp_text(off, idx, wt, init, merge=merge), capture_output=True,
                          timeout=timeout, check=True).stdout.decode()
     t, done, nodes, rounds, labels = _parse_ref_output(txt)
     n = len(off) - 1

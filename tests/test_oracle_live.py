@@ -60,3 +60,19 @@ def test_oracle_equals_valmari_with_initial_blocks(seed):
     ex = oracle.refine_exact(off, idx, init=init)
     val = oracle.run_ref_valmari(off, idx, init=init)
     assert np.array_equal(ex.labels, val.labels) and ex.blocks == val.blocks
+
+
+@pytest.mark.parametrize("seed", range(20, 24))
+def test_valmari_input_with_parallel_arcs_merged_is_the_same(seed):
+    """Parallel arcs merged into one transition with the summed weight give
+    Valmari the same lumping (the form used when the reader would refuse more
+    transitions than states squared)."""
+    import subprocess
+    off, idx = _messy(seed)
+    wt = np.random.default_rng(seed).integers(1, 6, size=len(idx)).astype(np.uint64) if seed % 2 else None
+    labels = []
+    for merge in (False, True):
+        txt = subprocess.run([oracle.REF_VALMARI], input=oracle.mdp_text(off, idx, wt, None, merge=merge),
+                             capture_output=True, check=True, timeout=120).stdout.decode()
+        labels.append(oracle._canon_u64(oracle._parse_ref_output(txt)[4]))
+    assert np.array_equal(labels[0], labels[1])
