@@ -23,16 +23,26 @@ namespace {
 inline bool is_space(char c) { return c == ' ' || c == '\n' || c == '\r' || c == '\t'; }
 
 // Reads one decimal number; returns false on a missing or malformed token.
+// Up to 19 digits cannot overflow; longer tokens (leading zeros, or values
+// near 2^64) are re-read with a check per digit.
 inline bool read_num(const char*& p, const char* end, uint64_t& out)
 {
     while (p < end && (*p == ' ' || *p == '\t' || *p == '\r')) ++p;
-    if (p >= end || *p < '0' || *p > '9') return false;
+    const char* s = p;
     uint64_t v = 0;
-    while (p < end && *p >= '0' && *p <= '9') {
-        const uint64_t d = (uint64_t)(*p - '0');
-        if (v > (UINT64_MAX - d) / 10) return false;
-        v = v * 10 + d;
+    while (p < end && (unsigned)(*p - '0') < 10u) {
+        v = v * 10u + (uint64_t)(*p - '0');
         ++p;
+    }
+    const size_t len = (size_t)(p - s);
+    if (len == 0) return false;
+    if (len > 19) {
+        v = 0;
+        for (const char* q = s; q < p; ++q) {
+            const uint64_t d = (uint64_t)(*q - '0');
+            if (v > (UINT64_MAX - d) / 10) return false;
+            v = v * 10 + d;
+        }
     }
     if (p < end && !is_space(*p)) return false;
     out = v;
@@ -47,13 +57,95 @@ inline bool end_line(const char*& p, const char* end)
     return true;
 }
 
-struct Chunk {
-    std::vector<uint32_t> src, dst;
-    std::vector<uint64_t> wt;
-    bool ok = true;
-    bool unit = true;
-    std::string err;
+// A run of consecutive arcs with one source.  `at`: first arc (within the
+// chunk while parsing, then global); `row_at`: where the run starts inside
+// its source's row (a row can span a chunk boundary).
+struct Run {
+    uint32_t u;
+    uint64_t at, cnt, row_at;
 };
+
+// One thread's share of the lines.  Heads in input order, sources as runs,
+// weights only from the first weight other than 1 on (earlier ones are 1).
+struct Chunk {
+    uint32_t* dst = nullptr;
+    uint64_t* wt = nullptr;
+    uint64_t n = 0;
+    std::vector<Run> runs;
+    bool ok = true;
+    std::string err;
+    ~Chunk()
+    {
+        std::free(dst);
+        std::free(wt);
+    }
+};
+
+void parse_chunk(Chunk& c, const char* q, const char* e, uint64_t N)
+{
+    // lines in the chunk: an upper bound of its arcs
+    uint64_t cap = 1;
+    for (const char* r = q; r < e;) {
+        const void* nl = std::memchr(r, '\n', (size_t)(e - r));
+        if (!nl) break;
+        ++cap;
+        r = static_cast<const char*>(nl) + 1;
+    }
+    c.dst = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * cap));
+    if (!c.dst) {
+        c.ok = false;
+        c.err = "out of host memory";
+        return;
+    }
+    uint64_t cur = UINT64_MAX;
+    while (q < e) {
+        // skip blank lines
+        const char* r = q;
+        while (r < e && (*r == ' ' || *r == '\t' || *r == '\r')) ++r;
+        if (r < e && *r == '\n') {
+            q = r + 1;
+            continue;
+        }
+        if (r >= e) break;
+        uint64_t u, w, v;
+        if (!read_num(q, e, u) || !read_num(q, e, w) || !read_num(q, e, v) || !end_line(q, e)) {
+            c.ok = false;
+            c.err = "malformed arc line";
+            return;
+        }
+        if (u >= N || v >= N) {
+            c.ok = false;
+            c.err = "node id out of range";
+            return;
+        }
+        if (u != cur) {
+            if (!c.runs.empty()) c.runs.back().cnt = c.n - c.runs.back().at;
+            c.runs.push_back(Run{(uint32_t)u, c.n, 0, 0});
+            cur = u;
+        }
+        if (w != 1 && !c.wt) {
+            c.wt = static_cast<uint64_t*>(std::malloc(sizeof(uint64_t) * cap));
+            if (!c.wt) {
+                c.ok = false;
+                c.err = "out of host memory";
+                return;
+            }
+            for (uint64_t i = 0; i < c.n; ++i) c.wt[i] = 1;
+        }
+        if (c.wt) c.wt[c.n] = w;
+        c.dst[c.n++] = (uint32_t)v;
+    }
+    if (!c.runs.empty()) c.runs.back().cnt = c.n - c.runs.back().at;
+}
+
+template <typename F>
+void parallel_for(int T, F&& f)
+{
+    std::vector<std::thread> ts;
+    for (int t = 1; t < T; ++t) ts.emplace_back(f, t);
+    f(0);
+    for (auto& x : ts) x.join();
+}
 
 }  // namespace
 
@@ -84,78 +176,71 @@ extern "C" rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_g
         cut[t] = q;
     }
     std::vector<Chunk> ch(T);
-    std::vector<std::thread> ts;
-    for (int t = 0; t < T; ++t)
-        ts.emplace_back([&, t] {
-            Chunk& c = ch[t];
-            const char* q = cut[t];
-            const char* e = cut[t + 1];
-            while (q < e) {
-                // skip blank lines
-                const char* r = q;
-                while (r < e && (*r == ' ' || *r == '\t' || *r == '\r')) ++r;
-                if (r < e && *r == '\n') { q = r + 1; continue; }
-                if (r >= e) break;
-                uint64_t u, w, v;
-                if (!read_num(q, e, u) || !read_num(q, e, w) || !read_num(q, e, v) || !end_line(q, e)) {
-                    c.ok = false;
-                    c.err = "malformed arc line";
-                    return;
-                }
-                if (u >= N || v >= N) {
-                    c.ok = false;
-                    c.err = "node id out of range";
-                    return;
-                }
-                c.src.push_back((uint32_t)u);
-                c.dst.push_back((uint32_t)v);
-                c.wt.push_back(w);
-                if (w != 1) c.unit = false;
-            }
-        });
-    for (auto& x : ts) x.join();
+    parallel_for(T, [&](int t) { parse_chunk(ch[t], cut[t], cut[t + 1], N); });
     uint64_t total = 0;
     bool unit = true;
-    for (auto& c : ch) {
-        if (!c.ok) return rbsc_fail(nullptr, RBSC_ERR_PARSE, "%s", c.err.c_str());
-        total += c.src.size();
-        unit = unit && c.unit;
+    std::vector<uint64_t> base(T + 1, 0);
+    for (int t = 0; t < T; ++t) {
+        if (!ch[t].ok) return rbsc_fail(nullptr, ch[t].err == "out of host memory" ? RBSC_ERR_OOM : RBSC_ERR_PARSE, "%s",
+                                        ch[t].err.c_str());
+        base[t] = total;
+        total += ch[t].n;
+        unit = unit && !ch[t].wt;
     }
+    base[T] = total;
     if (total != M)
         return rbsc_fail(nullptr, RBSC_ERR_PARSE, "header announces %llu arcs, input holds %llu", (unsigned long long)M,
                          (unsigned long long)total);
 
     // arcs must be grouped by source: every source starts exactly one run
-    std::vector<uint8_t> seen(N, 0);
+    // (a run cut by a chunk boundary continues in the next chunk)
     uint64_t* off = (uint64_t*)std::calloc(N + 1, sizeof(uint64_t));
     uint32_t* idx = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(M, 1));
     uint64_t* wt = unit ? nullptr : (uint64_t*)std::malloc(sizeof(uint64_t) * std::max<uint64_t>(M, 1));
+    std::vector<uint8_t> seen(N, 0);
     if (!off || !idx || (!unit && !wt)) {
         std::free(off); std::free(idx); std::free(wt);
         return rbsc_fail(nullptr, RBSC_ERR_OOM, "out of host memory");
     }
     int64_t prev = -1;
-    for (auto& c : ch)
-        for (size_t i = 0; i < c.src.size(); ++i) {
-            const uint32_t u = c.src[i];
-            if ((int64_t)u != prev) {
-                if (seen[u]) {
-                    std::free(off); std::free(idx); std::free(wt);
-                    return rbsc_fail(nullptr, RBSC_ERR_PARSE, "arcs of node %u are not contiguous (input must be grouped by source)", u);
-                }
-                seen[u] = 1;
-                prev = u;
+    bool sorted = true;
+    for (int t = 0; t < T; ++t)
+        for (Run& r : ch[t].runs) {
+            r.at += base[t];
+            if ((int64_t)r.u == prev) {  // continues the previous chunk's last run
+                r.row_at = off[r.u + 1];
+                off[r.u + 1] += r.cnt;
+                continue;
             }
-            ++off[u + 1];
+            if (seen[r.u]) {
+                std::free(off); std::free(idx); std::free(wt);
+                return rbsc_fail(nullptr, RBSC_ERR_PARSE, "arcs of node %u are not contiguous (input must be grouped by source)", r.u);
+            }
+            seen[r.u] = 1;
+            sorted = sorted && (int64_t)r.u > prev;
+            prev = r.u;
+            r.row_at = 0;
+            off[r.u + 1] = r.cnt;
         }
     for (uint64_t u = 0; u < N; ++u) off[u + 1] += off[u];
-    std::vector<uint64_t> fill(off, off + N);
-    for (auto& c : ch)
-        for (size_t i = 0; i < c.src.size(); ++i) {
-            const uint64_t k = fill[c.src[i]]++;
-            idx[k] = c.dst[i];
-            if (wt) wt[k] = c.wt[i];
+
+    // heads (and weights) to their rows: in source order the input already is
+    // the CSR, chunk by chunk; otherwise run by run
+    parallel_for(T, [&](int t) {
+        const Chunk& c = ch[t];
+        if (sorted) {
+            if (c.n) std::memcpy(idx + base[t], c.dst, sizeof(uint32_t) * c.n);
+            if (wt)
+                for (uint64_t i = 0; i < c.n; ++i) wt[base[t] + i] = c.wt ? c.wt[i] : 1u;
+            return;
         }
+        for (const Run& r : c.runs) {
+            const uint64_t from = r.at - base[t], to = off[r.u] + r.row_at;
+            std::memcpy(idx + to, c.dst + from, sizeof(uint32_t) * r.cnt);
+            if (wt)
+                for (uint64_t i = 0; i < r.cnt; ++i) wt[to + i] = c.wt ? c.wt[from + i] : 1u;
+        }
+    });
     out->n = (uint32_t)N;
     out->m = M;
     out->offsets = off;

@@ -120,3 +120,90 @@ def test_csr_cache_roundtrip_and_checks(tmp_path):
     for name in ("bad.csr", "short.csr", "text.csr"):
         with pytest.raises(R.RbscError):
             R.load_csr(str(tmp_path / name))
+
+
+def _arcs_text(n, rows, weights=None):
+    """arcs-cuda text with the rows given as (u, heads) in the listed order."""
+    lines, m = [], 0
+    for u, heads in rows:
+        for j, v in enumerate(heads):
+            w = 1 if weights is None else weights(u, j)
+            lines.append(f"{u} {w} {v}")
+            m += 1
+    return (f"{n}\n{m}\n" + "\n".join(lines) + "\n").encode()
+
+
+def _csr_of(n, rows, weights=None):
+    deg = np.zeros(n + 1, dtype=np.uint64)
+    for u, heads in rows:
+        deg[u + 1] = len(heads)
+    off = np.cumsum(deg, dtype=np.uint64)
+    idx = np.zeros(int(off[-1]), dtype=np.uint32)
+    wt = np.ones(int(off[-1]), dtype=np.uint64)
+    for u, heads in rows:
+        idx[off[u]:off[u + 1]] = heads
+        if weights is not None:
+            wt[off[u]:off[u + 1]] = [weights(u, j) for j in range(len(heads))]
+    return off, idx, wt
+
+
+def test_parse_large_unsorted_groups_across_threads():
+    """More than 1 MB of text (parsed by several threads): rows in random
+    order, one row long enough to cross chunk boundaries, weights other than 1
+    only near the end."""
+    rng = np.random.default_rng(5)
+    n = 40000
+    rows = [(u, rng.integers(0, n, size=int(rng.integers(1, 12)))) for u in range(0, n, 2)]
+    rows.append((1, rng.integers(0, n, size=200000)))  # ~2 MB of one row
+    order = rng.permutation(len(rows))
+    rows = [rows[i] for i in order]
+    late = {u for u, _ in rows[-50:]}
+    wfun = lambda u, j: (j % 5) + 2 if u in late else 1
+    text = _arcs_text(n, rows, wfun)
+    assert len(text) > (1 << 21)
+    off, idx, wt = R.parse_arcs(text)
+    eo, ei, ew = _csr_of(n, rows, wfun)
+    assert np.array_equal(off, eo) and np.array_equal(idx, ei) and np.array_equal(wt, ew)
+    # unit weights: no weight array; sorted rows: the same CSR
+    text = _arcs_text(n, sorted(rows, key=lambda r: r[0]))
+    off, idx, wt = R.parse_arcs(text)
+    assert wt is None and np.array_equal(off, eo) and np.array_equal(idx, ei)
+
+
+def test_parse_rejects_a_group_split_across_threads():
+    rng = np.random.default_rng(6)
+    n = 30000
+    rows = [(u, rng.integers(0, n, size=8)) for u in range(1, n)]
+    rows = [(0, [1, 2])] + rows + [(0, [3])]
+    with pytest.raises(R.RbscError) as e:
+        R.parse_arcs(_arcs_text(n, rows))
+    assert "grouped" in str(e.value)
+
+
+def test_parse_long_numbers():
+    big = (1 << 64) - 1
+    off, idx, wt = R.parse_arcs(f"3\n2\n0 {big} 00000000000000000000002\n2 0000000000000000000000007 1\n".encode())
+    assert idx.tolist() == [2, 1] and wt.tolist() == [big, 7]
+    with pytest.raises(R.RbscError):
+        R.parse_arcs(f"3\n1\n0 {big + 1} 2\n".encode())
+
+
+def test_csr_cache_reads_version_1_files(tmp_path):
+    """Files of the first format version (FNV-1a 64 over every byte) still
+    load; a wrong checksum is still refused."""
+    import struct
+    off = np.array([0, 2, 3, 3], dtype=np.uint64)
+    idx = np.array([1, 2, 0], dtype=np.uint32)
+    payload = off.tobytes() + idx.tobytes()
+    h = 0xcbf29ce484222325
+    for b in payload:
+        h = ((h ^ b) * 0x100000001b3) & 0xFFFFFFFFFFFFFFFF
+    head = b"RBSCCSR1" + struct.pack("<IIQQQ", 1, 0, 3, 3, h) + bytes(24)
+    p = str(tmp_path / "v1.csr")
+    open(p, "wb").write(head + payload)
+    o2, i2, w2 = R.load_csr(p)
+    assert o2.tolist() == off.tolist() and i2.tolist() == idx.tolist() and w2 is None
+    head = b"RBSCCSR1" + struct.pack("<IIQQQ", 1, 0, 3, 3, h ^ 1) + bytes(24)
+    open(p, "wb").write(head + payload)
+    with pytest.raises(R.RbscError):
+        R.load_csr(p)
