@@ -107,3 +107,42 @@ def test_gpu_streamed_equals_the_reference_programs(law):
         g.free()
     assert r.blocks == FX["blocks"] and r.rounds == FX["rounds"]
     assert _sha(r.labels.astype(np.uint32)) == FX["labels_sha256"]
+
+
+def _copy_bv(tmp_path, name, drop_offsets=False, drop_maxref=False, flip_at=None):
+    import shutil
+    dst = str(tmp_path / name)
+    for ext in (".graph", ".properties", ".offsets"):
+        if ext == ".offsets" and drop_offsets:
+            continue
+        shutil.copyfile(BV + ext, dst + ext)
+    if drop_maxref:
+        lines = [l for l in open(dst + ".properties") if not l.startswith("maxrefcount")]
+        open(dst + ".properties", "w").write("".join(lines))
+    if flip_at is not None:
+        raw = bytearray(open(dst + ".graph", "rb").read())
+        raw[int(len(raw) * flip_at)] ^= 0xff
+        open(dst + ".graph", "wb").write(bytes(raw))
+    return dst
+
+
+@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+def test_bv_reader_paths_agree(tmp_path):
+    """The threaded reader (offsets file and maxrefcount present: lists
+    decoded by node ranges) and the one-pass reader (no offsets file, or no
+    recorded maxrefcount) give the same CSR and statistics."""
+    ref = R.load_bvgraph(BV)
+    for kw in ({"drop_offsets": True}, {"drop_maxref": True}):
+        off, idx, st = R.load_bvgraph(_copy_bv(tmp_path, "one_pass_" + "_".join(kw), **kw))
+        assert np.array_equal(off, ref[0]) and np.array_equal(idx, ref[1])
+        for k in ("copied_arcs", "interval_arcs", "residual_arcs", "bits"):
+            assert st[k] == ref[2][k]
+        assert st["offsets_checked"] == (0 if "drop_offsets" in kw else 1)
+
+
+@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+@pytest.mark.parametrize("flip_at", [0.31, 0.77])
+def test_bv_reader_rejects_a_corrupted_stream(tmp_path, flip_at):
+    for kw in ({}, {"drop_maxref": True}):
+        with pytest.raises(R.RbscError):
+            R.load_bvgraph(_copy_bv(tmp_path, f"bad_{flip_at}_{len(kw)}", flip_at=flip_at, **kw))
