@@ -25,3 +25,18 @@ def test_reference_arm_prints_one_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] == 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": d["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+
+
+def test_cpu_baseline_has_the_reference_and_an_all_cores_port():
+    """The GPU arm's cpu_baseline leg, run here on the CPU: the reference
+    program on one core, and the oracle's threaded rsc restatement on every
+    core over the same sample with the same rounds and blocks."""
+    sys.path.insert(0, ROOT)
+    import bench
+    c = bench.cpu_baseline_reference()
+    assert c["value"] > 0 and c["unit"] == "edge-rounds/s" and c["cores"] == 1
+    p = c["port_all_cores"]
+    assert "unavailable" not in p, p
+    assert p["kind"] == "port" and p["cores"] == (os.cpu_count() or 1) and p["value"] > 0
+    if c["kind"] == "reference":
+        assert p["rounds"] == c["runs"][0]["rounds"] and p["blocks"] == c["runs"][0]["blocks"]
