@@ -33,13 +33,19 @@
 #include <string>
 #include <vector>
 
+#include <sys/stat.h>
+
 #include "../../include/rbsc.h"
 
+// Reads the whole stream; a regular file (stdin redirected from a file) is
+// read straight into a buffer of its size, a pipe in 4 MiB blocks.
 static bool read_all(FILE* f, std::string& s)
 {
-    char buf[1 << 16];
+    struct stat st;
+    if (fstat(fileno(f), &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) s.reserve((size_t)st.st_size + 1);
+    std::vector<char> buf((size_t)1 << 22);
     size_t k;
-    while ((k = fread(buf, 1, sizeof buf, f)) > 0) s.append(buf, k);
+    while ((k = fread(buf.data(), 1, buf.size(), f)) > 0) s.append(buf.data(), k);
     return !ferror(f);
 }
 
