@@ -26,6 +26,11 @@
 //   --csr-cache FILE        read the graph from this binary CSR cache when it
 //                           exists (stdin is not read); otherwise parse stdin
 //                           and write the cache
+//   --bv BASENAME           read the graph from BV (WebGraph) files
+//                           BASENAME.properties / .graph / .offsets instead of
+//                           stdin: the step the reference leaves to webgraph-rs
+//                           (its arcs-cuda output, unit weights); with
+//                           --csr-cache, the cache is written from it
 #include <cinttypes>
 #include <cstdio>
 #include <cstdlib>
@@ -54,6 +59,7 @@ int main(int argc, char** argv)
     const char* dump = nullptr;
     const char* init_path = nullptr;
     const char* cache_path = nullptr;
+    const char* bv_path = nullptr;
     bool want_stats = false, aggressive = false, exact = false;
     int relabel = RBSC_RELABEL_HASH;
     std::vector<const char*> pos;
@@ -64,6 +70,7 @@ int main(int argc, char** argv)
         else if (!std::strcmp(argv[i], "--aggressive")) aggressive = true;
         else if (!std::strcmp(argv[i], "--exact")) exact = true;
         else if (!std::strcmp(argv[i], "--csr-cache") && i + 1 < argc) cache_path = argv[++i];
+        else if (!std::strcmp(argv[i], "--bv") && i + 1 < argc) bv_path = argv[++i];
         else if (!std::strcmp(argv[i], "--relabel") && i + 1 < argc) relabel = !std::strcmp(argv[++i], "sort") ? RBSC_RELABEL_SORT : RBSC_RELABEL_HASH;
         else pos.push_back(argv[i]);
     }
@@ -81,14 +88,21 @@ int main(int argc, char** argv)
             return EXIT_FAILURE;
         }
     } else {
-        std::string text;
-        if (!read_all(stdin, text)) {
-            std::printf("failed to read standard input\n");
-            return EXIT_FAILURE;
-        }
-        if (rbsc_parse_arcs(text.data(), text.size(), &hg) != RBSC_OK) {
-            std::printf("input error: %s\n", rbsc_last_error(nullptr));
-            return EXIT_FAILURE;
+        if (bv_path) {
+            if (rbsc_bv_load(bv_path, &hg, nullptr) != RBSC_OK) {
+                std::printf("input error: %s\n", rbsc_last_error(nullptr));
+                return EXIT_FAILURE;
+            }
+        } else {
+            std::string text;
+            if (!read_all(stdin, text)) {
+                std::printf("failed to read standard input\n");
+                return EXIT_FAILURE;
+            }
+            if (rbsc_parse_arcs(text.data(), text.size(), &hg) != RBSC_OK) {
+                std::printf("input error: %s\n", rbsc_last_error(nullptr));
+                return EXIT_FAILURE;
+            }
         }
         if (cache_path) {
             rbsc_csr c{hg.n, hg.m, hg.offsets, 8, hg.indices, hg.weights};

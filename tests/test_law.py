@@ -146,3 +146,24 @@ def test_bv_reader_rejects_a_corrupted_stream(tmp_path, flip_at):
     for kw in ({}, {"drop_maxref": True}):
         with pytest.raises(R.RbscError):
             R.load_bvgraph(_copy_bv(tmp_path, f"bad_{flip_at}_{len(kw)}", flip_at=flip_at, **kw))
+
+
+@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+def test_cli_reads_bv_files(tmp_path):
+    """`rbsc --bv BASENAME` loads the graph from the BV files instead of
+    stdin (with --csr-cache the cache is written from them); without a GPU the
+    command stops after loading, at the device."""
+    import subprocess
+    import torch
+    cli = os.path.join(os.path.dirname(R.__file__), "rbsc")
+    cache = str(tmp_path / "cnr.csr")
+    r = subprocess.run([cli, "--bv", BV, "--csr-cache", cache], capture_output=True, timeout=600)
+    if torch.cuda.is_available():
+        lines = r.stdout.decode().split()
+        assert r.returncode == 0 and lines[1] == "1" and int(lines[2]) == FX["blocks"]
+    else:
+        assert r.returncode != 0 and b"CUDA setup failed" in r.stdout
+    off, idx, wt = R.load_csr(cache)
+    assert wt is None and _sha(off.astype(np.uint64), idx.astype(np.uint32)) == FX["csr_sha256"]
+    r = subprocess.run([cli, "--bv", str(tmp_path / "missing")], capture_output=True, timeout=60)
+    assert r.returncode != 0 and b"input error" in r.stdout
