@@ -27,7 +27,8 @@
 //                           exists (stdin is not read); otherwise parse stdin
 //                           and write the cache
 //   --bv BASENAME           read the graph from BV (WebGraph) files
-//                           BASENAME.properties / .graph / .offsets instead of
+//                           BASENAME.properties / .graph / .offsets (BASENAME
+//                           or BASENAME.graph may be given) instead of
 //                           stdin: the step the reference leaves to webgraph-rs
 //                           (its arcs-cuda output, unit weights); with
 //                           --csr-cache, the cache is written from it
@@ -89,7 +90,10 @@ int main(int argc, char** argv)
         }
     } else {
         if (bv_path) {
-            if (rbsc_bv_load(bv_path, &hg, nullptr) != RBSC_OK) {
+            // the basename, or the path of its .graph file
+            std::string base(bv_path);
+            if (base.size() > 6 && base.compare(base.size() - 6, 6, ".graph") == 0) base.resize(base.size() - 6);
+            if (rbsc_bv_load(base.c_str(), &hg, nullptr) != RBSC_OK) {
                 std::printf("input error: %s\n", rbsc_last_error(nullptr));
                 return EXIT_FAILURE;
             }

@@ -157,7 +157,7 @@ def test_cli_reads_bv_files(tmp_path):
     import torch
     cli = os.path.join(os.path.dirname(R.__file__), "rbsc")
     cache = str(tmp_path / "cnr.csr")
-    r = subprocess.run([cli, "--bv", BV, "--csr-cache", cache], capture_output=True, timeout=600)
+    r = subprocess.run([cli, "0", "1", "--bv", BV + ".graph", "--csr-cache", cache], capture_output=True, timeout=600)
     if torch.cuda.is_available():
         lines = r.stdout.decode().split()
         assert r.returncode == 0 and lines[1] == "1" and int(lines[2]) == FX["blocks"]
