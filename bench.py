@@ -18,9 +18,15 @@ independent replicas, `value` is the sum over ranks of arcs x rounds divided
 by the slowest rank's time.
 
 --impl reference: the reference's own CPU program (src/rsc/rsc.cpp, compiled
-unmodified into oracle/_ref/ref_rsc) on a bounded sample of the workload
-(R-MAT scale 20, same generator and parameters), timed by its own internal
-refinement timer, on rank 0 only.
+unmodified into oracle/_ref/ref_rsc) on the same R-MAT-24 graph, built by the
+oracle's generator (nothing of this package is loaded); one step = one rsc
+round over the whole graph, timed between rsc's per-round sorts, after a single
+parse of its input; rank 0 only.
+
+Beside the line: `cpu_baseline` (the same program, a bounded sample of rounds
+of the same graph, plus the oracle's rsc restatement on every host core) and
+`reference_gpu_program` (src/rbsc/rbsc.cu, unmodified, one batch, on the same
+graph: its own timer and block count).
 """
 from __future__ import annotations
 
@@ -41,7 +47,6 @@ sys.path.insert(0, ROOT)
 
 METRIC = "edge-rounds/s (R-MAT-24 colour refinement to the verified fixpoint)"
 UNIT = "edge-rounds/s"
-SAMPLE_SCALE = 20
 
 
 def env_rank():
@@ -142,103 +147,174 @@ class Clocks:
                 "samples": len(sm)}
 
 
-def cpu_baseline_reference(steps: int = 1):
-    """The reference rsc (oracle/_ref/ref_rsc, unmodified rsc.cpp) on the R-MAT
-    scale-20 sample; falls back to the oracle's restatement of rsc when the
-    reference binary was not built.  Returns the cpu_baseline object."""
-    import numpy as np
-    import rbsc_b200 as R
+def ref_rsc_round_samples(off, idx, samples: int, timeout: float = 1800.0):
+    """The reference rsc (oracle/_ref/ref_rsc: src/rsc/rsc.cpp compiled
+    unmodified) on one graph: the arcs-cuda text goes through a pipe, rsc's
+    input is parsed once, and refinements run in forked children until they
+    have reported `samples` round times (the time between successive entries
+    of the per-round sort of rsc.cpp:130, one complete round each).  Returns
+    {"round_s": [...], "runs": [{time_s, rounds, blocks}, ...]} where time_s is
+    rsc's own refinement timer (rsc.cpp:116-147) of each full run."""
+    import threading
     from oracle import oracle
-    off, idx = R.gen_rmat_host(SAMPLE_SCALE, 16, seed=1)
-    m = int(off[-1])
-    sample = (f"R-MAT scale {SAMPLE_SCALE}, edge factor 16, same generator ({m} arcs after dedup), "
-              f"uniform initial colours (rsc.cpp:118-121 fixes them); refinement time from the program's own timer")
+    rfd, wfd = os.pipe()
+    proc = subprocess.Popen([oracle.REF_RSC, "--round-samples", str(int(samples)), "--no-labels"], stdin=rfd,
+                            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL)
+    os.close(rfd)
+    err = []
+
+    def feed():
+        try:
+            oracle.write_arcs_file(f"/dev/fd/{wfd}", off, idx)
+        except Exception as e:  # reported below
+            err.append(e)
+        finally:
+            os.close(wfd)
+
+    th = threading.Thread(target=feed)
+    th.start()
+    out, _ = proc.communicate(timeout=timeout)
+    th.join()
+    if err or proc.returncode != 0:
+        raise RuntimeError(f"ref_rsc failed (rc {proc.returncode}): {err}")
+    lines = out.decode().split("\n")
+    runs, rs = [], []
+    i = 0
+    while i + 4 < len(lines) and lines[i + 3].startswith("rounds "):
+        runs.append({"time_s": float(lines[i]), "blocks": int(lines[i + 2]), "rounds": int(lines[i + 3].split()[1])})
+        rs.extend(float(x) for x in lines[i + 4].split()[1:])
+        i += 5
+    return {"round_s": rs, "runs": runs}
+
+
+def cpu_baseline_reference(off, idx, samples: int = 4):
+    """cpu_baseline of the bench line: the reference rsc on the workload's own
+    graph (R-MAT-24), a bounded sample of `samples` rounds (about 10 s of
+    refinement), single-threaded as rsc is; beside it the oracle's restatement
+    of rsc on every host core (orc_refine_rsc_mt) over the full refinement of
+    the same graph.  Falls back to the restatement alone when the reference
+    binary was not built."""
+    from oracle import oracle
+    m = len(idx)
+    sample = (f"{samples} rounds of rsc on the workload's own graph (R-MAT-24, {m} arcs); rsc.cpp:118-121 fixes "
+              "uniform initial colours (the degree classes come out of its first round; same final partition); "
+              "round time = interval between successive per-round sorts (rsc.cpp:130) in one refinement")
+
     def port_all_cores():
-        """The oracle's rsc restatement on every host core (orc_refine_rsc_mt:
-        the same ranks as rsc, on pthreads) over the same sample: a
-        multi-core CPU figure beside the single-threaded reference program."""
         try:
             thr = os.cpu_count() or 1
-            ts, r = [], None
-            for _ in range(3):
-                t0 = time.perf_counter()
-                r = oracle.refine_rsc(off, idx, threads=thr)
-                ts.append(time.perf_counter() - t0)
-            t = sorted(ts)[1]
+            t0 = time.perf_counter()
+            r = oracle.refine_rsc(off, idx, threads=thr)
+            t = time.perf_counter() - t0
             return {"value": m * r.rounds_cpu / t, "unit": UNIT, "cores": thr, "kind": "port", "time_s": t,
                     "rounds": r.rounds_cpu, "blocks": r.blocks,
-                    "note": "wall time of the call (median of 3), refinement only, same sample"}
+                    "note": "orc_refine_rsc_mt: the same ranks as rsc, on pthreads; wall time of the call, refinement only"}
         except Exception as e:  # an informational figure: never fails the bench
             return {"unavailable": str(e)[:200]}
 
     if os.path.exists(oracle.REF_RSC):
-        with tempfile.TemporaryDirectory() as d:
-            path = os.path.join(d, "rmat.txt")
-            oracle.write_arcs_file(path, off, idx)
-            tot_t, tot_er, runs = 0.0, 0.0, []
-            for _ in range(steps):
-                t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
-                tot_t += t
-                tot_er += m * rounds
-                runs.append(dict(time_s=t, rounds=rounds, blocks=blocks, wall_s=round(wall, 3)))
-        law = None
-        g = oracle.load_law()
-        if g is not None:
-            with tempfile.TemporaryDirectory() as d:
-                path = os.path.join(d, "cnr.txt")
-                oracle.write_arcs_file(path, g[0], g[1])
-                t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
-            law = {"graph": "cnr-2000", "time_s": t, "rounds": rounds, "blocks": blocks, "wall_s": round(wall, 3),
-                   "edge_rounds_per_s": len(g[1]) * rounds / t}
-        return {"value": tot_er / tot_t, "unit": UNIT, "cores": 1, "kind": "reference",
-                "sample": sample, "runs": runs, "host_cores": os.cpu_count(), "law_cnr2000": law,
-                "port_all_cores": port_all_cores()}
+        r = ref_rsc_round_samples(off, idx, samples)
+        ts = r["round_s"][:samples]
+        own = r["runs"][0]
+        return {"value": m * len(ts) / sum(ts), "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample,
+                "round_s": ts, "rsc_own_timer": {"time_s": own["time_s"], "rounds": own["rounds"],
+                                                 "blocks": own["blocks"],
+                                                 "edge_rounds_per_s": m * own["rounds"] / own["time_s"]},
+                "host_cores": os.cpu_count(), "port_all_cores": port_all_cores()}
+    pa = port_all_cores()
+    return {"value": pa.get("value"), "unit": UNIT, "cores": pa.get("cores"), "kind": "port",
+            "sample": "the oracle's rsc restatement, full refinement of the workload's graph", "host_cores": os.cpu_count()}
+
+
+def reference_gpu_program(off, idx, blocks: int, timeout: float = 900.0):
+    """The reference GPU program (src/rbsc/rbsc.cu, unmodified, its stdin served
+    from memory: oracle/_ref/ref_rbsc_fast) on the workload's graph, one batch
+    (edge_batch_size = M), uniform initial colours as it takes them.  Its own
+    timer (rbsc.cu:272, 489-494) covers the H2D copies and the round loop; its
+    "nodes" line must equal the blocks found here.  Informational."""
+    import threading
+    from oracle import oracle
+    exe = os.path.join(oracle.REF_DIR, "ref_rbsc_fast")
+    if not os.path.exists(exe):
+        return {"unavailable": "oracle/_ref/ref_rbsc_fast was not built (reference tree absent at build time)"}
+    rfd, wfd = os.pipe()
     t0 = time.perf_counter()
-    r = oracle.refine_rsc(off, idx)
-    t = time.perf_counter() - t0
-    return {"value": m * r.rounds_cpu / t, "unit": UNIT, "cores": 1, "kind": "port", "sample": sample,
-            "host_cores": os.cpu_count(), "port_all_cores": port_all_cores()}
+    proc = subprocess.Popen([exe, str(len(idx))], stdin=rfd, stdout=subprocess.PIPE, stderr=subprocess.PIPE)
+    os.close(rfd)
+
+    def feed():
+        try:
+            oracle.write_arcs_file(f"/dev/fd/{wfd}", off, idx)
+        finally:
+            os.close(wfd)
+
+    th = threading.Thread(target=feed)
+    th.start()
+    try:
+        out, errb = proc.communicate(timeout=timeout)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        proc.communicate()
+        th.join()
+        return {"unavailable": f"no result within {timeout:.0f} s"}
+    th.join()
+    wall = time.perf_counter() - t0
+    lines = out.decode().split("\n")
+    if proc.returncode != 0 or len(lines) < 3:
+        return {"unavailable": f"rc {proc.returncode}: {(out + errb).decode()[-200:]}"}
+    t, done, nodes = float(lines[0]), int(lines[1]), int(lines[2])
+    return {"program": "src/rbsc/rbsc.cu (unmodified), edge_batch_size = M, one GPU", "time_s": t, "done": done,
+            "nodes": nodes, "same_block_count": nodes == blocks, "wall_s_with_parse": wall,
+            "note": "its own timer: from after setup to the end of refinement, H2D of the arcs included"}
 
 
-def config(n=None, m=None, rounds=None, scale=24, ef=16):
+def config(n=None, m=None, scale=24, ef=16):
     return {"workload": f"rmat{scale}_ef{ef}", "model": "none (graph refinement)", "scale": scale, "edge_factor": ef,
-            "rmat_abc": [0.57, 0.19, 0.19], "nodes": n, "arcs": m, "rounds": rounds,
+            "rmat_abc": [0.57, 0.19, 0.19], "nodes": n, "arcs": m,
             "initial_colors": "floor(log2(out_degree+1))", "offsets": "int64", "indices": "int32",
             "l2": "no flush: inputs larger than L2 (heads 4 B/arc)", "parallelism": "replicas",
             "global_batch": 1, "seq_len": None}
 
 
 def run_reference(args, rank, world):
+    """The reference arm: rsc (src/rsc/rsc.cpp, unmodified) on the same
+    workload graph, generated by the oracle (oracle.c: orc_gen_rmat, the same
+    arcs as the product's generator) so that nothing of the product is
+    loaded.  One step = one rsc round over the whole graph (rsc processes every
+    arc and node in every round); W + K round samples from refinements forked
+    after a single parse.  Rank 0 only."""
     if rank != 0:
         return 0
-    import numpy as np
-    import rbsc_b200 as R
     from oracle import oracle
-    off, idx = R.gen_rmat_host(SAMPLE_SCALE, 16, seed=1)
-    m = int(off[-1])
     if not os.path.exists(oracle.REF_RSC):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/ref_rsc was not built (reference tree absent at build time)"}))
         return 0
-    with tempfile.TemporaryDirectory() as d:
-        path = os.path.join(d, "rmat.txt")
-        oracle.write_arcs_file(path, off, idx)
-        for _ in range(args.warmup):
-            oracle.run_ref_rsc_file(path)
-        tot_t, tot_er, rounds = 0.0, 0.0, None
-        for _ in range(args.steps):
-            t, blocks, rounds, wall = oracle.run_ref_rsc_file(path)
-            tot_t += t
-            tot_er += m * rounds
-    value = tot_er / tot_t
-    sample = (f"R-MAT scale {SAMPLE_SCALE}, edge factor 16, same generator ({m} arcs), uniform initial colours; "
-              f"each step one full rsc run, refinement time from rsc.cpp's own timer")
+    t0 = time.perf_counter()
+    off, idx = oracle.gen_rmat(args.scale, args.ef, seed=args.seed)
+    n, m = len(off) - 1, len(idx)
+    gen_s = time.perf_counter() - t0
+    r = ref_rsc_round_samples(off, idx, args.warmup + args.steps)
+    rs = r["round_s"]
+    timed = rs[args.warmup: args.warmup + args.steps]
+    tot = sum(timed)
+    value = m * len(timed) / tot
+    own_t = sum(x["time_s"] for x in r["runs"])
+    own_er = sum(m * x["rounds"] for x in r["runs"])
+    sample = (f"one step = one rsc round over the whole R-MAT scale {args.scale} graph ({m} arcs, {n} nodes; "
+              "rsc touches every arc and node every round); round time = interval between successive per-round "
+              "sorts (rsc.cpp:130); rsc.cpp:118-121 fixes uniform initial colours (the degree classes come out of "
+              "its first round; same final partition)")
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * tot_t / args.steps,
+            "steps": len(timed), "warmup": args.warmup, "ms_per_step": 1000.0 * tot / len(timed),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-            "config": config(), "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference",
-                                                 "sample": sample, "host_cores": os.cpu_count()},
+            "config": config(n, m, args.scale, args.ef),
+            "rounds": r["runs"][0]["rounds"], "blocks": r["runs"][0]["blocks"],
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "reference", "sample": sample,
+                             "host_cores": os.cpu_count()},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "gpu_launches": 0}
+            "rsc_own_timer": {"runs": r["runs"], "edge_rounds_per_s": own_er / own_t},
+            "generation_s": gen_s, "gpu_launches": 0,
+            "program": "oracle/_ref/ref_rsc: src/rsc/rsc.cpp compiled unmodified (-O2), single-threaded"}
     print(json.dumps(line))
     return 0
 
@@ -270,7 +346,8 @@ def run_ours(args, rank, world, local_rank):
         g.refine_device(d_init.data_ptr(), d_out.data_ptr())
         times, pr = g.profile(d_init.data_ptr())
         if rank == 0:
-            print(json.dumps({"profile_refine": config(n, m, pr.rounds, args.scale, args.ef), "device_ms": pr.device_ms,
+            print(json.dumps({"profile_refine": config(n, m, args.scale, args.ef), "rounds": pr.rounds,
+                              "device_ms": pr.device_ms,
                               "times": times}))
         g.free()
         ctx.close()
@@ -397,18 +474,21 @@ def run_ours(args, rank, world, local_rank):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_reference()
+        cpu = cpu_baseline_reference(off_np, idx_np)
+    ref_gpu = None
+    if rank == 0 and world == 1 and not args.no_ref_gpu:
+        ref_gpu = reference_gpu_program(off_np, idx_np, results[0].blocks)
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
-                "config": config(n, m, rounds, args.scale, args.ef), "time_to_fixpoint_ms": dev_ms / args.steps,
+                "config": config(n, m, args.scale, args.ef), "rounds": rounds, "time_to_fixpoint_ms": dev_ms / args.steps,
                 "blocks": results[0].blocks, "verify_ms": results[0].verify_ms,
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "autotune": tune, "batched": batched,
-                "served": served, "law_cnr2000": law, "streamed": streamed}
+                "served": served, "law_cnr2000": law, "streamed": streamed, "reference_gpu_program": ref_gpu}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -733,6 +813,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--relabel", choices=["hash", "sort"], default="hash")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-ref-gpu", action="store_true",
+                    help="skip the reference GPU program (src/rbsc/rbsc.cu) on the same graph")
     ap.add_argument("--batch-graphs", type=int, default=100000, help="small-graph batch size (0: skip)")
     ap.add_argument("--batch-steps", type=int, default=5)
     ap.add_argument("--batch-sample", type=int, default=1000, help="graphs refined one call each")

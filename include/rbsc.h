@@ -505,7 +505,10 @@ rbsc_status rbsc_serve_stats_get(rbsc_server* srv, rbsc_serve_stats* stats);
  * RBSC_NOALLOC_MAX_ARCS; larger graphs are rejected with RBSC_ERR_TOO_LARGE.
  * d_init_colors (may be NULL), d_out_labels (N uint32, canonical labels) and
  * d_result are device pointers; d_result is written when the kernel ends
- * (status RBSC_OK, RBSC_ERR_NOT_CONVERGED or RBSC_ERR_DEVICE).  opts may be
+ * (status RBSC_OK, RBSC_ERR_NOT_CONVERGED, RBSC_ERR_DEVICE, or RBSC_ERR_INVALID
+ * when the kernel's own check of the graph fails: offsets[0] != 0, offsets
+ * decreasing, offsets[N] != M, or a head >= N; that check runs before any read
+ * indexed by the graph, and d_out_labels is then left untouched).  opts may be
  * NULL (defaults; relabel, verify and use_graph are ignored: the kernel always
  * hashes and checks exactly).  The return value reports argument errors and
  * launch failures only; synchronise the stream before reading d_result.
@@ -514,7 +517,10 @@ rbsc_status rbsc_serve_stats_get(rbsc_server* srv, rbsc_serve_stats* stats);
  * the library, held by every GPU that loads it until the process exits, and
  * shared by all calls -- calls whose kernels overlap on the GPU race on it.
  * The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress); make that first call before any stream capture. */
+ * (cudaGetSymbolAddress) and keeps it for the life of the process; make that
+ * first call before any stream capture, and do not call this entry point on a
+ * device after cudaDeviceReset on it (the kept address may no longer be
+ * mapped). */
 #define RBSC_NOALLOC_MAX_NODES 16384u
 #define RBSC_NOALLOC_MAX_ARCS (1u << 24)
 

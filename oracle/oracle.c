@@ -768,3 +768,266 @@ int orc_refine_edge_batches(uint32_t n, const uint64_t* off, const uint32_t* idx
     free(loff); free(lidx); free(lwt); free(widx); free(considered);
     return 0;
 }
+
+/* ------------------------------------------------------------------ */
+/* workload generator and reference-format writers                     */
+/* ------------------------------------------------------------------ */
+/*
+ * The checkers and the CPU baseline build their inputs here, so that nothing
+ * that times or checks the product has to load the product library.
+ *
+ * R-MAT (Chakrabarti, Zhan, Faloutsos, SDM 2004) with counter-based draws:
+ * arc e of m0 = edge_factor * 2^scale starts from base = fmix64(seed ^ e *
+ * 0x9E3779B97F4A7C15); at level l = 0 .. scale-1 the draw r is the high 32
+ * bits of fmix64(base + (l + 1) * 0xD1B54A32D192ED03), and the quadrant bits
+ * are u_bit = (r >= T_ab), v_bit = (T_a <= r < T_ab) or (r >= T_abc), with
+ * T_x = floor(x * 2^32) (0xFFFFFFFF at the top).  Duplicate arcs and
+ * self-loops are dropped and every row is sorted by head.  These are the
+ * rules of the product's generator (gen.cu), restated, so the two produce the
+ * same graph; tests compare them.
+ */
+static uint64_t orc_fmix64(uint64_t k)
+{
+    k ^= k >> 33;
+    k *= 0xff51afd7ed558ccdULL;
+    k ^= k >> 33;
+    k *= 0xc4ceb9fe1a85ec53ULL;
+    k ^= k >> 33;
+    return k;
+}
+
+static uint32_t orc_thr(double x)
+{
+    if (x <= 0) return 0;
+    const double t = x * 4294967296.0;
+    return t >= 4294967295.0 ? 0xffffffffu : (uint32_t)t;
+}
+
+typedef struct {
+    uint64_t seed, m0;
+    uint32_t scale, ta, tab, tabc, threads;
+    uint64_t* cur;      /* [n]: row counts, then scatter cursors */
+    uint32_t* heads;    /* [m0]: raw heads by row */
+    const uint64_t* raw;/* [n + 1]: raw row offsets */
+    uint64_t* keep;     /* [n]: heads kept per row */
+    uint64_t* off;      /* [n + 1] final */
+    uint32_t* idx;      /* final heads */
+    uint64_t next;      /* row-chunk work counter */
+    int phase;
+} gen_ctx;
+
+static void orc_rmat_arc(const gen_ctx* g, uint64_t e, uint32_t* u, uint32_t* v)
+{
+    const uint64_t base = orc_fmix64(g->seed ^ (e * 0x9E3779B97F4A7C15ULL));
+    uint32_t uu = 0, vv = 0;
+    for (uint32_t l = 0; l < g->scale; ++l) {
+        const uint32_t r = (uint32_t)(orc_fmix64(base + (uint64_t)(l + 1) * 0xd1b54a32d192ed03ULL) >> 32);
+        uu = (uu << 1) | (r >= g->tab ? 1u : 0u);
+        vv = (vv << 1) | (((r >= g->ta && r < g->tab) || r >= g->tabc) ? 1u : 0u);
+    }
+    *u = uu;
+    *v = vv;
+}
+
+static int cmp_u32(const void* x, const void* y)
+{
+    const uint32_t a = *(const uint32_t*)x, b = *(const uint32_t*)y;
+    return a < b ? -1 : a > b;
+}
+
+#define GEN_ROW_CHUNK 4096u
+
+typedef struct { gen_ctx* g; uint32_t t; } gen_arg;
+
+static void* gen_worker(void* p)
+{
+    const gen_arg* a = (const gen_arg*)p;
+    gen_ctx* g = a->g;
+    const uint64_t n = 1ull << g->scale;
+    if (g->phase == 0 || g->phase == 1) {  /* count, then scatter, over this thread's arcs */
+        const uint64_t lo = g->m0 * a->t / g->threads, hi = g->m0 * (a->t + 1) / g->threads;
+        for (uint64_t e = lo; e < hi; ++e) {
+            uint32_t u, v;
+            orc_rmat_arc(g, e, &u, &v);
+            const uint64_t pos = __atomic_fetch_add(&g->cur[u], 1ull, __ATOMIC_RELAXED);
+            if (g->phase == 1) g->heads[pos] = v;
+        }
+        return NULL;
+    }
+    for (;;) {  /* rows in chunks: sort + dedup (phase 2), copy (phase 3) */
+        const uint64_t c0 = __atomic_fetch_add(&g->next, (uint64_t)GEN_ROW_CHUNK, __ATOMIC_RELAXED);
+        if (c0 >= n) break;
+        const uint64_t c1 = c0 + GEN_ROW_CHUNK < n ? c0 + GEN_ROW_CHUNK : n;
+        for (uint64_t u = c0; u < c1; ++u) {
+            uint32_t* r = g->heads + g->raw[u];
+            const uint64_t len = g->raw[u + 1] - g->raw[u];
+            if (g->phase == 2) {
+                if (len <= 32) {
+                    for (uint64_t i = 1; i < len; ++i) {
+                        const uint32_t x = r[i];
+                        uint64_t j = i;
+                        while (j > 0 && r[j - 1] > x) { r[j] = r[j - 1]; --j; }
+                        r[j] = x;
+                    }
+                } else {
+                    qsort(r, (size_t)len, sizeof(uint32_t), cmp_u32);
+                }
+                uint64_t k = 0;
+                for (uint64_t i = 0; i < len; ++i)
+                    if ((i == 0 || r[i] != r[i - 1]) && r[i] != (uint32_t)u) r[k++] = r[i];
+                g->keep[u] = k;
+            } else {
+                memcpy(g->idx + g->off[u], r, sizeof(uint32_t) * g->keep[u]);
+            }
+        }
+    }
+    return NULL;
+}
+
+static void gen_run(gen_ctx* g, int phase)
+{
+    pthread_t th[256];
+    gen_arg args[256];
+    int made[256];
+    g->phase = phase;
+    g->next = 0;
+    for (uint32_t t = 0; t < g->threads; ++t) {
+        args[t].g = g;
+        args[t].t = t;
+        made[t] = pthread_create(&th[t], NULL, gen_worker, &args[t]) == 0;
+        if (!made[t]) gen_worker(&args[t]);
+    }
+    for (uint32_t t = 0; t < g->threads; ++t)
+        if (made[t]) pthread_join(th[t], NULL);
+}
+
+/* R-MAT graph as CSR (malloc'd; release with orc_free).  Returns 0, -1 for
+ * bad sizes, -2 when memory is short. */
+int orc_gen_rmat(uint32_t scale, uint32_t edge_factor, double a, double b, double c, uint64_t seed, uint32_t threads,
+                 uint64_t** off_out, uint32_t** idx_out, uint64_t* m_out)
+{
+    *off_out = NULL;
+    *idx_out = NULL;
+    *m_out = 0;
+    if (scale < 1 || scale > 30 || edge_factor == 0) return -1;
+    if (threads < 1) threads = 1;
+    if (threads > 256) threads = 256;
+    const uint64_t n = 1ull << scale;
+    gen_ctx g;
+    memset(&g, 0, sizeof g);
+    g.seed = seed;
+    g.scale = scale;
+    g.m0 = (uint64_t)edge_factor << scale;
+    g.ta = orc_thr(a);
+    g.tab = orc_thr(a + b);
+    g.tabc = orc_thr(a + b + c);
+    g.threads = threads;
+    uint64_t* raw = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    g.cur = (uint64_t*)calloc(n, sizeof(uint64_t));
+    g.heads = (uint32_t*)malloc(sizeof(uint32_t) * g.m0);
+    g.keep = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    g.off = (uint64_t*)malloc(sizeof(uint64_t) * (n + 1));
+    if (!raw || !g.cur || !g.heads || !g.keep || !g.off) {
+        free(raw); free(g.cur); free(g.heads); free(g.keep); free(g.off);
+        return -2;
+    }
+    gen_run(&g, 0);
+    raw[0] = 0;
+    for (uint64_t u = 0; u < n; ++u) {
+        raw[u + 1] = raw[u] + g.cur[u];
+        g.cur[u] = raw[u];
+    }
+    g.raw = raw;
+    gen_run(&g, 1);
+    gen_run(&g, 2);
+    g.off[0] = 0;
+    for (uint64_t u = 0; u < n; ++u) g.off[u + 1] = g.off[u] + g.keep[u];
+    g.idx = (uint32_t*)malloc(sizeof(uint32_t) * (g.off[n] ? g.off[n] : 1));
+    if (!g.idx) {
+        free(raw); free(g.cur); free(g.heads); free(g.keep); free(g.off);
+        return -2;
+    }
+    gen_run(&g, 3);
+    free(raw); free(g.cur); free(g.heads); free(g.keep);
+    *off_out = g.off;
+    *idx_out = g.idx;
+    *m_out = g.off[n];
+    return 0;
+}
+
+void orc_free(void* p) { free(p); }
+
+static char* put_u64(char* end, uint64_t x)
+{
+    do { *--end = (char)('0' + x % 10); x /= 10; } while (x);
+    return end;
+}
+
+/* Valmari MDP text (src/part_ref/MDP_read.cc:51-63, as valmari-adapter:9-16
+ * converts arcs-cuda): "n 0 0 m nb", then one "u+1 w v+1" line per arc, then
+ * for every initial colour but the smallest its member states (1-based,
+ * increasing) followed by 0 -- block 1 is the rest (MDP_read.cc:140-150).
+ * init NULL = one block.  Returns 0 or -1. */
+int orc_write_mdp(const char* path, uint32_t n, const uint64_t* off, const uint32_t* idx, const uint64_t* wt,
+                  const uint32_t* init)
+{
+    uint32_t* colours = NULL;
+    uint32_t* order = NULL;
+    uint64_t* start = NULL;
+    uint32_t nc = 1;
+    if (init && n) {
+        colours = (uint32_t*)malloc(sizeof(uint32_t) * n);
+        if (!colours) return -1;
+        memcpy(colours, init, sizeof(uint32_t) * n);
+        qsort(colours, n, sizeof(uint32_t), cmp_u32);
+        nc = 0;
+        for (uint32_t i = 0; i < n; ++i)
+            if (i == 0 || colours[i] != colours[i - 1]) colours[nc++] = colours[i];
+        /* members per colour rank, by counting sort (increasing node id) */
+        start = (uint64_t*)calloc((size_t)nc + 1, sizeof(uint64_t));
+        order = (uint32_t*)malloc(sizeof(uint32_t) * n);
+        uint32_t* rank = (uint32_t*)malloc(sizeof(uint32_t) * n);
+        if (!start || !order || !rank) { free(colours); free(start); free(order); free(rank); return -1; }
+        for (uint32_t u = 0; u < n; ++u) {
+            uint32_t lo = 0, hi = nc;
+            while (hi - lo > 1) { const uint32_t mid = (lo + hi) / 2; if (colours[mid] <= init[u]) lo = mid; else hi = mid; }
+            rank[u] = lo;
+            ++start[lo + 1];
+        }
+        for (uint32_t r = 0; r < nc; ++r) start[r + 1] += start[r];
+        uint64_t* pos = (uint64_t*)malloc(sizeof(uint64_t) * nc);
+        if (!pos) { free(colours); free(start); free(order); free(rank); return -1; }
+        memcpy(pos, start, sizeof(uint64_t) * nc);
+        for (uint32_t u = 0; u < n; ++u) order[pos[rank[u]]++] = u;
+        free(pos);
+        free(rank);
+    }
+    FILE* f = fopen(path, "w");
+    if (!f) { free(colours); free(start); free(order); return -1; }
+    static char buf[1 << 20];
+    setvbuf(f, buf, _IOFBF, sizeof buf);
+    fprintf(f, "%u 0 0 %llu %u\n", n, (unsigned long long)(n ? off[n] : 0), nc);
+    char line[80];
+    for (uint32_t u = 0; u < n; ++u)
+        for (uint64_t k = off[u]; k < off[u + 1]; ++k) {
+            char* p = line + sizeof line;
+            *--p = '\n';
+            p = put_u64(p, (uint64_t)idx[k] + 1u);
+            *--p = ' ';
+            p = put_u64(p, wt ? wt[k] : 1u);
+            *--p = ' ';
+            p = put_u64(p, (uint64_t)u + 1u);
+            fwrite(p, 1, (size_t)(line + sizeof line - p), f);
+        }
+    for (uint32_t r = 1; init && r < nc; ++r) {
+        for (uint64_t i = start[r]; i < start[r + 1]; ++i) {
+            char* p = line + sizeof line;
+            *--p = ' ';
+            p = put_u64(p, (uint64_t)order[i] + 1u);
+            fwrite(p, 1, (size_t)(line + sizeof line - p), f);
+        }
+        fputs("0\n", f);
+    }
+    free(colours); free(start); free(order);
+    return fclose(f) == 0 ? 0 : -1;
+}

@@ -36,6 +36,20 @@ REF_RBSC = os.path.join(REF_DIR, "ref_rbsc")
 LAW_CNR2000 = os.path.join(REF_DIR, "cnr-2000.npz")
 
 
+def reference_tree() -> str | None:
+    """The reference checkout used to build oracle/_ref and the fixtures:
+    $RBSC_REFERENCE, else the location oracle/Makefile names; None when that
+    directory does not exist on this machine."""
+    ref = os.environ.get("RBSC_REFERENCE")
+    if not ref:
+        try:
+            ref = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True,
+                                 timeout=30).stdout.strip()
+        except (OSError, subprocess.SubprocessError):
+            ref = None
+    return ref if ref and os.path.isdir(ref) else None
+
+
 def prepare_law(ref: str | None) -> str | None:
     """Decodes the reference's cnr-2000 BV graph (webgraph-rs/data) into
     LAW_CNR2000, once; returns the path or None when the reference tree is
@@ -99,6 +113,14 @@ def _load():
         lib.orc_refine_edge_batches.argtypes = [ctypes.c_uint32, _u64p, _u32p, _u64p, ctypes.c_uint64, ctypes.c_int,
                                                 _u32p, _u32p, _u32p, _u32p]
         lib.orc_refine_edge_batches.restype = ctypes.c_int
+        lib.orc_gen_rmat.argtypes = [ctypes.c_uint32, ctypes.c_uint32, ctypes.c_double, ctypes.c_double,
+                                     ctypes.c_double, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_u64p),
+                                     ctypes.POINTER(_u32p), ctypes.POINTER(ctypes.c_uint64)]
+        lib.orc_gen_rmat.restype = ctypes.c_int
+        lib.orc_free.argtypes = [ctypes.c_void_p]
+        lib.orc_free.restype = None
+        lib.orc_write_mdp.argtypes = [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p]
+        lib.orc_write_mdp.restype = ctypes.c_int
         _lib = lib
     return _lib
 
@@ -269,6 +291,36 @@ def write_arcs_file(path: str, off, idx, wt=None) -> None:
     off, idx, wt = _csr(off, idx, wt)
     n = len(off) - 1
     if _load().orc_write_arcs(path.encode(), n, _p64(off), _p32(idx), _p64(wt)) != 0:
+        raise OSError(f"cannot write {path}")
+
+
+def gen_rmat(scale: int, edge_factor: int, a: float = 0.57, b: float = 0.19, c: float = 0.19, seed: int = 1,
+             threads: int | None = None):
+    """R-MAT CSR (offsets uint64, heads uint32) by oracle.c: orc_gen_rmat, the
+    same graph as the product's generator, without loading the product."""
+    lib = _load()
+    po, pi, m = _u64p(), _u32p(), ctypes.c_uint64()
+    st = lib.orc_gen_rmat(scale, edge_factor, a, b, c, seed, int(threads or os.cpu_count() or 1),
+                          ctypes.byref(po), ctypes.byref(pi), ctypes.byref(m))
+    if st != 0:
+        raise MemoryError(f"orc_gen_rmat failed ({st})")
+    n = 1 << scale
+    try:
+        off = np.ctypeslib.as_array(po, shape=(n + 1,)).copy()
+        idx = np.ctypeslib.as_array(pi, shape=(max(m.value, 1),))[: m.value].copy()
+    finally:
+        lib.orc_free(ctypes.cast(po, ctypes.c_void_p))
+        lib.orc_free(ctypes.cast(pi, ctypes.c_void_p))
+    return off, idx
+
+
+def write_mdp_file(path: str, off, idx, wt=None, init=None) -> None:
+    """Valmari MDP text of a CSR with initial colours as <blocks>, written by C
+    (oracle.c: orc_write_mdp; the same text as mdp_text without merging)."""
+    off, idx, wt = _csr(off, idx, wt)
+    n = len(off) - 1
+    init = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+    if _load().orc_write_mdp(path.encode(), n, _p64(off), _p32(idx), _p64(wt), _p32(init)) != 0:
         raise OSError(f"cannot write {path}")
 
 

@@ -21,8 +21,13 @@
 // needs at the start of every call; two calls whose kernels overlap on the GPU
 // (different streams, no ordering between them) race on it and give wrong
 // results.  The first call on a device resolves the array's device address with
-// cudaGetSymbolAddress (with that device current); make that first call before
-// any stream capture that would include it.
+// cudaGetSymbolAddress (with that device current) and keeps it until the
+// process exits; make that first call before any stream capture that would
+// include it, and make no call on a device after cudaDeviceReset on it.
+//
+// Unlike the reference (which trusts its input, rbsc.cu:156-180), the kernel
+// checks the graph before its first indexed read, as the regular path's
+// k_validate does: a malformed graph returns RBSC_ERR_INVALID in d_result.
 #include <cstring>
 #include <mutex>
 
@@ -153,6 +158,34 @@ static __global__ void __launch_bounds__(kNaThreads) k_refine_small(NaArgs a)
         }
         return;
     }
+
+    // The graph is checked before any read indexed by it: offsets[0] = 0,
+    // offsets non-decreasing, offsets[n] = m (the stated arc count, at most
+    // RBSC_NOALLOC_MAX_ARCS), every head < n.  Only then do col[idx[k]] and
+    // cnt[col[idx[k]]] stay inside the scratch array.  A malformed graph ends
+    // the call with RBSC_ERR_INVALID in d_result, nothing written to d_out.
+    if (threadIdx.x == 0) s_err = 0;
+    __syncthreads();
+    for (uint32_t u = threadIdx.x; u <= n; u += kNaThreads) {
+        const uint64_t o = na_off(a.off, a.off64, u);
+        const bool bad = (u == 0 && o != 0ull) || (u == n && o != a.m) || (u < n && o > na_off(a.off, a.off64, u + 1));
+        if (bad) s_err = 1;
+    }
+    __syncthreads();
+    if (!*(volatile uint32_t*)&s_err)
+        for (uint64_t k = threadIdx.x; k < a.m; k += kNaThreads)
+            if (a.idx[k] >= n) s_err = 1;
+    __syncthreads();
+    if (*(volatile uint32_t*)&s_err) {
+        if (threadIdx.x == 0) {
+            a.result->blocks = 0;
+            a.result->rounds = 0;
+            a.result->repairs = 0;
+            a.result->status = RBSC_ERR_INVALID;
+        }
+        return;
+    }
+    __syncthreads();
 
     // the scratch keeps the previous call's contents: clear what must start at zero
     if (threadIdx.x == 0) {

@@ -10,9 +10,10 @@ that makes it, with a checksum), the canonical labels (or their checksum), the
 block count and the round count reported by rsc (converted to the GPU
 program's convention, rbsc.cu:339).
 
-Run from the repository root (needs the reference tree, default /root/reference):
+Run from the repository root (needs the reference tree: --ref, else $RBSC_REFERENCE, else the
+location oracle/Makefile names):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py [--ref REFERENCE_CHECKOUT]
 """
 from __future__ import annotations
 
@@ -93,8 +94,9 @@ def run_both(off, idx, wt, init):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: oracle.reference_tree())")
     args = ap.parse_args()
+    args.ref = args.ref or oracle.reference_tree()
     oracle.build(ref=args.ref)
     index = {}
     for name, off, idx, wt, init in cases():

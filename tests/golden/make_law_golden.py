@@ -13,7 +13,7 @@ checksums of the decoded CSR and of the canonical labels, the block count and
 the round count (the GPU program's convention), and the programs' own
 refinement times.  Uniform initial colours: the reference programs have none.
 
-    python tests/golden/make_law_golden.py [--ref /root/reference] [--gpu]
+    python tests/golden/make_law_golden.py [--ref REFERENCE_CHECKOUT] [--gpu]
 """
 from __future__ import annotations
 
@@ -45,9 +45,10 @@ def sha(*arrays) -> str:
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="reference checkout (default: oracle.reference_tree())")
     ap.add_argument("--gpu", action="store_true", help="add the reference GPU program's output (needs a CUDA device)")
     args = ap.parse_args()
+    args.ref = args.ref or oracle.reference_tree()
     if oracle.prepare_law(args.ref) is None:
         raise SystemExit("cnr-2000 not available (no reference tree, no decoded copy)")
     off, idx = oracle.load_law()

@@ -19,7 +19,8 @@ from conftest import GOLDEN
 from oracle import oracle
 
 FX = json.load(open(os.path.join(GOLDEN, "law_cnr2000.json")))
-BV = "/root/reference/webgraph-rs/data/cnr-2000"
+_REF = oracle.reference_tree()
+BV = os.path.join(_REF, "webgraph-rs", "data", "cnr-2000") if _REF else ""
 
 
 def _sha(*arrays):
@@ -39,7 +40,8 @@ def law():
     return off, idx
 
 
-@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+@pytest.mark.skipif(not BV or not os.path.exists(BV + ".graph"),
+                    reason="reference checkout not found ($RBSC_REFERENCE, else the location oracle/Makefile names)")
 def test_bv_reader_on_the_reference_sample():
     off, idx, st = R.load_bvgraph(BV)
     assert len(off) - 1 == FX["n"] and len(idx) == FX["m"]
@@ -126,7 +128,8 @@ def _copy_bv(tmp_path, name, drop_offsets=False, drop_maxref=False, flip_at=None
     return dst
 
 
-@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+@pytest.mark.skipif(not BV or not os.path.exists(BV + ".graph"),
+                    reason="reference checkout not found ($RBSC_REFERENCE, else the location oracle/Makefile names)")
 def test_bv_reader_paths_agree(tmp_path):
     """The threaded reader (offsets file and maxrefcount present: lists
     decoded by node ranges) and the one-pass reader (no offsets file, or no
@@ -140,7 +143,8 @@ def test_bv_reader_paths_agree(tmp_path):
         assert st["offsets_checked"] == (0 if "drop_offsets" in kw else 1)
 
 
-@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+@pytest.mark.skipif(not BV or not os.path.exists(BV + ".graph"),
+                    reason="reference checkout not found ($RBSC_REFERENCE, else the location oracle/Makefile names)")
 @pytest.mark.parametrize("flip_at", [0.31, 0.77])
 def test_bv_reader_rejects_a_corrupted_stream(tmp_path, flip_at):
     for kw in ({}, {"drop_maxref": True}):
@@ -148,7 +152,8 @@ def test_bv_reader_rejects_a_corrupted_stream(tmp_path, flip_at):
             R.load_bvgraph(_copy_bv(tmp_path, f"bad_{flip_at}_{len(kw)}", flip_at=flip_at, **kw))
 
 
-@pytest.mark.skipif(not os.path.exists(BV + ".graph"), reason="reference tree not present")
+@pytest.mark.skipif(not BV or not os.path.exists(BV + ".graph"),
+                    reason="reference checkout not found ($RBSC_REFERENCE, else the location oracle/Makefile names)")
 def test_cli_reads_bv_files(tmp_path):
     """`rbsc --bv BASENAME` loads the graph from the BV files instead of
     stdin (with --csr-cache the cache is written from them); without a GPU the
