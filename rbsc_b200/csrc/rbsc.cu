@@ -1204,6 +1204,8 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_refine_persistent, kNodeThreads, 0));
     const unsigned grid = (unsigned)std::max(1, bps) * (unsigned)ctx->sm_count;
     CK(cudaMemsetAsync(g->d_gsync, 0, sizeof(GridSync), s));
+    // the persistent kernel's per-parity counters and representative flags
+    CK(cudaMemsetAsync(g->d_st->pcount, 0, sizeof g->d_st->pcount + sizeof g->d_st->prep, s));
     PersistArgs a;
     a.as = g->d_as;
     a.st = g->d_st;
@@ -1384,8 +1386,8 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
     }
     VerifyLists vl{g->d_vl8, g->d_vl32, g->d_vllong, counts};
     ++rbsc::launch_counter();
-    k_verify_classify<<<grid_for(n, 256), 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->weighted ? 1 : 0, vl, g->d_vflag,
-                                                      g->d_fail);
+    k_verify_classify<<<persistent_grid(ctx, n, 256), 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->weighted ? 1 : 0, vl,
+                                                                  g->d_vflag, g->d_fail);
     const unsigned sgrid = persistent_grid(ctx, n, 256);
     ++rbsc::launch_counter();
     k_verify_short<8><<<sgrid, 256, 0, s>>>(n, g->d_vl8, counts + 0, col, g->d_off, vstart, vidx, g->d_fail, counts + 3);

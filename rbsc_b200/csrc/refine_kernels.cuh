@@ -47,8 +47,14 @@ struct RoundState {
     uint32_t rank_bad;       // k_insert_init could not rank every class (dense ranks by scan instead)
     uint32_t pad;
     uint64_t seed;
+    uint32_t pcount[2];      // k_refine_persistent: block counts of even / odd passes
+    uint32_t prep[2];        // k_refine_persistent: rep_changed of even / odd passes
     uint32_t round_blocks[kRoundLog];
 };
+
+// The pass bodies read the pass number (and stamp) from RoundState unless the
+// caller passes its own copy (the persistent kernel keeps them per block).
+constexpr uint32_t kRoundFromState = 0xffffffffu;
 
 constexpr uint32_t kErrProbe = 1u;   // relabel table full (cannot happen at load <= 1/2)
 constexpr uint32_t kErrRounds = 2u;  // max_rounds reached
@@ -409,7 +415,8 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
                                                const ColT* __restrict__ col, Sig* __restrict__ sig,
                                                TileRange rng = TileRange{0u, 0u, nullptr, nullptr, 0ull},
                                                const uint32_t* __restrict__ hot_idx = nullptr,
-                                               const uint8_t* __restrict__ s_hot = nullptr)
+                                               const uint8_t* __restrict__ s_hot = nullptr,
+                                               uint32_t round = kRoundFromState)
 {
     static_assert(!HOT || (sizeof(ColT) == 1 && !RANGE), "hot heads: resident arcs, 1-byte ranks");
     const uint32_t lane = threadIdx.x & 31;
@@ -422,7 +429,7 @@ __device__ __forceinline__ void signature_body(const ActiveSet* __restrict__ as,
     const uint32_t* __restrict__ idx = HOT ? hot_idx : (RANGE ? rng.idx : as->idx);
     const uint64_t* __restrict__ wt = RANGE ? rng.wt : as->wt;
     const uint64_t ebase = RANGE ? rng.base : 0ull;
-    const uint64_t salt = pass_salt1(st->seed, st->round);
+    const uint64_t salt = pass_salt1(st->seed, round == kRoundFromState ? st->round : round);
     const uint32_t warps = gridDim.x * WPB;
 
     for (uint32_t tile = (RANGE ? rng.lo : 0u) + blockIdx.x * WPB + (threadIdx.x >> 5); tile < ntiles;
@@ -770,18 +777,19 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
                                                      const uint32_t* __restrict__ col,
                                                      const Sig* __restrict__ sig, Entry* __restrict__ tab,
                                                      uint32_t log2size, uint32_t* __restrict__ slot,
-                                                     uint32_t* __restrict__ joined)
+                                                     uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
+                                                     uint32_t stamp_in = 0u)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
-    const uint32_t stamp = st->stamp;
+    const uint32_t stamp = round == kRoundFromState ? st->stamp : stamp_in;
     const uint32_t hb = st->hash_bits;
     const uint64_t seed = st->seed;
     const uint32_t stride = gridDim.x * kNodeThreads;
     // probe only the first 2^k entries, 2^k >= 2 * list length: the table of
     // a late pass with few active nodes stays in L2
     const uint32_t log2win = table_window(nn, log2size);
-    const uint32_t tag = st->round + 1u;
+    const uint32_t tag = (round == kRoundFromState ? st->round : round) + 1u;
     const uint32_t lane = threadIdx.x & 31;
     uint32_t made = 0;
     // each warp takes kInsertU x 32 consecutive list entries per iteration and
@@ -1021,9 +1029,11 @@ template <bool NC>
 __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                   uint32_t* __restrict__ col, const Entry* __restrict__ tab,
                                                   const uint32_t* __restrict__ slot, Sig* __restrict__ sig,
-                                                  const uint32_t* __restrict__ joined)
+                                                  const uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
+                                                  uint32_t* __restrict__ rep_changed = nullptr)
 {
-    const uint32_t tag = st->round + 1u;
+    const uint32_t tag = (round == kRoundFromState ? st->round : round) + 1u;
+    uint32_t* const repc = rep_changed ? rep_changed : &st->rep_changed;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
     const uint32_t stride = gridDim.x * kNodeThreads;
@@ -1059,7 +1069,7 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
             }
             if (nc != c[j]) {
                 col[u[j]] = nc;
-                if (rep[j]) st->rep_changed = 1u;
+                if (rep[j]) *repc = 1u;
             }
         }
     }
@@ -1110,13 +1120,14 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_all(uint32_t n,
 // Followers (arc-less nodes that are not their group's representative) take
 // the representative's colour.  pairs[i] = (follower, representative).
 __device__ __forceinline__ void follow_body(const ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
-                                            const uint2* __restrict__ pairs, uint32_t* __restrict__ col)
+                                            const uint2* __restrict__ pairs, uint32_t* __restrict__ col,
+                                            const uint32_t* rep_changed = nullptr)
 {
     // the representatives' colours are those of their groups: they change
     // in the pass after the lists are built, and then only when a block of
     // arc-less nodes loses a member with arcs that merged into it by a hash
     // collision; nothing to copy otherwise
-    if (!*(const volatile uint32_t*)&st->rep_changed) return;
+    if (!*(const volatile uint32_t*)(rep_changed ? rep_changed : &st->rep_changed)) return;
     const uint32_t nf = as->nfollow;
     const uint32_t stride = gridDim.x * kNodeThreads;
     for (uint32_t i = blockIdx.x * kNodeThreads + threadIdx.x; i < nf; i += stride) {
@@ -1685,6 +1696,14 @@ __device__ __forceinline__ void clear_table_body(const RoundState* __restrict__ 
     }
 }
 
+__device__ __forceinline__ void clear_table_all(Entry* __restrict__ tab, uint64_t entries)
+{
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < entries; i += (uint64_t)gridDim.x * blockDim.x) {
+        tab[i].k1 = 0ull;
+        tab[i].hi = 0ull;
+    }
+}
+
 static __global__ void k_clear_table(const RoundState* __restrict__ st, Entry* __restrict__ tab, uint64_t entries)
 {
     clear_table_body(st, tab, entries);
@@ -1747,26 +1766,64 @@ struct PersistArgs {
     uint32_t* joined;
 };
 
+// Per pass: [table clear when the stamp wrapped] + signatures | inserts |
+// relabel | [followers, only when a representative changed], three grid
+// barriers (four with followers).  The clear may share the signature phase:
+// the signatures do not touch the table, and the barrier after them orders
+// the clear before every insert.  The end-of-pass decision (blocks counted,
+// fixpoint, round limit) is taken by every block from its own copy of the pass
+// state (round, stamp, previous count) and the counter of the pass, which is
+// final after the insert barrier; counters and the representative flag come
+// in pairs by pass parity, so block 0 can reset the next pass's pair while
+// other blocks still read this pass's.  Block 0 mirrors the state into
+// RoundState for the host.
 static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
 {
     static_assert(kNodeThreads == kTileThreads, "the signature phase runs one tile per warp");
     __shared__ BlockReserveSmem<kNodeThreads> sm;
+    RoundState* st = a.st;
+    uint32_t round = st->round, stamp = st->stamp, prev = st->prev;
+    bool clear = st->clear_pending != 0u;
+    const uint32_t max_rounds = st->max_rounds;
+    const uint32_t retired = a.as->retired;
+    const TileRange all{0u, 0u, nullptr, nullptr, 0ull};
     for (;;) {
-        clear_table_body(a.st, a.tab, a.tab_entries);
-        if (!grid_barrier(a.gs, a.st)) return;
-        if (a.weighted) signature_body<true, uint32_t, false>(a.as, a.st, a.col, a.sig);
-        else signature_body<false, uint32_t, false>(a.as, a.st, a.col, a.sig);
-        if (!grid_barrier(a.gs, a.st)) return;
-        const uint32_t made = insert_list_body(a.as, a.st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined);
-        block_count<kNodeThreads>(made, &a.st->count, sm);
-        if (!grid_barrier(a.gs, a.st)) return;
-        relabel_list_body<false>(a.as, a.st, a.col, a.tab, a.slot, a.sig, a.joined);
-        if (!grid_barrier(a.gs, a.st)) return;
-        follow_body(a.as, a.st, a.pairs, a.col);
-        if (!grid_barrier(a.gs, a.st)) return;
-        if (blockIdx.x == 0 && threadIdx.x == 0) fixpoint_body<kFixHash>(a.st, a.as, 1);
-        if (!grid_barrier(a.gs, a.st)) return;
-        if (*(volatile uint32_t*)&a.st->done || *(volatile uint32_t*)&a.st->error) return;
+        const uint32_t p = round & 1u;
+        if (clear) clear_table_all(a.tab, a.tab_entries);
+        if (a.weighted) signature_body<true, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
+        else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
+        if (!grid_barrier(a.gs, st)) return;
+        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp);
+        block_count<kNodeThreads>(made, &st->pcount[p], sm);
+        if (!grid_barrier(a.gs, st)) return;
+        relabel_list_body<false>(a.as, st, a.col, a.tab, a.slot, a.sig, a.joined, round, &st->prep[p]);
+        if (!grid_barrier(a.gs, st)) return;
+        if (*(volatile uint32_t*)&st->prep[p]) {
+            follow_body(a.as, st, a.pairs, a.col, &st->prep[p]);
+            if (!grid_barrier(a.gs, st)) return;
+        }
+        const uint32_t cnt = *(volatile uint32_t*)&st->pcount[p] + retired;
+        const bool done = cnt == prev;
+        ++round;
+        prev = cnt;
+        stamp = stamp % 255u + 1u;
+        clear = stamp == 1u;
+        const bool over = !done && round >= max_rounds;
+        const bool err = *(volatile uint32_t*)&st->error != 0u;
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            st->round = round;
+            if (round < kRoundLog) st->round_blocks[round] = cnt;
+            st->prev = cnt;
+            st->stamp = stamp;
+            st->clear_pending = clear ? 1u : 0u;
+            st->count = 0u;
+            st->rep_changed = 0u;
+            st->pcount[p ^ 1u] = 0u;
+            st->prep[p ^ 1u] = 0u;
+            if (done) st->done = 1u;
+            if (over) atomicOr(&st->error, kErrRounds);
+        }
+        if (done || over || err) return;
     }
 }
 

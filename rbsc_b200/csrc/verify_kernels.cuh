@@ -34,40 +34,54 @@ struct VerifyLists {
 // Classifies every node against its block's representative r (the block's
 // smallest node): quick failures (initial colour, row length), empty rows
 // (equal), short rows (lists l8 / l32), long or weighted rows (list llong;
-// their and r's rows are flagged for the global path in vflag).
-static __global__ void k_verify_classify(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ initlab,
-                                         const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
-                                         uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
+// their and r's rows are flagged for the global path in vflag).  Grid-stride
+// over the nodes with the list appends buffered per block (BlockAppend): one
+// reservation per kVerifyBuf listed nodes instead of one per 256 nodes, which
+// on a grid of one block per 256 nodes serialised in L2 on the three counters.
+constexpr int kVerifyBuf = 2048;
+
+static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, const uint32_t* __restrict__ col,
+                                                                const uint32_t* __restrict__ initlab,
+                                                                const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
+                                                                uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
 {
-    const uint32_t u = blockIdx.x * blockDim.x + threadIdx.x;
-    bool t8 = false, t32 = false, tl = false, bad = false;
-    if (u < n) {
-        const uint32_t c = col[u];
-        const uint32_t r = c & kLabelMask;
-        if (!(c & kSingleton) && r != u) {
-            const uint64_t du = off[u + 1] - off[u], dr = off[r + 1] - off[r];
-            if (initlab[u] != initlab[r]) bad = true;
-            else if (weighted) tl = du > 0 || dr > 0;
-            else if (du != dr) bad = true;
-            else if (du == 0) {}
-            else if (du <= 8) t8 = true;
-            else if (du <= 32) t32 = true;
-            else tl = true;
-            if (tl) {
-                vflag[u] = 1u;
-                vflag[r] = 1u;
-            }
-            if (bad) fail[u] = 1u;
-        }
-    }
+    __shared__ BlockAppend<uint32_t, kVerifyBuf, 256> s8, s32, sl;
     __shared__ BlockReserveSmem<256> sm;
-    uint32_t p = block_reserve<256>(t8, &vl.counts[0], sm);
-    if (t8) vl.l8[p] = u;
-    p = block_reserve<256>(t32, &vl.counts[1], sm);
-    if (t32) vl.l32[p] = u;
-    p = block_reserve<256>(tl, &vl.counts[2], sm);
-    if (tl) vl.llong[p] = u;
-    block_count<256>(bad ? 1u : 0u, &vl.counts[3], sm);
+    block_append_begin(s8);
+    block_append_begin(s32);
+    block_append_begin(sl);
+    uint32_t nbad = 0;
+    for (uint32_t base = blockIdx.x * 256u; base < n; base += gridDim.x * 256u) {
+        const uint32_t u = base + threadIdx.x;
+        bool t8 = false, t32 = false, tl = false, bad = false;
+        if (u < n) {
+            const uint32_t c = col[u];
+            const uint32_t r = c & kLabelMask;
+            if (!(c & kSingleton) && r != u) {
+                const uint64_t du = off[u + 1] - off[u], dr = off[r + 1] - off[r];
+                if (initlab[u] != initlab[r]) bad = true;
+                else if (weighted) tl = du > 0 || dr > 0;
+                else if (du != dr) bad = true;
+                else if (du == 0) {}
+                else if (du <= 8) t8 = true;
+                else if (du <= 32) t32 = true;
+                else tl = true;
+                if (tl) {
+                    vflag[u] = 1u;
+                    vflag[r] = 1u;
+                }
+                if (bad) fail[u] = 1u;
+            }
+        }
+        block_append(s8, t8, u, &vl.counts[0], vl.l8);
+        block_append(s32, t32, u, &vl.counts[1], vl.l32);
+        block_append(sl, tl, u, &vl.counts[2], vl.llong);
+        nbad += bad ? 1u : 0u;
+    }
+    block_append_flush(s8, &vl.counts[0], vl.l8);
+    block_append_flush(s32, &vl.counts[1], vl.l32);
+    block_append_flush(sl, &vl.counts[2], vl.llong);
+    block_count<256>(nbad, &vl.counts[3], sm);
 }
 
 // Bitonic sort of one value per lane across aligned groups of G lanes.
