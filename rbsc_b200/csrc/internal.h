@@ -101,6 +101,7 @@ struct rbsc_graph {
     uint64_t* d_vdeg = nullptr;
     uint64_t* d_vstart = nullptr;    // exact check: row starts in the compacted active set
     uint32_t* d_fail = nullptr;
+    bool verify_dirty = false;  // d_vflag / d_fail may hold flags (they are zero between checks otherwise)
     unsigned long long* d_keys[2] = {nullptr, nullptr};
     unsigned long long* d_vals[2] = {nullptr, nullptr};
     uint64_t key_cap = 0;

@@ -1360,12 +1360,19 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
         CKS(dev_alloc(ctx, (void**)&g->d_vl8, 4 * ((size_t)n + 1)));
         CKS(dev_alloc(ctx, (void**)&g->d_vl32, 4 * ((size_t)n + 1)));
         CKS(dev_alloc(ctx, (void**)&g->d_vllong, 4 * ((size_t)n + 1)));
+        // zero between checks from here on: a check that sets flags clears
+        // them after use (the long-row path below, the repair pass)
+        CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), ctx->stream));
+        CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), ctx->stream));
     }
     uint32_t* counts = reinterpret_cast<uint32_t*>(g->d_small);          // [0..3] list sizes, failures
     uint64_t* tot = reinterpret_cast<uint64_t*>(g->d_small) + 4;          // [0] rows, [1] keys of the global path
     CK(cudaMemsetAsync(g->d_small, 0, 64, s));
-    CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), s));
-    CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
+    if (g->verify_dirty) {  // a check or repair that ended early left flags set
+        CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), s));
+        CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));
+    }
+    g->verify_dirty = true;
     // the arc view: the graph's own arrays, or -- when those are in host
     // memory and the active set was compacted into device memory -- the
     // compacted rows (every row the check reads is among them)
@@ -1449,10 +1456,12 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
         k_verify_compare<<<cgrid, 256, 0, s>>>(g->d_vllong, counts + 2, col, g->d_initlab, g->d_off, g->d_vdeg, keys, vals,
                                                g->d_fail, counts + 3);
         CK(cudaGetLastError());
+        CK(cudaMemsetAsync(g->d_vflag, 0, 4 * ((size_t)n + 1), s));
         CK(cudaMemcpyAsync(hc, counts, sizeof hc, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
     }
     *nfail = hc[3];
+    g->verify_dirty = hc[3] != 0;  // failure flags stay set for the repair pass
     return RBSC_OK;
 }
 
@@ -1468,6 +1477,8 @@ static rbsc_status repair_pass(rbsc_ctx* ctx, rbsc_graph* g)
     ++rbsc::launch_counter();
     k_insert_all<kModeRepair><<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_st, g->d_col[0], g->d_fail,
                                                                                              g->d_tab, g->log2tab, g->d_slot);
+    CK(cudaMemsetAsync(g->d_fail, 0, 4 * ((size_t)n + 1), s));  // the failure flags are consumed
+    g->verify_dirty = false;
     ++rbsc::launch_counter();
     k_relabel_all<<<persistent_grid(ctx, n, kNodeThreads), kNodeThreads, 0, s>>>(n, g->d_col[0], g->d_tab, g->d_slot, nullptr);
     ++rbsc::launch_counter();

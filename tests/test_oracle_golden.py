@@ -61,3 +61,25 @@ def test_randomize_is_the_reference_mixer():
         return (((z << 7) | (z >> 57)) & M) * 9 & M
     for x in (0, 1, 2, 12345, (1 << 63) + 7, (1 << 64) - 1):
         assert oracle.rsc_randomize(x) == ref(x)
+
+
+@pytest.mark.parametrize("scale,ef,seed", [(6, 2, 1), (10, 8, 5), (14, 16, 1), (16, 16, 3)])
+def test_oracle_rmat_generator_equals_the_products(scale, ef, seed):
+    """The oracle's R-MAT (oracle.c: orc_gen_rmat) builds the workloads of the
+    reference arm and of the config-scale fixtures without the product; it
+    must give the product generator's graph bit for bit."""
+    import rbsc_b200 as R
+    off, idx = oracle.gen_rmat(scale, ef, seed=seed, threads=3)
+    o2, i2 = R.gen_rmat_host(scale, ef, seed=seed)
+    assert np.array_equal(off, np.asarray(o2, dtype=np.uint64)) and np.array_equal(idx, i2)
+
+
+def test_mdp_writer_equals_the_python_text(tmp_path):
+    from rbsc_b200 import graphs as G
+    off, idx = G.rmat(9, 4, seed=2)
+    init = np.random.default_rng(3).integers(0, 5, size=len(off) - 1).astype(np.uint32)
+    wt = np.random.default_rng(4).integers(1, 9, size=len(idx)).astype(np.uint64)
+    for w, i in ((None, None), (wt, None), (None, init), (wt, init)):
+        p = str(tmp_path / "g.txt")
+        oracle.write_mdp_file(p, off, idx, wt=w, init=i)
+        assert open(p, "rb").read() == oracle.mdp_text(off, idx, w, i)
