@@ -347,7 +347,7 @@ def run_ours(args, rank, world, local_rank):
         times, pr = g.profile(d_init.data_ptr())
         if rank == 0:
             print(json.dumps({"profile_refine": config(n, m, args.scale, args.ef), "rounds": pr.rounds,
-                              "device_ms": pr.device_ms,
+                              "device_ms": pr.device_ms, "round_blocks": list(pr.round_blocks),
                               "times": times}))
         g.free()
         ctx.close()
@@ -609,6 +609,50 @@ def served_pool(args):
     return pool
 
 
+def served_breakdown(ctx, pool, pick):
+    """Where a one-graph-per-call refinement of the served mix spends its time,
+    per request of the stream (pool graphs weighted by how often they are
+    drawn): wall time of the call, device time of the refinement, host-link
+    copies (bytes and time), the rest on the host.  From it, two floors of any
+    server on one GPU fed from host memory: every request's bytes must cross
+    the host link (measured copy bandwidth), and every refinement must run on
+    the device; the served throughput cannot exceed the smaller of the two."""
+    import numpy as np
+    import torch
+    hbuf = torch.empty(1 << 28, dtype=torch.int32, pin_memory=True)
+    dbuf = torch.empty(1 << 28, dtype=torch.int32, device="cuda")
+    bw = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        dbuf.copy_(hbuf, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        bw.append(4.0 * (1 << 28) / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    del hbuf, dbuf
+    link = max(bw)
+    rows = {}
+    for k in sorted(set(pick.tolist())):
+        _, off, idx = pool[k]
+        ctx.refine(off, idx)
+        ts = [ctx.refine(off, idx) for _ in range(3)]
+        r = min(ts, key=lambda x: x.time_s)
+        rows[k] = (1e3 * r.time_s, r.device_ms, r.h2d_ms, r.d2h_ms, r.h2d_bytes + r.d2h_bytes)
+    w = np.array([rows[int(k)] for k in pick])
+    wall, dev, h2d, d2h, nbytes = (float(x) for x in w.mean(axis=0))
+    link_ms = nbytes / (link * 1e9) * 1e3
+    out = {"per_request_mean": {"wall_ms": wall, "device_ms": dev, "h2d_ms": h2d, "d2h_ms": d2h,
+                                "host_ms": max(0.0, wall - dev - h2d - d2h), "bytes": nbytes},
+           "host_link_gbs_measured": link,
+           "floor_ms_per_request": {"host_link": link_ms, "device": dev},
+           "bound_graphs_per_s": 1e3 / max(link_ms, dev),
+           "one_per_call_graphs_per_s": 1e3 / wall,
+           "note": "device_ms is the refinement's device time with the call's own copies outside it; the bound "
+                   "assumes perfect overlap of copies and refinements across requests"}
+    out["bound_speedup_vs_one_per_call"] = out["bound_graphs_per_s"] / out["one_per_call_graphs_per_s"]
+    return out
+
+
 def run_served(args, world, dist, local_rank):
     """Served refinement (the served-stream configuration): a Poisson stream of
     requests drawn from a pool of seeded graphs, through a server with
@@ -630,6 +674,7 @@ def run_served(args, world, dist, local_rank):
         for k in sorted(set(pick.tolist())):
             _, off, idx = pool[k]
             ref[k] = c.refine(off, idx)
+        breakdown = served_breakdown(c, pool, pick)
 
     def start(slots, pack):
         kw = dict(slots=slots) if pack else dict(slots=slots, pack_max_graphs=1)
@@ -682,6 +727,7 @@ def run_served(args, world, dist, local_rank):
            "paths": {"served": "rbsc_serve_submit / rbsc_serve_wait: several slots, packing, footprint admission",
                      "serial": "the same server with one slot and no packing: one rbsc_refine per request in order"}}
     out["saturated_speedup"] = out["served_saturated"]["graphs_per_s"] / out["serial_saturated"]["graphs_per_s"]
+    out["breakdown"] = breakdown
     return out
 
 

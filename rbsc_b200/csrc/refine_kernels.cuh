@@ -1766,6 +1766,86 @@ struct PersistArgs {
     uint32_t* joined;
 };
 
+// Signatures of the small tail, one row per lane: a warp takes 32 consecutive
+// rows of the active arc set; each lane folds its row's arcs (rows of at most
+// kRowLong arcs), and the rows longer than that are folded by the whole warp
+// afterwards, one at a time (a strided loop and a shuffle reduction).  The
+// sums are the tiled kernel's (wrap-around sums of the same per-arc terms, in
+// another order), and every row is written whole, with no atomics.  Few
+// registers: the persistent kernel that runs it keeps more warps resident than
+// one built around the 16-arcs-per-lane tile fold.  Colours are read at L2:
+// the same launch rewrites them between its phases.
+constexpr uint32_t kRowLong = 32;
+constexpr int kPersistBlocksPerSM = 4;  // 4 x 256 threads resident per SM (64 registers, no spills)
+
+template <bool WEIGHTED>
+__device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__ as, const uint32_t* __restrict__ col,
+                                                   Sig* __restrict__ sig, uint64_t salt)
+{
+    const uint32_t K = as->K;
+    const bool r64 = as->roff64 != 0;
+    const uint64_t* __restrict__ roff64 = reinterpret_cast<const uint64_t*>(as->roff);
+    const uint32_t* __restrict__ roff32 = reinterpret_cast<const uint32_t*>(as->roff);
+    const uint32_t* __restrict__ rows = as->rows;
+    const uint32_t* __restrict__ idx = as->idx;
+    const uint64_t* __restrict__ wt = as->wt;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t wpb = blockDim.x >> 5;
+    const uint32_t nwarps = gridDim.x * wpb;
+    for (uint32_t base = (blockIdx.x * wpb + (threadIdx.x >> 5)) * 32u; base < K; base += nwarps * 32u) {
+        const uint32_t k = base + lane;
+        uint64_t b = 0, e = 0;
+        if (k < K) {
+            b = r64 ? roff64[k] : (uint64_t)roff32[k];
+            e = r64 ? roff64[k + 1] : (uint64_t)roff32[k + 1];
+        }
+        const bool longrow = e - b > kRowLong;
+        if (k < K && !longrow) {
+            uint64_t s1 = 0;
+            uint32_t s2 = 0;
+            for (uint64_t a = b; a < e; ++a) {
+                uint64_t t1;
+                uint32_t t2;
+                arc_terms(__ldcg(col + idx[a]), salt, t1, t2);
+                if (WEIGHTED) {
+                    const uint64_t w = wt[a];
+                    t1 *= w;
+                    t2 *= (uint32_t)w;
+                }
+                s1 += t1;
+                s2 += t2;
+            }
+            sig_store(&sig[rows[k]], s1, s2);
+        }
+        unsigned lm = __ballot_sync(0xffffffffu, k < K && longrow);
+        while (lm) {
+            const int src = __ffs(lm) - 1;
+            lm &= lm - 1u;
+            const uint64_t bb = __shfl_sync(0xffffffffu, b, src), ee = __shfl_sync(0xffffffffu, e, src);
+            uint64_t s1 = 0;
+            uint32_t s2 = 0;
+            for (uint64_t a = bb + lane; a < ee; a += 32) {
+                uint64_t t1;
+                uint32_t t2;
+                arc_terms(__ldcg(col + idx[a]), salt, t1, t2);
+                if (WEIGHTED) {
+                    const uint64_t w = wt[a];
+                    t1 *= w;
+                    t2 *= (uint32_t)w;
+                }
+                s1 += t1;
+                s2 += t2;
+            }
+#pragma unroll
+            for (int d = 16; d > 0; d >>= 1) {
+                s1 += __shfl_xor_sync(0xffffffffu, s1, d);
+                s2 += __shfl_xor_sync(0xffffffffu, s2, d);
+            }
+            if (lane == (uint32_t)src) sig_store(&sig[rows[k]], s1, s2);
+        }
+    }
+}
+
 // Per pass: [table clear when the stamp wrapped] + signatures | inserts |
 // relabel | [followers, only when a representative changed], three grid
 // barriers (four with followers).  The clear may share the signature phase:
@@ -1777,21 +1857,20 @@ struct PersistArgs {
 // in pairs by pass parity, so block 0 can reset the next pass's pair while
 // other blocks still read this pass's.  Block 0 mirrors the state into
 // RoundState for the host.
-static __global__ void __launch_bounds__(kNodeThreads, 3) k_refine_persistent(PersistArgs a)
+static __global__ void __launch_bounds__(kNodeThreads, kPersistBlocksPerSM) k_refine_persistent(PersistArgs a)
 {
-    static_assert(kNodeThreads == kTileThreads, "the signature phase runs one tile per warp");
     __shared__ BlockReserveSmem<kNodeThreads> sm;
     RoundState* st = a.st;
     uint32_t round = st->round, stamp = st->stamp, prev = st->prev;
     bool clear = st->clear_pending != 0u;
     const uint32_t max_rounds = st->max_rounds;
     const uint32_t retired = a.as->retired;
-    const TileRange all{0u, 0u, nullptr, nullptr, 0ull};
+    const uint64_t seed = st->seed;
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
-        if (a.weighted) signature_body<true, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
-        else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
+        if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
+        else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
         if (!grid_barrier(a.gs, st)) return;
         const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);

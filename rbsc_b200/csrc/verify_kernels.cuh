@@ -31,28 +31,56 @@ struct VerifyLists {
     uint32_t* counts; // [0] = |l8|, [1] = |l32|, [2] = |llong|, [3] = failures
 };
 
+// Warp-private buffered append: a warp gathers its flagged values in a
+// shared-memory buffer of kWarpBuf entries and reserves space in the global
+// list (one atomicAdd by lane 0) only when the buffer could overflow and at
+// the end.  No block barrier: only the warp's own lanes take part.
+constexpr uint32_t kWarpBuf = 256;
+
+__device__ __forceinline__ void warp_append_flush(uint32_t* buf, uint32_t& cnt, uint32_t* counter, uint32_t* out)
+{
+    __syncwarp();
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0 && cnt) base = atomicAdd(counter, cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < cnt; i += 32) out[base + i] = buf[i];
+    __syncwarp();
+    cnt = 0;
+}
+
+__device__ __forceinline__ void warp_append(bool take, uint32_t v, uint32_t* buf, uint32_t& cnt, uint32_t* counter,
+                                            uint32_t* out)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    if (cnt + 32u > kWarpBuf) warp_append_flush(buf, cnt, counter, out);  // warp-uniform
+    if (take) buf[cnt + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
+    cnt += (uint32_t)__popc(m);
+}
+
 // Classifies every node against its block's representative r (the block's
 // smallest node): quick failures (initial colour, row length), empty rows
 // (equal), short rows (lists l8 / l32), long or weighted rows (list llong;
 // their and r's rows are flagged for the global path in vflag).  Grid-stride
-// over the nodes with the list appends buffered per block (BlockAppend): one
-// reservation per kVerifyBuf listed nodes instead of one per 256 nodes, which
-// on a grid of one block per 256 nodes serialised in L2 on the three counters.
-constexpr int kVerifyBuf = 2048;
-
+// by warps, 32 consecutive nodes per warp and step, list appends buffered per
+// warp (warp_append): a global counter is touched once per ~kWarpBuf listed
+// nodes, and no block-wide barrier is needed.
 static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, const uint32_t* __restrict__ col,
                                                                 const uint32_t* __restrict__ initlab,
                                                                 const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
                                                                 uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
 {
-    __shared__ BlockAppend<uint32_t, kVerifyBuf, 256> s8, s32, sl;
-    __shared__ BlockReserveSmem<256> sm;
-    block_append_begin(s8);
-    block_append_begin(s32);
-    block_append_begin(sl);
-    uint32_t nbad = 0;
-    for (uint32_t base = blockIdx.x * 256u; base < n; base += gridDim.x * 256u) {
-        const uint32_t u = base + threadIdx.x;
+    __shared__ uint32_t s_buf[256 / 32][3][kWarpBuf];
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* b8 = s_buf[warp][0];
+    uint32_t* b32 = s_buf[warp][1];
+    uint32_t* bl = s_buf[warp][2];
+    uint32_t c8 = 0, c32 = 0, cl = 0, nbad = 0;
+    const uint32_t nwarps = gridDim.x * (256u / 32u);
+    for (uint32_t base = (blockIdx.x * (256u / 32u) + warp) * 32u; base < n; base += nwarps * 32u) {
+        const uint32_t u = base + lane;
         bool t8 = false, t32 = false, tl = false, bad = false;
         if (u < n) {
             const uint32_t c = col[u];
@@ -73,15 +101,16 @@ static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, cons
                 if (bad) fail[u] = 1u;
             }
         }
-        block_append(s8, t8, u, &vl.counts[0], vl.l8);
-        block_append(s32, t32, u, &vl.counts[1], vl.l32);
-        block_append(sl, tl, u, &vl.counts[2], vl.llong);
+        warp_append(t8, u, b8, c8, &vl.counts[0], vl.l8);
+        warp_append(t32, u, b32, c32, &vl.counts[1], vl.l32);
+        warp_append(tl, u, bl, cl, &vl.counts[2], vl.llong);
         nbad += bad ? 1u : 0u;
     }
-    block_append_flush(s8, &vl.counts[0], vl.l8);
-    block_append_flush(s32, &vl.counts[1], vl.l32);
-    block_append_flush(sl, &vl.counts[2], vl.llong);
-    block_count<256>(nbad, &vl.counts[3], sm);
+    warp_append_flush(b8, c8, &vl.counts[0], vl.l8);
+    warp_append_flush(b32, c32, &vl.counts[1], vl.l32);
+    warp_append_flush(bl, cl, &vl.counts[2], vl.llong);
+    nbad = __reduce_add_sync(0xffffffffu, nbad);
+    if (lane == 0 && nbad) atomicAdd(&vl.counts[3], nbad);
 }
 
 // Bitonic sort of one value per lane across aligned groups of G lanes.
