@@ -1228,7 +1228,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet
 // past the current set's row count is not written.
 constexpr int kCompactRows = 8;
 
-static __global__ void __launch_bounds__(kNodeThreads) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
+static __global__ void __launch_bounds__(kNodeThreads, 4) k_compact_rows(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
     constexpr int W = kNodeThreads / 32;
@@ -1351,7 +1351,7 @@ static __global__ void k_compact_decide(ActiveSet* as, const RoundState* st, Com
 // entering the split list gets its signatures zeroed here.  COPY false: the
 // bookkeeping only (the arcs were copied by k_compact_copy_tiles).
 template <bool COPY>
-static __global__ void __launch_bounds__(kNodeThreads) k_compact_arcs(ActiveSet* __restrict__ as, CompactBufs bufs,
+static __global__ void __launch_bounds__(kNodeThreads, 4) k_compact_arcs(ActiveSet* __restrict__ as, CompactBufs bufs,
                                                                       Sig* __restrict__ sig)
 {
     if (!as->do_copy) return;
