@@ -62,7 +62,8 @@ class Opts(ctypes.Structure):
         ("grid_per_sm", ctypes.c_int32),
         ("sig_kernel", ctypes.c_int32),
         ("hot_log2", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 2),
+        ("persist_bps", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 1),
     ]
 
 

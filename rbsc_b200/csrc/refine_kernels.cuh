@@ -45,7 +45,7 @@ struct RoundState {
     uint32_t handoff;        // the active set is small: the persistent kernel takes over
     uint32_t ranks;          // initial classes given a dense rank by k_insert_init
     uint32_t rank_bad;       // k_insert_init could not rank every class (dense ranks by scan instead)
-    uint32_t pad;
+    uint32_t active_nodes;   // listed nodes after the last compaction (sizes the persistent kernel's grid)
     uint64_t seed;
     uint32_t pcount[2];      // k_refine_persistent: block counts of even / odd passes
     uint32_t prep[2];        // k_refine_persistent: rep_changed of even / odd passes
@@ -1526,6 +1526,7 @@ static __global__ void k_compact_finalize(ActiveSet* as, RoundState* st, Compact
     as->splitctr = 0;
     const bool small = handoff_arcs > 0 && as->m <= handoff_arcs && as->nnodes <= handoff_nodes;
     st->handoff = small ? 1u : 0u;
+    st->active_nodes = as->nnodes;
     if (use_handle) cudaGraphSetConditional(handle, small ? 0u : 1u);
 }
 
