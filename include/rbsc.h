@@ -86,8 +86,7 @@ typedef struct {
     int32_t hot_log2;         /* hot heads: at most 2^hot_log2 nodes, those with the
                                  most in-arcs (0 = default 17; 10..17)                  */
     int32_t persist_bps;      /* blocks of 256 threads per SM of the persistent tail
-                                 kernel (0 = from the active set's size: about 8 listed
-                                 nodes per thread, at least 1, at most what fits)       */
+                                 kernel (0 = as many as fit, 4 on a B200)                */
     int32_t reserved[1];
 } rbsc_opts;
 

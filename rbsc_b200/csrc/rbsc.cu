@@ -1203,14 +1203,10 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     int bps = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_refine_persistent, kNodeThreads, 0));
     bps = std::max(1, bps);
-    // more blocks hide more latency in the phases, fewer make every grid
-    // barrier cheaper: about 8 listed nodes per thread, unless the options
-    // fix the count
-    int want = ctx->opts.persist_bps;
-    if (want <= 0) {
-        const uint64_t per_sm_block = (uint64_t)ctx->sm_count * kNodeThreads * 8u;
-        want = (int)std::max<uint64_t>(1, ceil_div<uint64_t>(g->h_st->active_nodes, per_sm_block));
-    }
+    // as many blocks as fit (measured best on R-MAT-24 and cnr-2000: the
+    // phases are latency-bound, and fewer blocks do not make the barriers
+    // cheap enough to pay for it), unless the options fix the count
+    const int want = ctx->opts.persist_bps > 0 ? ctx->opts.persist_bps : bps;
     const unsigned grid = (unsigned)std::min(bps, want) * (unsigned)ctx->sm_count;
     CK(cudaMemsetAsync(g->d_gsync, 0, sizeof(GridSync), s));
     // the persistent kernel's per-parity counters and representative flags

@@ -1768,8 +1768,8 @@ struct PersistArgs {
 };
 
 // Signatures of the small tail, one row per lane: a warp takes 32 consecutive
-// rows of the active arc set; each lane folds its row's arcs (rows of at most
-// kRowLong arcs), and the rows longer than that are folded by the whole warp
+// rows of the active arc set; each lane folds its row's arcs four at a time
+// (rows of at most kRowLong arcs), and the rows longer than that are folded by the whole warp
 // afterwards, one at a time (a strided loop and a shuffle reduction).  The
 // sums are the tiled kernel's (wrap-around sums of the same per-arc terms, in
 // another order), and every row is written whole, with no atomics.  Few
@@ -1804,17 +1804,28 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
         if (k < K && !longrow) {
             uint64_t s1 = 0;
             uint32_t s2 = 0;
-            for (uint64_t a = b; a < e; ++a) {
-                uint64_t t1;
-                uint32_t t2;
-                arc_terms(__ldcg(col + idx[a]), salt, t1, t2);
-                if (WEIGHTED) {
-                    const uint64_t w = wt[a];
-                    t1 *= w;
-                    t2 *= (uint32_t)w;
+            // four arcs at a time: their head loads, then their colour loads,
+            // are issued side by side (one dependent pair per four arcs)
+            for (uint64_t a = b; a < e; a += 4) {
+                uint32_t h[4], c[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) h[j] = a + j < e ? idx[a + j] : 0u;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) c[j] = a + j < e ? __ldcg(col + h[j]) : 0u;
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    if (a + j >= e) break;
+                    uint64_t t1;
+                    uint32_t t2;
+                    arc_terms(c[j], salt, t1, t2);
+                    if (WEIGHTED) {
+                        const uint64_t w = wt[a + j];
+                        t1 *= w;
+                        t2 *= (uint32_t)w;
+                    }
+                    s1 += t1;
+                    s2 += t2;
                 }
-                s1 += t1;
-                s2 += t2;
             }
             sig_store(&sig[rows[k]], s1, s2);
         }
