@@ -86,8 +86,11 @@ typedef struct {
     int32_t hot_log2;         /* hot heads: at most 2^hot_log2 nodes, those with the
                                  most in-arcs (0 = default 17; 10..17)                  */
     int32_t persist_bps;      /* blocks of 256 threads per SM of the persistent tail
-                                 kernel (0 = as many as fit, 4 on a B200)                */
-    int32_t reserved[1];
+                                 kernel (0 = as many as fit)                            */
+    int32_t persist_sig;      /* signature phase of the persistent tail kernel: 0 = by
+                                 the active rows' mean length (one row per lane for
+                                 short rows, 4 blocks per SM; 512-arc tiles per warp
+                                 otherwise, 3 blocks per SM), 1 = rows, 2 = tiles      */
 } rbsc_opts;
 
 typedef struct {

@@ -105,7 +105,7 @@ class Context:
     def __init__(self, device: int = 0, relabel: int = RELABEL_HASH, verify: bool = True, max_rounds: int = 0,
                  use_graph: bool = True, seed: int = 0x5EED5EED12345678, test_hash_bits: int = 0,
                  persistent: bool = True, persist_log2: int = 0, grid_per_sm: int = 0, sig_kernel: int = 0,
-                 hot_log2: int = 0, persist_bps: int = 0):
+                 hot_log2: int = 0, persist_bps: int = 0, persist_sig: int = 0):
         self._lib = _lib.load()
         o = _lib.Opts()
         self._lib.rbsc_opts_default(ctypes.byref(o))
@@ -121,6 +121,7 @@ class Context:
         o.sig_kernel = sig_kernel
         o.hot_log2 = hot_log2
         o.persist_bps = persist_bps
+        o.persist_sig = persist_sig
         self._opts = o
         h = self._lib.rbsc_ctx_create(device, ctypes.byref(o))
         if not h:

@@ -63,7 +63,7 @@ class Opts(ctypes.Structure):
         ("sig_kernel", ctypes.c_int32),
         ("hot_log2", ctypes.c_int32),
         ("persist_bps", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 1),
+        ("persist_sig", ctypes.c_int32),
     ]
 
 

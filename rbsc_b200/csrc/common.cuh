@@ -198,6 +198,38 @@ __device__ __forceinline__ void block_append(BlockAppend<T, CAP, BLOCK>& s, bool
     if (threadIdx.x == 0) s.count = cnt + total;
 }
 
+// Warp-private buffered append: a warp gathers its flagged values in a
+// shared-memory buffer of kWarpBuf entries and reserves space in the global
+// list (one atomicAdd by lane 0) only when the buffer could overflow and at
+// the end.  No block barrier: only the warp's own lanes take part, so it
+// costs a ballot and a few shuffles per call where BlockAppend costs two
+// block-wide barriers.  Calls are warp-collective (all 32 lanes).
+constexpr uint32_t kWarpBuf = 256;
+
+template <typename T>
+__device__ __forceinline__ void warp_append_flush(T* buf, uint32_t& cnt, uint32_t* counter, T* out)
+{
+    __syncwarp();
+    const uint32_t lane = threadIdx.x & 31;
+    uint32_t base = 0;
+    if (lane == 0 && cnt) base = atomicAdd(counter, cnt);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    for (uint32_t i = lane; i < cnt; i += 32) out[base + i] = buf[i];
+    __syncwarp();
+    cnt = 0;
+}
+
+template <typename T>
+__device__ __forceinline__ void warp_append(bool take, const T& v, T* buf, uint32_t& cnt, uint32_t* counter, T* out)
+{
+    const uint32_t lane = threadIdx.x & 31;
+    const unsigned m = __ballot_sync(0xffffffffu, take);
+    if (!m) return;
+    if (cnt + 32u > kWarpBuf) warp_append_flush(buf, cnt, counter, out);  // warp-uniform
+    if (take) buf[cnt + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
+    cnt += (uint32_t)__popc(m);
+}
+
 // Kernels enqueued by the calling host thread (reported in rbsc_stats).
 inline uint64_t& launch_counter()
 {

@@ -1200,8 +1200,14 @@ static rbsc_status run_loop(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt,
 static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* kt)
 {
     cudaStream_t s = ctx->stream;
+    // signature phase: one row per lane when the active rows are short (mean
+    // at most 4 arcs), else the tile fold (rows of a web graph's tail)
+    const RoundState& hs = *g->h_st;
+    const bool rows = ctx->opts.persist_sig == 1 ||
+                      (ctx->opts.persist_sig != 2 && (uint64_t)hs.active_arcs <= 4ull * std::max<uint32_t>(hs.active_rows, 1u));
+    const void* kern = rows ? (const void*)k_refine_persistent<true> : (const void*)k_refine_persistent<false>;
     int bps = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, k_refine_persistent, kNodeThreads, 0));
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, kNodeThreads, 0));
     bps = std::max(1, bps);
     // as many blocks as fit (measured best on R-MAT-24 and cnr-2000: the
     // phases are latency-bound, and fewer blocks do not make the barriers
@@ -1228,7 +1234,7 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     const uint32_t r0 = g->h_st->round;
     if (kt) CK(cudaEventRecord(ctx->ev[2], s));
     ++rbsc::launch_counter();
-    CK(cudaLaunchCooperativeKernel((const void*)k_refine_persistent, dim3(grid), dim3(kNodeThreads), args, 0, s));
+    CK(cudaLaunchCooperativeKernel(kern, dim3(grid), dim3(kNodeThreads), args, 0, s));
     if (kt) CK(cudaEventRecord(ctx->ev[3], s));
     CKS(read_state(ctx, g));
     if (kt) {

@@ -45,7 +45,10 @@ struct RoundState {
     uint32_t handoff;        // the active set is small: the persistent kernel takes over
     uint32_t ranks;          // initial classes given a dense rank by k_insert_init
     uint32_t rank_bad;       // k_insert_init could not rank every class (dense ranks by scan instead)
-    uint32_t active_nodes;   // listed nodes after the last compaction (sizes the persistent kernel's grid)
+    uint32_t active_nodes;   // listed nodes after the last compaction
+    uint32_t active_rows;    // rows of the active arc set after the last compaction
+    uint32_t active_arcs;    // its arcs (saturating at 2^32 - 1)
+    uint32_t pad2;
     uint64_t seed;
     uint32_t pcount[2];      // k_refine_persistent: block counts of even / odd passes
     uint32_t prep[2];        // k_refine_persistent: rep_changed of even / odd passes
@@ -1190,28 +1193,29 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
 
 // Keeps the non-singleton entries of the node list (order is not kept: the
 // relabel does not depend on it); dropped nodes are singleton blocks for good.
-// Appends are buffered per block (one reservation per kListBuf kept nodes).
+// Appends are buffered per warp (warp_append: one reservation per ~kWarpBuf
+// kept nodes, no block barrier per step).
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                        const uint32_t* __restrict__ col, CompactBufs bufs)
 {
-    __shared__ BlockAppend<uint32_t, kListBuf, kNodeThreads> sa;
+    __shared__ uint32_t s_buf[kNodeThreads / 32][kWarpBuf];
     __shared__ BlockReserveSmem<kNodeThreads> sm;
     if (st->done || st->error) return;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ src = as->nodes;
     uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
     const uint32_t stride = gridDim.x * kNodeThreads;
-    uint32_t dropped = 0;
-    block_append_begin(sa);
+    uint32_t* buf = s_buf[threadIdx.x >> 5];
+    uint32_t cnt = 0, dropped = 0;
     for (uint32_t base = blockIdx.x * kNodeThreads; base < nn; base += stride) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < nn;
         const uint32_t e = valid ? src[i] : 0u;
         const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
-        block_append(sa, keep, e, &as->nodectr, dst);
+        warp_append<uint32_t>(keep, e, buf, cnt, &as->nodectr, dst);
         dropped += (valid && !keep) ? 1u : 0u;
     }
-    block_append_flush(sa, &as->nodectr, dst);
+    warp_append_flush<uint32_t>(buf, cnt, &as->nodectr, dst);
     block_count<kNodeThreads>(dropped, &as->retired, sm);
 }
 
@@ -1527,6 +1531,8 @@ static __global__ void k_compact_finalize(ActiveSet* as, RoundState* st, Compact
     const bool small = handoff_arcs > 0 && as->m <= handoff_arcs && as->nnodes <= handoff_nodes;
     st->handoff = small ? 1u : 0u;
     st->active_nodes = as->nnodes;
+    st->active_rows = as->K;
+    st->active_arcs = (uint32_t)min(as->m, (uint64_t)0xffffffffu);
     if (use_handle) cudaGraphSetConditional(handle, small ? 0u : 1u);
 }
 
@@ -1606,13 +1612,8 @@ static __global__ void __launch_bounds__(256) k_group_reps(uint32_t n, const uin
 
 // Node list = non-singleton nodes that are not followers (representatives
 // flagged); follower pairs; singleton count.  Grid-stride, both lists written
-// through shared-memory buffers (few reservations on the two counters).
-struct BuildListsSmem {
-    BlockAppend<uint32_t, kListBuf, kNodeThreads> nodes;
-    BlockAppend<uint2, kListBuf, kNodeThreads> pairs;
-    BlockReserveSmem<kNodeThreads> sm;
-};
-
+// through warp-private shared-memory buffers (warp_append: few reservations
+// on the two counters, no block barrier per step).
 static __global__ void __launch_bounds__(kNodeThreads) k_build_lists(uint32_t n, const uint64_t* __restrict__ off,
                                                                      const uint32_t* __restrict__ initlab,
                                                                      const uint32_t* __restrict__ col,
@@ -1621,9 +1622,12 @@ static __global__ void __launch_bounds__(kNodeThreads) k_build_lists(uint32_t n,
                                                                      ActiveSet* __restrict__ as, uint32_t* __restrict__ nodes,
                                                                      uint2* __restrict__ pairs)
 {
-    __shared__ BuildListsSmem s;
-    block_append_begin(s.nodes);
-    block_append_begin(s.pairs);
+    constexpr int W = kNodeThreads / 32;
+    __shared__ uint32_t s_nodes[W][kWarpBuf];
+    __shared__ uint2 s_pairs[W][kWarpBuf];
+    __shared__ BlockReserveSmem<kNodeThreads> sm;
+    const uint32_t warp = threadIdx.x >> 5;
+    uint32_t cn = 0, cp = 0;
     uint32_t singles = 0;
     // 4 nodes per thread and step: their dependent loads (offsets, then the
     // initial label, then the group words) overlap
@@ -1659,13 +1663,13 @@ static __global__ void __launch_bounds__(kNodeThreads) k_build_lists(uint32_t n,
             }
             const bool listed = valid && !single[j] && !follower;
             singles += single[j] ? 1u : 0u;
-            block_append(s.nodes, listed, u | (rep ? kRepFlag : 0u), &as->nodectr, nodes);
-            block_append(s.pairs, follower, make_uint2(u, r), &as->nfollow, pairs);
+            warp_append<uint32_t>(listed, u | (rep ? kRepFlag : 0u), s_nodes[warp], cn, &as->nodectr, nodes);
+            warp_append<uint2>(follower, make_uint2(u, r), s_pairs[warp], cp, &as->nfollow, pairs);
         }
     }
-    block_append_flush(s.nodes, &as->nodectr, nodes);
-    block_append_flush(s.pairs, &as->nfollow, pairs);
-    block_count<kNodeThreads>(singles, &as->retired, s.sm);
+    warp_append_flush<uint32_t>(s_nodes[warp], cn, &as->nodectr, nodes);
+    warp_append_flush<uint2>(s_pairs[warp], cp, &as->nfollow, pairs);
+    block_count<kNodeThreads>(singles, &as->retired, sm);
 }
 
 // Publishes the node list that k_build_lists wrote into buffer 0 (the next
@@ -1869,8 +1873,14 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
 // in pairs by pass parity, so block 0 can reset the next pass's pair while
 // other blocks still read this pass's.  Block 0 mirrors the state into
 // RoundState for the host.
-static __global__ void __launch_bounds__(kNodeThreads, kPersistBlocksPerSM) k_refine_persistent(PersistArgs a)
+// ROWS: the signature phase folds one row per lane (short rows; fewer
+// registers, kPersistBlocksPerSM blocks per SM); otherwise it runs the
+// 512-arc tile fold of k_signature (load-balanced for long rows; 3 blocks per
+// SM).  Both write the same sums.
+template <bool ROWS>
+static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerSM : 3) k_refine_persistent(PersistArgs a)
 {
+    static_assert(kNodeThreads == kTileThreads, "the tile fold runs one tile per warp");
     __shared__ BlockReserveSmem<kNodeThreads> sm;
     RoundState* st = a.st;
     uint32_t round = st->round, stamp = st->stamp, prev = st->prev;
@@ -1881,8 +1891,14 @@ static __global__ void __launch_bounds__(kNodeThreads, kPersistBlocksPerSM) k_re
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
-        if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
-        else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
+        if (ROWS) {
+            if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
+            else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
+        } else {
+            const TileRange all{0u, 0u, nullptr, nullptr, 0ull};
+            if (a.weighted) signature_body<true, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
+            else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
+        }
         if (!grid_barrier(a.gs, st)) return;
         const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);

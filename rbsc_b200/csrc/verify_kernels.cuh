@@ -31,35 +31,6 @@ struct VerifyLists {
     uint32_t* counts; // [0] = |l8|, [1] = |l32|, [2] = |llong|, [3] = failures
 };
 
-// Warp-private buffered append: a warp gathers its flagged values in a
-// shared-memory buffer of kWarpBuf entries and reserves space in the global
-// list (one atomicAdd by lane 0) only when the buffer could overflow and at
-// the end.  No block barrier: only the warp's own lanes take part.
-constexpr uint32_t kWarpBuf = 256;
-
-__device__ __forceinline__ void warp_append_flush(uint32_t* buf, uint32_t& cnt, uint32_t* counter, uint32_t* out)
-{
-    __syncwarp();
-    const uint32_t lane = threadIdx.x & 31;
-    uint32_t base = 0;
-    if (lane == 0 && cnt) base = atomicAdd(counter, cnt);
-    base = __shfl_sync(0xffffffffu, base, 0);
-    for (uint32_t i = lane; i < cnt; i += 32) out[base + i] = buf[i];
-    __syncwarp();
-    cnt = 0;
-}
-
-__device__ __forceinline__ void warp_append(bool take, uint32_t v, uint32_t* buf, uint32_t& cnt, uint32_t* counter,
-                                            uint32_t* out)
-{
-    const uint32_t lane = threadIdx.x & 31;
-    const unsigned m = __ballot_sync(0xffffffffu, take);
-    if (!m) return;
-    if (cnt + 32u > kWarpBuf) warp_append_flush(buf, cnt, counter, out);  // warp-uniform
-    if (take) buf[cnt + (uint32_t)__popc(m & ((1u << lane) - 1u))] = v;
-    cnt += (uint32_t)__popc(m);
-}
-
 // Classifies every node against its block's representative r (the block's
 // smallest node): quick failures (initial colour, row length), empty rows
 // (equal), short rows (lists l8 / l32), long or weighted rows (list llong;
@@ -72,7 +43,7 @@ static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, cons
                                                                 const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
                                                                 uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
 {
-    __shared__ uint32_t s_buf[256 / 32][3][kWarpBuf];
+    __shared__ uint32_t s_buf[256 / 32][3][kWarpBuf];  // kWarpBuf: common.cuh
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t* b8 = s_buf[warp][0];
     uint32_t* b32 = s_buf[warp][1];
