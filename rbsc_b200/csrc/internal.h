@@ -73,7 +73,8 @@ struct rbsc_graph {
     bool hot_active = false;         // the running refinement's first pass uses it
     uint32_t* d_srank = nullptr;     // rank of the initial class claimed at each table slot
     uint32_t* d_init = nullptr;
-    rbsc::Entry* d_tab = nullptr;
+    rbsc::Entry* d_tab = nullptr;            // 16-byte entries: initial and repair passes
+    unsigned long long* d_tab8 = nullptr;    // 8-byte entries: the list passes (same entry count)
     uint32_t log2tab = 0;
     uint32_t next_stamp = 1;
     rbsc::RoundState* d_st = nullptr;

@@ -286,6 +286,7 @@ static void graph_release_refine(rbsc_graph* g)
     dev_free(g->ctx, (void*&)g->d_slot);
     dev_free(g->ctx, (void*&)g->d_joined);
     dev_free(g->ctx, (void*&)g->d_tab);
+    dev_free(g->ctx, (void*&)g->d_tab8);
     dev_free(g->ctx, (void*&)g->d_srank);
     dev_free(g->ctx, (void*&)g->d_st);
     dev_free(g->ctx, (void*&)g->d_out);
@@ -700,6 +701,7 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     CKS(dev_alloc(ctx, (void**)&g->d_small, 256));
     g->log2tab = std::max<uint32_t>(10, log2_ceil(2ull * n));
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
+    CKS(dev_alloc(ctx, (void**)&g->d_tab8, sizeof(unsigned long long) << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_srank, (size_t)4 << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
     CKS(host_alloc(ctx, (void**)&g->h_st, sizeof(RoundState)));
@@ -974,6 +976,11 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (t) CK(cudaEventRecord(t->ev[0], s));
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
+    if (hash) {
+        // the list passes' 8-byte table, over this pass's window
+        ++rbsc::launch_counter();
+        k_clear_window8<<<clear_grid, 256, 0, s>>>(g->d_as, g->d_tab8, g->log2tab);
+    }
     if (t) CK(cudaEventRecord(t->ev[1], s));
     // the host-launched first pass is never captured: time its signature kernel
     if (first != kPassFull) CK(cudaEventRecord(ctx->ev_sig[0], s));
@@ -1035,11 +1042,11 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         if (t) CK(cudaEventRecord(t->ev[3], s));
     } else {
         ++rbsc::launch_counter();
-        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab, g->log2tab, g->d_slot,
+        k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab8, g->log2tab, g->d_slot,
                                                      g->d_joined);
         if (t) CK(cudaEventRecord(t->ev[3], s));
         ++rbsc::launch_counter();
-        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_tab, g->d_slot, g->d_sig,
+        k_relabel_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_tab8, g->d_slot, g->d_sig,
                                                       g->d_joined);
     }
     ++rbsc::launch_counter();
@@ -1223,6 +1230,7 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     a.col = g->d_col[0];
     a.sig = g->d_sig;
     a.tab = g->d_tab;
+    a.tab8 = g->d_tab8;
     a.log2tab = g->log2tab;
     a.tab_entries = 1ull << g->log2tab;
     a.slot = g->d_slot;

@@ -231,6 +231,60 @@ __device__ __forceinline__ uint32_t table_insert(Entry* tab, uint32_t log2size, 
 }
 
 // ---------------------------------------------------------------------------
+// The list passes' relabel table: 8-byte entries, half the bytes of Entry per
+// probe (a 32-B sector holds four), cleared over the pass's window before its
+// inserts (no stamp).  Entry word: low 32 bits = value (smallest member |
+// kJoined), high 32 bits = tag (23 bits of the key's hash, top bit set so a
+// claimed entry is never 0) << 8 | probe distance d.  A key is identified by
+// its tag and its home slot (= slot - d): 23 + log2(window) bits of a 64-bit
+// hash of (k1, k2), 47 bits for a 2^24-entry window.  Two different keys that
+// share both would be merged into one class; the exact check at the fixpoint
+// finds and splits any such merge, as it does for signature collisions.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kProbeMax8 = 256;  // d fits in 8 bits
+
+__device__ __forceinline__ uint32_t table_insert8(unsigned long long* tab, uint32_t log2win, uint64_t k1, uint32_t k2,
+                                                  uint32_t u, bool multi, bool* claimed, uint32_t* err)
+{
+    const uint64_t h = fmix64(k1 ^ ((uint64_t)(k2 & 0xffffff00u) * kGolden));
+    const uint32_t mask = (1u << log2win) - 1u;
+    const uint32_t tag = ((uint32_t)(h >> 8) & 0x7fffffu) | 0x800000u;
+    uint32_t s = (uint32_t)(h >> (64 - log2win)) & mask;
+    const uint32_t val = u | (multi ? kJoined : 0u);
+    for (uint32_t d = 0; d < kProbeMax8 && d <= mask; ++d, s = (s + 1u) & mask) {
+        const uint32_t hi = (tag << 8) | d;
+        const unsigned long long old = atomicCAS(tab + s, 0ull, ((unsigned long long)hi << 32) | val);
+        if (old == 0ull) {
+            *claimed = true;
+            return s;
+        }
+        if ((uint32_t)(old >> 32) == hi) {
+            const uint32_t v = (uint32_t)old;
+            if (!(v & kJoined) || (v & kLabelMask) > u) {
+                uint32_t* vp = reinterpret_cast<uint32_t*>(tab + s);  // the value word (little-endian low half)
+                atomicOr(vp, kJoined);
+                atomicMin(vp, u | kJoined);
+            }
+            *claimed = false;
+            return s;
+        }
+    }
+    atomicOr(err, kErrProbe);
+    *claimed = false;
+    return 0;
+}
+
+// New colour word from an 8-byte entry (see relabel_one).
+template <bool NC>
+__device__ __forceinline__ uint32_t relabel_one8(uint32_t c, const unsigned long long* tab, uint32_t s)
+{
+    if (c & kSingleton) return c;
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(tab + s);
+    const uint32_t v = NC ? __ldg(w) : __ldcg(w);
+    return (v & kLabelMask) | ((v & kJoined) ? 0u : kSingleton);
+}
+
+// ---------------------------------------------------------------------------
 // Per-arc term of the signature: an injective function of the head's label
 // (the multiply by an odd constant, the xor-shift and the second multiply are
 // all bijections of uint64), salted per pass.  t1 feeds the 64-bit sum, t2 a
@@ -754,6 +808,45 @@ __device__ __forceinline__ void insert_warp(bool need, uint32_t u, uint32_t slot
     }
 }
 
+// insert_warp on the 8-byte table of the list passes.
+__device__ __forceinline__ void insert_warp8(bool need, uint32_t u, uint32_t slot_index, bool rep, uint64_t k1, uint32_t k2,
+                                             unsigned long long* tab, uint32_t log2win, uint32_t* slot, uint32_t* err,
+                                             bool& new_block)
+{
+    const int lane = threadIdx.x & 31;
+    const unsigned need_mask = __ballot_sync(0xffffffffu, need);
+    const unsigned rep_mask = __ballot_sync(0xffffffffu, need && rep);
+    if (need) {
+        const unsigned peers = __match_any_sync(need_mask, k1) & __match_any_sync(need_mask, k2);
+        const int leader = __ffs(peers) - 1;
+        const uint32_t umin = __reduce_min_sync(peers, u);
+        uint32_t s = 0;
+        bool claimed = false;
+        if (lane == leader)
+            s = table_insert8(tab, log2win, k1, k2, umin, __popc(peers) > 1 || (rep_mask & peers), &claimed, err);
+        s = __shfl_sync(peers, s, leader);
+        slot[slot_index] = s;
+        new_block = (lane == leader) && claimed;
+    }
+}
+
+// Zeroes the 8-byte list table over the window the next inserts of the pass
+// use (table_window of the listed node count): grid-stride, 16 B per store.
+__device__ __forceinline__ void clear_window8(const ActiveSet* __restrict__ as, unsigned long long* __restrict__ tab,
+                                              uint32_t log2size)
+{
+    const uint64_t entries = 1ull << table_window(as->nnodes, log2size);
+    ulonglong2* t2 = reinterpret_cast<ulonglong2*>(tab);
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < entries / 2; i += (uint64_t)gridDim.x * blockDim.x)
+        t2[i] = make_ulonglong2(0ull, 0ull);
+}
+
+static __global__ void k_clear_window8(const ActiveSet* __restrict__ as, unsigned long long* __restrict__ tab,
+                                       uint32_t log2size)
+{
+    clear_window8(as, tab, log2size);
+}
+
 __device__ __forceinline__ void count_blocks(bool new_block, uint32_t* counter)
 {
     const unsigned nb = __ballot_sync(0xffffffffu, new_block);
@@ -778,7 +871,7 @@ constexpr int kInsertU = 1;  // list entries per thread and iteration of the has
 // Late passes, where few blocks split, do almost no table work.
 __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                      const uint32_t* __restrict__ col,
-                                                     const Sig* __restrict__ sig, Entry* __restrict__ tab,
+                                                     const Sig* __restrict__ sig, unsigned long long* __restrict__ tab,
                                                      uint32_t log2size, uint32_t* __restrict__ slot,
                                                      uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
                                                      uint32_t stamp_in = 0u)
@@ -853,7 +946,7 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
             // a singleton or a representative stands for a block of its own
             // so far; the others count only when they open a class
             bool nb = (active && (c[j] & kSingleton)) || is_rep;
-            insert_warp(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
+            insert_warp8(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, tab, log2win, slot, &st->error, nb);
             made += nb ? 1u : 0u;
         }
     }
@@ -863,7 +956,7 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
 static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                                      const uint32_t* __restrict__ col,
                                                                      const Sig* __restrict__ sig,
-                                                                     Entry* __restrict__ tab, uint32_t log2size,
+                                                                     unsigned long long* __restrict__ tab, uint32_t log2size,
                                                                      uint32_t* __restrict__ slot, uint32_t* __restrict__ joined)
 {
     __shared__ BlockReserveSmem<kNodeThreads> sm;
@@ -1030,7 +1123,7 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 // and iteration, so their dependent loads overlap.
 template <bool NC>
 __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
-                                                  uint32_t* __restrict__ col, const Entry* __restrict__ tab,
+                                                  uint32_t* __restrict__ col, const unsigned long long* __restrict__ tab,
                                                   const uint32_t* __restrict__ slot, Sig* __restrict__ sig,
                                                   const uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
                                                   uint32_t* __restrict__ rep_changed = nullptr)
@@ -1068,7 +1161,7 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
                     (NC ? __ldg(joined + u[j]) : __ldcg(joined + u[j])) != tag)
                     nc = c[j] | kSingleton;
             } else {
-                nc = relabel_one<NC>(c[j], tab, s[j]);
+                nc = relabel_one8<NC>(c[j], tab, s[j]);
             }
             if (nc != c[j]) {
                 col[u[j]] = nc;
@@ -1086,7 +1179,7 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
 
 static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const ActiveSet* __restrict__ as,
                                                                       RoundState* __restrict__ st, uint32_t* __restrict__ col,
-                                                                      const Entry* __restrict__ tab,
+                                                                      const unsigned long long* __restrict__ tab,
                                                                       const uint32_t* __restrict__ slot,
                                                                       Sig* __restrict__ sig, const uint32_t* __restrict__ joined)
 {
@@ -1761,7 +1854,8 @@ struct PersistArgs {
     RoundState* st;
     uint32_t* col;
     Sig* sig;
-    Entry* tab;
+    Entry* tab;                  // 16-byte table (initial and repair passes): cleared when the stamp wraps
+    unsigned long long* tab8;    // 8-byte table of the list passes: cleared over the window every pass
     uint32_t log2tab;
     uint64_t tab_entries;
     uint32_t* slot;
@@ -1891,6 +1985,7 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
+        clear_window8(a.as, a.tab8, a.log2tab);
         if (ROWS) {
             if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
             else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
@@ -1900,10 +1995,10 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
             else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
         }
         if (!grid_barrier(a.gs, st)) return;
-        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp);
+        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab8, a.log2tab, a.slot, a.joined, round, stamp);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);
         if (!grid_barrier(a.gs, st)) return;
-        relabel_list_body<false>(a.as, st, a.col, a.tab, a.slot, a.sig, a.joined, round, &st->prep[p]);
+        relabel_list_body<false>(a.as, st, a.col, a.tab8, a.slot, a.sig, a.joined, round, &st->prep[p]);
         if (!grid_barrier(a.gs, st)) return;
         if (*(volatile uint32_t*)&st->prep[p]) {
             follow_body(a.as, st, a.pairs, a.col, &st->prep[p]);

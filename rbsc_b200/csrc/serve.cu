@@ -134,8 +134,8 @@ extern "C" uint64_t rbsc_serve_footprint(uint64_t n, uint64_t m, int32_t weighte
     // per node: colours, initial labels, signatures, slots, output, ranks, follower
     // pairs, group representatives and counts, two node lists, uploaded colours
     b += N * (4 + 4 + 16 + 4 + 4 + 2 + 8 + 4 + 4 + 8 + 4);
-    // relabel table: 16-B entries and 4-B class ranks
-    b += tab * 20;
+    // relabel tables: 16-B and 8-B entries, 4-B class ranks
+    b += tab * 28;
     // compacted arc sets: two copies of heads, bitmap, row data
     b += 2 * (4 * mpad + mpad / 8 + 12 * N + mpad / 128);
     // exact check: per-node lists, and at worst one 8-B key (twice) per arc
