@@ -243,8 +243,14 @@ __device__ __forceinline__ uint32_t table_insert(Entry* tab, uint32_t log2size, 
 // ---------------------------------------------------------------------------
 constexpr uint32_t kProbeMax8 = 256;  // d fits in 8 bits
 
+// load_first: read the entry before any atomic and try the claim only on an
+// empty one.  A class that many nodes join (the first pass, whose keys are the
+// few initial classes' refinements) then costs plain loads at its entry
+// instead of an atomic per joining group, which serialise at one L2 slice;
+// otherwise (most inserts claim a new class) the CAS goes first and saves the
+// load's round trip.
 __device__ __forceinline__ uint32_t table_insert8(unsigned long long* tab, uint32_t log2win, uint64_t k1, uint32_t k2,
-                                                  uint32_t u, bool multi, bool* claimed, uint32_t* err)
+                                                  uint32_t u, bool multi, bool* claimed, uint32_t* err, bool load_first)
 {
     const uint64_t h = fmix64(k1 ^ ((uint64_t)(k2 & 0xffffff00u) * kGolden));
     const uint32_t mask = (1u << log2win) - 1u;
@@ -253,10 +259,13 @@ __device__ __forceinline__ uint32_t table_insert8(unsigned long long* tab, uint3
     const uint32_t val = u | (multi ? kJoined : 0u);
     for (uint32_t d = 0; d < kProbeMax8 && d <= mask; ++d, s = (s + 1u) & mask) {
         const uint32_t hi = (tag << 8) | d;
-        const unsigned long long old = atomicCAS(tab + s, 0ull, ((unsigned long long)hi << 32) | val);
+        unsigned long long old = load_first ? *reinterpret_cast<volatile unsigned long long*>(tab + s) : 0ull;
         if (old == 0ull) {
-            *claimed = true;
-            return s;
+            old = atomicCAS(tab + s, 0ull, ((unsigned long long)hi << 32) | val);
+            if (old == 0ull) {
+                *claimed = true;
+                return s;
+            }
         }
         if ((uint32_t)(old >> 32) == hi) {
             const uint32_t v = (uint32_t)old;
@@ -811,7 +820,7 @@ __device__ __forceinline__ void insert_warp(bool need, uint32_t u, uint32_t slot
 // insert_warp on the 8-byte table of the list passes.
 __device__ __forceinline__ void insert_warp8(bool need, uint32_t u, uint32_t slot_index, bool rep, uint64_t k1, uint32_t k2,
                                              unsigned long long* tab, uint32_t log2win, uint32_t* slot, uint32_t* err,
-                                             bool& new_block)
+                                             bool load_first, bool& new_block)
 {
     const int lane = threadIdx.x & 31;
     const unsigned need_mask = __ballot_sync(0xffffffffu, need);
@@ -823,7 +832,7 @@ __device__ __forceinline__ void insert_warp8(bool need, uint32_t u, uint32_t slo
         uint32_t s = 0;
         bool claimed = false;
         if (lane == leader)
-            s = table_insert8(tab, log2win, k1, k2, umin, __popc(peers) > 1 || (rep_mask & peers), &claimed, err);
+            s = table_insert8(tab, log2win, k1, k2, umin, __popc(peers) > 1 || (rep_mask & peers), &claimed, err, load_first);
         s = __shfl_sync(peers, s, leader);
         slot[slot_index] = s;
         new_block = (lane == leader) && claimed;
@@ -874,7 +883,7 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
                                                      const Sig* __restrict__ sig, unsigned long long* __restrict__ tab,
                                                      uint32_t log2size, uint32_t* __restrict__ slot,
                                                      uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
-                                                     uint32_t stamp_in = 0u)
+                                                     uint32_t stamp_in = 0u, uint32_t prev_in = 0u)
 {
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ nodes = as->nodes;
@@ -886,6 +895,9 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
     // a late pass with few active nodes stays in L2
     const uint32_t log2win = table_window(nn, log2size);
     const uint32_t tag = (round == kRoundFromState ? st->round : round) + 1u;
+    // many listed nodes per block so far: most inserts join a few big classes
+    const uint32_t prev = round == kRoundFromState ? st->prev : prev_in;
+    const bool load_first = (uint64_t)nn > 8ull * prev;
     const uint32_t lane = threadIdx.x & 31;
     uint32_t made = 0;
     // each warp takes kInsertU x 32 consecutive list entries per iteration and
@@ -946,7 +958,7 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
             // a singleton or a representative stands for a block of its own
             // so far; the others count only when they open a class
             bool nb = (active && (c[j] & kSingleton)) || is_rep;
-            insert_warp8(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, tab, log2win, slot, &st->error, nb);
+            insert_warp8(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, tab, log2win, slot, &st->error, load_first, nb);
             made += nb ? 1u : 0u;
         }
     }
@@ -1995,7 +2007,7 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
             else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
         }
         if (!grid_barrier(a.gs, st)) return;
-        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab8, a.log2tab, a.slot, a.joined, round, stamp);
+        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab8, a.log2tab, a.slot, a.joined, round, stamp, prev);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);
         if (!grid_barrier(a.gs, st)) return;
         relabel_list_body<false>(a.as, st, a.col, a.tab8, a.slot, a.sig, a.joined, round, &st->prep[p]);
