@@ -75,7 +75,6 @@ struct rbsc_graph {
     uint32_t* d_init = nullptr;
     rbsc::Entry* d_tab = nullptr;            // 16-byte entries: initial and repair passes
     unsigned long long* d_tab8 = nullptr;    // 8-byte entries: the list passes (same entry count)
-    bool tab8_dirty = false;                 // a refinement may have left d_tab8 entries set
     uint32_t log2tab = 0;
     uint32_t next_stamp = 1;
     rbsc::RoundState* d_st = nullptr;

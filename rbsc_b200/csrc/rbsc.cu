@@ -702,7 +702,6 @@ static rbsc_status ensure_refine_bufs(rbsc_ctx* ctx, rbsc_graph* g)
     g->log2tab = std::max<uint32_t>(10, log2_ceil(2ull * n));
     CKS(dev_alloc(ctx, (void**)&g->d_tab, sizeof(Entry) << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_tab8, sizeof(unsigned long long) << g->log2tab));
-    g->tab8_dirty = true;  // pool memory: zeroed before the first list pass
     CKS(dev_alloc(ctx, (void**)&g->d_srank, (size_t)4 << g->log2tab));
     CKS(dev_alloc(ctx, (void**)&g->d_st, sizeof(RoundState)));
     CKS(host_alloc(ctx, (void**)&g->h_st, sizeof(RoundState)));
@@ -977,6 +976,11 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     if (t) CK(cudaEventRecord(t->ev[0], s));
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
+    if (hash) {
+        // the list passes' 8-byte table, over this pass's window
+        ++rbsc::launch_counter();
+        k_clear_window8<<<clear_grid, 256, 0, s>>>(g->d_as, g->d_tab8, g->log2tab);
+    }
     if (t) CK(cudaEventRecord(t->ev[1], s));
     // the host-launched first pass is never captured: time its signature kernel
     if (first != kPassFull) CK(cudaEventRecord(ctx->ev_sig[0], s));
@@ -1052,8 +1056,7 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     k_fixpoint<kFixHash><<<1, 1, 0, s>>>(g->d_st, g->d_as, hash ? 1 : 0);
     // compaction for the next pass
     ++rbsc::launch_counter();
-    k_compact_nodes<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb, g->d_slot, hash ? g->d_tab8 : nullptr,
-                                                   1ull << g->log2tab);
+    k_compact_nodes<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->cb);
     if (g->compact_arcs) {
         const unsigned kgrid = persistent_grid(ctx, g->K, kNodeThreads);
         const unsigned agrid = persistent_grid(ctx, ceil_div<uint64_t>(g->m, 16), kNodeThreads);
@@ -1525,10 +1528,6 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     g->streamed_bytes = 0;
     g->streamed_passes = 0;
     CK(cudaMemsetAsync(g->d_joined, 0, 4 * (size_t)n, s));
-    // the list passes leave the 8-byte table clean (k_compact_nodes, the
-    // persistent kernel's exit); a refinement that stopped half-way may not
-    if (g->tab8_dirty) CK(cudaMemsetAsync(g->d_tab8, 0, sizeof(unsigned long long) << g->log2tab, s));
-    g->tab8_dirty = true;
     RoundState& hs = *g->h_st;
     std::memset(&hs, 0, sizeof hs);
     hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);
@@ -1653,7 +1652,6 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         CKS(read_state(ctx, g));
     }
     g->next_stamp = hs.stamp;
-    g->tab8_dirty = hs.error != 0;
     if (hs.error & kErrProbe) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "relabel table overflow");
     if (hs.error & kErrStage) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "signature: a staged tile copy did not complete");
     if (hs.error & kErrInput) return rbsc_fail(ctx, RBSC_ERR_INVALID, "an arc head is >= N");

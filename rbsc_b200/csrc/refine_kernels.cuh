@@ -850,19 +850,6 @@ __device__ __forceinline__ void clear_window8(const ActiveSet* __restrict__ as, 
         t2[i] = make_ulonglong2(0ull, 0ull);
 }
 
-// Zeroes the 8-byte entries the last insert over this node list claimed or
-// joined: the slots of the listed nodes (kRepSlot and stale slots of nodes
-// that skipped the insert are harmless: out of range, or already clean).
-__device__ __forceinline__ void zero_slots8(const ActiveSet* __restrict__ as, const uint32_t* __restrict__ slot,
-                                            unsigned long long* __restrict__ tab, uint64_t entries)
-{
-    const uint32_t nn = as->nnodes;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nn; i += gridDim.x * blockDim.x) {
-        const uint32_t sl = slot[i];
-        if (sl < entries) tab[sl] = 0ull;
-    }
-}
-
 static __global__ void k_clear_window8(const ActiveSet* __restrict__ as, unsigned long long* __restrict__ tab,
                                        uint32_t log2size)
 {
@@ -1314,15 +1301,11 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
 // Appends are buffered per warp (warp_append: one reservation per ~kWarpBuf
 // kept nodes, no block barrier per step).
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
-                                                                       const uint32_t* __restrict__ col, CompactBufs bufs,
-                                                                       const uint32_t* __restrict__ slot,
-                                                                       unsigned long long* __restrict__ tab8, uint64_t tab8_entries)
+                                                                       const uint32_t* __restrict__ col, CompactBufs bufs)
 {
     __shared__ uint32_t s_buf[kNodeThreads / 32][kWarpBuf];
     __shared__ BlockReserveSmem<kNodeThreads> sm;
-    // the list passes' table is cleaned here, also in the pass that ends the
-    // loop: every entry this pass claimed is the slot of a listed node
-    const bool live = !(st->done || st->error);
+    if (st->done || st->error) return;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ src = as->nodes;
     uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
@@ -1332,17 +1315,11 @@ static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet
     for (uint32_t base = blockIdx.x * kNodeThreads; base < nn; base += stride) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < nn;
-        if (tab8 && valid) {
-            const uint32_t sl = slot[i];
-            if (sl < tab8_entries) tab8[sl] = 0ull;
-        }
-        if (!live) continue;
         const uint32_t e = valid ? src[i] : 0u;
         const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
         warp_append<uint32_t>(keep, e, buf, cnt, &as->nodectr, dst);
         dropped += (valid && !keep) ? 1u : 0u;
     }
-    if (!live) return;
     warp_append_flush<uint32_t>(buf, cnt, &as->nodectr, dst);
     block_count<kNodeThreads>(dropped, &as->retired, sm);
 }
@@ -2020,7 +1997,7 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
-        zero_slots8(a.as, a.slot, a.tab8, a.tab_entries);
+        clear_window8(a.as, a.tab8, a.log2tab);
         if (ROWS) {
             if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
             else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
@@ -2047,7 +2024,6 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
         clear = stamp == 1u;
         const bool over = !done && round >= max_rounds;
         const bool err = *(volatile uint32_t*)&st->error != 0u;
-        if (done || over || err) zero_slots8(a.as, a.slot, a.tab8, a.tab_entries);  // leave the table clean
         if (blockIdx.x == 0 && threadIdx.x == 0) {
             st->round = round;
             if (round < kRoundLog) st->round_blocks[round] = cnt;
