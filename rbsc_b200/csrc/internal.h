@@ -31,6 +31,10 @@ struct rbsc_ctx {
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[6] = {};
     cudaEvent_t ev_sig[2] = {};  // around the host-launched first signature kernel
+    // a pass clears the list table's window on this stream beside its
+    // signature kernel (fork / join events, no timing)
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int sm_count = 148;
     std::string err;
 };

@@ -216,6 +216,13 @@ extern "C" rbsc_ctx* rbsc_ctx_create(int32_t device, const rbsc_opts* opts)
     }
     for (auto& ev : ctx->ev) cudaEventCreate(&ev);
     for (auto& ev : ctx->ev_sig) cudaEventCreate(&ev);
+    if ((e = cudaStreamCreateWithFlags(&ctx->side, cudaStreamNonBlocking)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_join, cudaEventDisableTiming)) != cudaSuccess) {
+        rbsc_fail(nullptr, RBSC_ERR_CUDA, "context setup failed: %s", cudaGetErrorString(e));
+        rbsc_ctx_destroy(ctx);
+        return nullptr;
+    }
     cudaDeviceGetAttribute(&ctx->sm_count, cudaDevAttrMultiProcessorCount, device);
     return ctx;
 }
@@ -227,6 +234,12 @@ extern "C" void rbsc_ctx_destroy(rbsc_ctx* ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto& ev : ctx->ev) cudaEventDestroy(ev);
     for (auto& ev : ctx->ev_sig) cudaEventDestroy(ev);
+    if (ctx->ev_fork) cudaEventDestroy(ctx->ev_fork);
+    if (ctx->ev_join) cudaEventDestroy(ctx->ev_join);
+    if (ctx->side) {
+        cudaStreamSynchronize(ctx->side);
+        cudaStreamDestroy(ctx->side);
+    }
     cudaStreamDestroy(ctx->stream);
     pool_release(ctx->dpool);
     pool_release(ctx->hpool);
@@ -977,9 +990,14 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
     ++rbsc::launch_counter();
     k_clear_table<<<clear_grid, 256, 0, s>>>(g->d_st, g->d_tab, 1ull << g->log2tab);
     if (hash) {
-        // the list passes' 8-byte table, over this pass's window
+        // the list table's window, zeroed on the side stream beside the
+        // signature kernel (which neither reads nor writes the table); the
+        // inserts wait for it below
+        CK(cudaEventRecord(ctx->ev_fork, s));
+        CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
         ++rbsc::launch_counter();
-        k_clear_window8<<<clear_grid, 256, 0, s>>>(g->d_as, g->d_tab8, g->log2tab);
+        k_clear_window8<<<clear_grid, 256, 0, ctx->side>>>(g->d_as, g->d_tab8, g->log2tab);
+        CK(cudaEventRecord(ctx->ev_join, ctx->side));
     }
     if (t) CK(cudaEventRecord(t->ev[1], s));
     // the host-launched first pass is never captured: time its signature kernel
@@ -1041,6 +1059,7 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
         CKS(launch_sort_relabel(ctx, g, s));
         if (t) CK(cudaEventRecord(t->ev[3], s));
     } else {
+        CK(cudaStreamWaitEvent(s, ctx->ev_join, 0));
         ++rbsc::launch_counter();
         k_insert_list<<<ngrid, kNodeThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, g->d_tab8, g->log2tab, g->d_slot,
                                                      g->d_joined);
