@@ -1249,7 +1249,6 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     a.col = g->d_col[0];
     a.sig = g->d_sig;
     a.tab = g->d_tab;
-    a.tab8 = g->d_tab8;
     a.log2tab = g->log2tab;
     a.tab_entries = 1ull << g->log2tab;
     a.slot = g->d_slot;

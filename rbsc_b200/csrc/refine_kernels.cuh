@@ -878,9 +878,15 @@ constexpr int kInsertU = 1;  // list entries per thread and iteration of the has
 // its class has another member.  Only the nodes that differ from their
 // representative go through the table, keyed by (label, signature) as before.
 // Late passes, where few blocks split, do almost no table work.
+//
+// TAB: the table the keys go to -- unsigned long long (the 8-byte list table,
+// zeroed over the window before the pass) or Entry (the 16-byte stamped
+// table, which needs no zeroing: the persistent tail kernel uses it, where a
+// zeroing per pass would cost more than its few inserts).
+template <typename TAB>
 __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
                                                      const uint32_t* __restrict__ col,
-                                                     const Sig* __restrict__ sig, unsigned long long* __restrict__ tab,
+                                                     const Sig* __restrict__ sig, TAB* __restrict__ tab,
                                                      uint32_t log2size, uint32_t* __restrict__ slot,
                                                      uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
                                                      uint32_t stamp_in = 0u, uint32_t prev_in = 0u)
@@ -958,7 +964,10 @@ __device__ __forceinline__ uint32_t insert_list_body(const ActiveSet* __restrict
             // a singleton or a representative stands for a block of its own
             // so far; the others count only when they open a class
             bool nb = (active && (c[j] & kSingleton)) || is_rep;
-            insert_warp8(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, tab, log2win, slot, &st->error, load_first, nb);
+            if constexpr (sizeof(TAB) == 8)
+                insert_warp8(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, tab, log2win, slot, &st->error, load_first, nb);
+            else
+                insert_warp(need, u[j], idx[j], (e[j] & kRepFlag) != 0, k1, k2, stamp, tab, log2win, slot, &st->error, nb);
             made += nb ? 1u : 0u;
         }
     }
@@ -972,7 +981,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_insert_list(const Activ
                                                                      uint32_t* __restrict__ slot, uint32_t* __restrict__ joined)
 {
     __shared__ BlockReserveSmem<kNodeThreads> sm;
-    const uint32_t made = insert_list_body(as, st, col, sig, tab, log2size, slot, joined);
+    const uint32_t made = insert_list_body<unsigned long long>(as, st, col, sig, tab, log2size, slot, joined);
     block_count<kNodeThreads>(made, &st->count, sm);
 }
 
@@ -1133,9 +1142,9 @@ __device__ __forceinline__ uint32_t relabel_one(uint32_t c, const Entry* tab, ui
 // position); also zeroes the signatures of the rows that cross a tile edge
 // (the next pass adds into them atomically).  Four list entries per thread
 // and iteration, so their dependent loads overlap.
-template <bool NC>
+template <bool NC, typename TAB>
 __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ as, RoundState* __restrict__ st,
-                                                  uint32_t* __restrict__ col, const unsigned long long* __restrict__ tab,
+                                                  uint32_t* __restrict__ col, const TAB* __restrict__ tab,
                                                   const uint32_t* __restrict__ slot, Sig* __restrict__ sig,
                                                   const uint32_t* __restrict__ joined, uint32_t round = kRoundFromState,
                                                   uint32_t* __restrict__ rep_changed = nullptr)
@@ -1173,7 +1182,8 @@ __device__ __forceinline__ void relabel_list_body(const ActiveSet* __restrict__ 
                     (NC ? __ldg(joined + u[j]) : __ldcg(joined + u[j])) != tag)
                     nc = c[j] | kSingleton;
             } else {
-                nc = relabel_one8<NC>(c[j], tab, s[j]);
+                if constexpr (sizeof(TAB) == 8) nc = relabel_one8<NC>(c[j], tab, s[j]);
+                else nc = relabel_one<NC>(c[j], tab, s[j]);
             }
             if (nc != c[j]) {
                 col[u[j]] = nc;
@@ -1195,7 +1205,7 @@ static __global__ void __launch_bounds__(kNodeThreads) k_relabel_list(const Acti
                                                                       const uint32_t* __restrict__ slot,
                                                                       Sig* __restrict__ sig, const uint32_t* __restrict__ joined)
 {
-    relabel_list_body<true>(as, st, col, tab, slot, sig, joined);
+    relabel_list_body<true, unsigned long long>(as, st, col, tab, slot, sig, joined);
 }
 
 // New colours of all nodes (after k_insert_all), in place.
@@ -1866,8 +1876,7 @@ struct PersistArgs {
     RoundState* st;
     uint32_t* col;
     Sig* sig;
-    Entry* tab;                  // 16-byte table (initial and repair passes): cleared when the stamp wraps
-    unsigned long long* tab8;    // 8-byte table of the list passes: cleared over the window every pass
+    Entry* tab;                  // the 16-byte stamped table (cleared when the stamp wraps)
     uint32_t log2tab;
     uint64_t tab_entries;
     uint32_t* slot;
@@ -1997,7 +2006,6 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
-        clear_window8(a.as, a.tab8, a.log2tab);
         if (ROWS) {
             if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
             else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
@@ -2007,10 +2015,10 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
             else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
         }
         if (!grid_barrier(a.gs, st)) return;
-        const uint32_t made = insert_list_body(a.as, st, a.col, a.sig, a.tab8, a.log2tab, a.slot, a.joined, round, stamp, prev);
+        const uint32_t made = insert_list_body<Entry>(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp, prev);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);
         if (!grid_barrier(a.gs, st)) return;
-        relabel_list_body<false>(a.as, st, a.col, a.tab8, a.slot, a.sig, a.joined, round, &st->prep[p]);
+        relabel_list_body<false, Entry>(a.as, st, a.col, a.tab, a.slot, a.sig, a.joined, round, &st->prep[p]);
         if (!grid_barrier(a.gs, st)) return;
         if (*(volatile uint32_t*)&st->prep[p]) {
             follow_body(a.as, st, a.pairs, a.col, &st->prep[p]);
