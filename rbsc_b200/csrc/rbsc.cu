@@ -1384,7 +1384,7 @@ static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
 
 // Exact check of the current fixpoint.  Returns the number of failing nodes in
 // *nfail (0 = the partition is the coarsest stable one).
-static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail)
+static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail, uint32_t* out)
 {
     cudaStream_t s = ctx->stream;
     const uint32_t n = g->n;
@@ -1431,7 +1431,7 @@ static rbsc_status verify_fixpoint(rbsc_ctx* ctx, rbsc_graph* g, uint32_t* nfail
     VerifyLists vl{g->d_vl8, g->d_vl32, g->d_vllong, counts};
     ++rbsc::launch_counter();
     k_verify_classify<<<persistent_grid(ctx, n, 256), 256, 0, s>>>(n, col, g->d_initlab, g->d_off, g->weighted ? 1 : 0, vl,
-                                                                  g->d_vflag, g->d_fail);
+                                                                  g->d_vflag, g->d_fail, out);
     const unsigned sgrid = persistent_grid(ctx, n, 256);
     ++rbsc::launch_counter();
     k_verify_short<8><<<sgrid, 256, 0, s>>>(n, g->d_vl8, counts + 0, col, g->d_off, vstart, vidx, g->d_fail, counts + 3);
@@ -1642,6 +1642,8 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
 
     float verify_ms = 0.f, loop_ms = 0.f;
     uint32_t repairs = 0;
+    uint32_t* out = d_out ? d_out : g->d_out;
+    bool labels_out = false;  // a passed exact check wrote them
     for (;;) {
         if (hs.error) break;
         CK(cudaEventRecord(ctx->ev[4], s));
@@ -1658,7 +1660,8 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         if (!ctx->opts.verify) break;
         CK(cudaEventRecord(ctx->ev[2], s));
         uint32_t nfail = 0;
-        CKS(verify_fixpoint(ctx, g, &nfail));
+        CKS(verify_fixpoint(ctx, g, &nfail, out));
+        labels_out = nfail == 0;
         CK(cudaEventRecord(ctx->ev[3], s));
         CK(cudaEventSynchronize(ctx->ev[3]));
         float ms = 0.f;
@@ -1674,10 +1677,11 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     if (hs.error & kErrStage) return rbsc_fail(ctx, RBSC_ERR_DEVICE, "signature: a staged tile copy did not complete");
     if (hs.error & kErrInput) return rbsc_fail(ctx, RBSC_ERR_INVALID, "an arc head is >= N");
     if (hs.error & kErrRounds) return rbsc_fail(ctx, RBSC_ERR_NOT_CONVERGED, "no fixpoint after %u passes", hs.round);
-    uint32_t* out = d_out ? d_out : g->d_out;
-    ++rbsc::launch_counter();
-    k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], out);
-    CK(cudaGetLastError());
+    if (!labels_out) {
+        ++rbsc::launch_counter();
+        k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], out);
+        CK(cudaGetLastError());
+    }
     CK(cudaEventRecord(ctx->ev[1], s));
     CK(cudaEventSynchronize(ctx->ev[1]));
     float total_ms = 0.f;

@@ -37,11 +37,14 @@ struct VerifyLists {
 // their and r's rows are flagged for the global path in vflag).  Grid-stride
 // by warps, 32 consecutive nodes per warp and step, list appends buffered per
 // warp (warp_append): a global counter is touched once per ~kWarpBuf listed
-// nodes, and no block-wide barrier is needed.
+// nodes, and no block-wide barrier is needed.  It also writes every node's
+// canonical label to `out` (the refinement's result when the check passes,
+// so no separate pass over the colours is needed then).
 static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, const uint32_t* __restrict__ col,
                                                                 const uint32_t* __restrict__ initlab,
                                                                 const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
-                                                                uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail)
+                                                                uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail,
+                                                                uint32_t* __restrict__ out)
 {
     __shared__ uint32_t s_buf[256 / 32][3][kWarpBuf];  // kWarpBuf: common.cuh
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -56,6 +59,7 @@ static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, cons
         if (u < n) {
             const uint32_t c = col[u];
             const uint32_t r = c & kLabelMask;
+            out[u] = r;  // the canonical labels, final when the check passes
             if (!(c & kSingleton) && r != u) {
                 const uint64_t du = off[u + 1] - off[u], dr = off[r + 1] - off[r];
                 if (initlab[u] != initlab[r]) bad = true;
