@@ -14,6 +14,11 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200); run with -m gpu")
+    # always list the reasons of skipped tests in the summary (a test that
+    # needs the reference checkout or a fixture says which)
+    rc = getattr(config.option, "reportchars", None) or ""
+    if "s" not in rc and "a" not in rc and "A" not in rc:
+        config.option.reportchars = rc + "s"
 
 
 def load_index():
