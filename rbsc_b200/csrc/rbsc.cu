@@ -1249,6 +1249,9 @@ static rbsc_status run_persistent(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_time
     a.col = g->d_col[0];
     a.sig = g->d_sig;
     a.tab = g->d_tab;
+    a.tab8 = g->d_tab8;
+    // windows of at most 2^20 entries (8 MB to zero per pass): the 8-byte table
+    a.use8 = g->h_st->active_nodes <= (1u << 19) ? 1 : 0;
     a.log2tab = g->log2tab;
     a.tab_entries = 1ull << g->log2tab;
     a.slot = g->d_slot;

@@ -1308,29 +1308,31 @@ static __global__ void k_fixpoint(RoundState* st, const ActiveSet* as, int add_r
 
 // Keeps the non-singleton entries of the node list (order is not kept: the
 // relabel does not depend on it); dropped nodes are singleton blocks for good.
-// Appends are buffered per warp (warp_append: one reservation per ~kWarpBuf
-// kept nodes, no block barrier per step).
+// Appends are buffered per block (BlockAppend: one reservation per kListBuf
+// kept nodes).  Warp-private buffers were measured slower here: the kept list
+// is long, and one reservation per 256 entries on the single counter
+// serialises in L2 (R-MAT-22 pass 1: 16.9 -> 26.0 us).
 static __global__ void __launch_bounds__(kNodeThreads) k_compact_nodes(ActiveSet* __restrict__ as, const RoundState* __restrict__ st,
                                                                        const uint32_t* __restrict__ col, CompactBufs bufs)
 {
-    __shared__ uint32_t s_buf[kNodeThreads / 32][kWarpBuf];
+    __shared__ BlockAppend<uint32_t, kListBuf, kNodeThreads> sa;
     __shared__ BlockReserveSmem<kNodeThreads> sm;
     if (st->done || st->error) return;
     const uint32_t nn = as->nnodes;
     const uint32_t* __restrict__ src = as->nodes;
     uint32_t* __restrict__ dst = bufs.nodes[as->dst_nodes];
     const uint32_t stride = gridDim.x * kNodeThreads;
-    uint32_t* buf = s_buf[threadIdx.x >> 5];
-    uint32_t cnt = 0, dropped = 0;
+    uint32_t dropped = 0;
+    block_append_begin(sa);
     for (uint32_t base = blockIdx.x * kNodeThreads; base < nn; base += stride) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < nn;
         const uint32_t e = valid ? src[i] : 0u;
         const bool keep = valid && !(col[e & ~kRepFlag] & kSingleton);
-        warp_append<uint32_t>(keep, e, buf, cnt, &as->nodectr, dst);
+        block_append(sa, keep, e, &as->nodectr, dst);
         dropped += (valid && !keep) ? 1u : 0u;
     }
-    warp_append_flush<uint32_t>(buf, cnt, &as->nodectr, dst);
+    block_append_flush(sa, &as->nodectr, dst);
     block_count<kNodeThreads>(dropped, &as->retired, sm);
 }
 
@@ -1877,6 +1879,9 @@ struct PersistArgs {
     uint32_t* col;
     Sig* sig;
     Entry* tab;                  // the 16-byte stamped table (cleared when the stamp wraps)
+    unsigned long long* tab8;    // the 8-byte list table (zeroed over the window every pass)
+    int use8;                    // the passes use tab8: small windows, whose zeroing costs less than
+                                 // the 16-byte table's extra load per insert
     uint32_t log2tab;
     uint64_t tab_entries;
     uint32_t* slot;
@@ -2006,6 +2011,7 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
     for (;;) {
         const uint32_t p = round & 1u;
         if (clear) clear_table_all(a.tab, a.tab_entries);
+        if (a.use8) clear_window8(a.as, a.tab8, a.log2tab);
         if (ROWS) {
             if (a.weighted) row_signature_body<true>(a.as, a.col, a.sig, pass_salt1(seed, round));
             else row_signature_body<false>(a.as, a.col, a.sig, pass_salt1(seed, round));
@@ -2015,10 +2021,13 @@ static __global__ void __launch_bounds__(kNodeThreads, ROWS ? kPersistBlocksPerS
             else signature_body<false, uint32_t, false>(a.as, st, a.col, a.sig, all, nullptr, nullptr, round);
         }
         if (!grid_barrier(a.gs, st)) return;
-        const uint32_t made = insert_list_body<Entry>(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp, prev);
+        const uint32_t made =
+            a.use8 ? insert_list_body<unsigned long long>(a.as, st, a.col, a.sig, a.tab8, a.log2tab, a.slot, a.joined, round, stamp, prev)
+                   : insert_list_body<Entry>(a.as, st, a.col, a.sig, a.tab, a.log2tab, a.slot, a.joined, round, stamp, prev);
         block_count<kNodeThreads>(made, &st->pcount[p], sm);
         if (!grid_barrier(a.gs, st)) return;
-        relabel_list_body<false, Entry>(a.as, st, a.col, a.tab, a.slot, a.sig, a.joined, round, &st->prep[p]);
+        if (a.use8) relabel_list_body<false, unsigned long long>(a.as, st, a.col, a.tab8, a.slot, a.sig, a.joined, round, &st->prep[p]);
+        else relabel_list_body<false, Entry>(a.as, st, a.col, a.tab, a.slot, a.sig, a.joined, round, &st->prep[p]);
         if (!grid_barrier(a.gs, st)) return;
         if (*(volatile uint32_t*)&st->prep[p]) {
             follow_body(a.as, st, a.pairs, a.col, &st->prep[p]);
