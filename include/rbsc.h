@@ -263,6 +263,25 @@ rbsc_status rbsc_refine_edge_batches(rbsc_ctx* ctx, const rbsc_csr* host_graph, 
                                      int32_t aggressive, uint32_t* out_labels, rbsc_stats* stats,
                                      rbsc_edge_batch_info* info);
 
+/* ---- lumping with double weights ------------------------------------------
+ * Replaces Valmari's minimiser built with MDP_weight_is_double
+ * (src/part_ref/MDPmin.cc:37, 107-113; MDP_minimize.cc:567-637): the weight of
+ * a node into a block is the double sum of its arcs' weights into the block,
+ * taken in arc order and rounded to float (MDP_round_weight); a sum that
+ * rounds to zero counts as no arc.  The result is the coarsest partition that
+ * refines the initial colours (NULL = one block) and in which the members of
+ * every block have equal rounded sums into every block; labels canonical
+ * (smallest node id per block), checked exactly before they are returned.
+ * host_graph->weights must be NULL: `weights` (host, m doubles, finite, of
+ * magnitude below 2^960) replaces it; m < 2^32.  stats: rounds (passes until
+ * the block count stopped changing), blocks, verified, repairs, device_ms,
+ * round_blocks, kernel_launches.  The minimiser adds a block's weights in
+ * the order of the block's members: its float can differ from this one's
+ * only when the two double sums fall on different sides of a float rounding
+ * boundary. */
+rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph, const double* weights,
+                            const uint32_t* init_colors, uint32_t* out_labels, rbsc_stats* stats);
+
 /* ---- autotuning (no reference counterpart) --------------------------------
  * Times refinements of a resident graph (d_init_colors: device colours or
  * NULL) under every combination of the candidate knobs below and returns the

@@ -208,6 +208,130 @@ int orc_refine_exact(uint32_t n, const uint64_t* off, const uint32_t* idx, const
 }
 
 /* ------------------------------------------------------------------ */
+/* exact refinement with double weights                                */
+/* ------------------------------------------------------------------ */
+typedef struct { uint32_t lab; uint32_t pos; double w; } ld_arc;
+
+/* successor block, then arc position: a stable order of the row */
+static int cmp_ld(const void* x, const void* y)
+{
+    const ld_arc* a = (const ld_arc*)x;
+    const ld_arc* b = (const ld_arc*)y;
+    if (a->lab != b->lab) return a->lab < b->lab ? -1 : 1;
+    return a->pos < b->pos ? -1 : (a->pos > b->pos ? 1 : 0);
+}
+
+/*
+ * Exact coarsest stable refinement with double weights, the lumping of
+ * Valmari's minimiser built with MDP_weight_is_double
+ * (src/part_ref/MDPmin.cc:107-113, MDP_minimize.cc:567-637): the weight of a
+ * node into a block is the double sum of its arcs' weights into that block,
+ * rounded to float (MDP_round_weight), and a sum that rounds to zero counts
+ * as no arc into the block (MDP_minimize.cc:596-599).  Two nodes are
+ * equivalent iff they are in the same block and their rounded sums into
+ * every block are equal.  The double sum of a (node, block) pair is taken in
+ * arc order (the minimiser adds in the order of its block's members, which
+ * gives the same float except when the two double sums fall on different
+ * sides of a float rounding boundary).
+ *   wt[m] (finite doubles) replaces orc_refine_exact's integer weights; the
+ *   other arguments and the result are orc_refine_exact's.
+ */
+int orc_refine_f64(uint32_t n, const uint64_t* off, const uint32_t* idx, const double* wt,
+                   const uint32_t* init, uint32_t* labels_out, uint32_t* rounds_out,
+                   uint32_t* blocks_out, uint32_t* round_blocks, uint32_t max_rounds)
+{
+    *rounds_out = 0; *blocks_out = 0;
+    if (n == 0) { if (round_blocks) round_blocks[0] = 0; return 0; }
+    uint64_t m = off[n];
+    uint32_t* cur = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* nxt = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* ord = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* tmp = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint64_t* sstart = (uint64_t*)malloc(sizeof(uint64_t) * n);
+    uint32_t* slen = (uint32_t*)malloc(sizeof(uint32_t) * n);
+    uint32_t* slab = (uint32_t*)malloc(sizeof(uint32_t) * (m ? m : 1));
+    uint64_t* sbits = (uint64_t*)malloc(sizeof(uint64_t) * (m ? m : 1));
+    ld_arc* row = (ld_arc*)malloc(sizeof(ld_arc) * (m ? m : 1));
+
+    uint32_t prev;
+    if (init) prev = orc_canonicalize(n, init, cur);
+    else { for (uint32_t i = 0; i < n; ++i) cur[i] = 0; prev = 1; }
+    if (round_blocks) round_blocks[0] = prev;
+
+    int status = -1;
+    uint32_t r = 0;
+    while (r < max_rounds) {
+        for (uint32_t u = 0; u < n; ++u) {
+            uint64_t b = off[u], e = off[u + 1], d = e - b;
+            for (uint64_t k = 0; k < d; ++k) {
+                row[k].lab = cur[idx[b + k]];
+                row[k].pos = (uint32_t)k;
+                row[k].w = wt[b + k];
+            }
+            qsort(row, (size_t)d, sizeof(ld_arc), cmp_ld);
+            uint32_t len = 0;
+            sstart[u] = b;
+            for (uint64_t k = 0; k < d;) {
+                uint32_t lab = row[k].lab;
+                double s = 0.0;
+                while (k < d && row[k].lab == lab) { s += row[k].w; ++k; }
+                const float f = (float)s;
+                if (f != 0.0f) {
+                    uint32_t bits;
+                    memcpy(&bits, &f, sizeof bits);
+                    slab[b + len] = lab; sbits[b + len] = bits; ++len;
+                }
+            }
+            slen[u] = len;
+        }
+        exact_ctx c = { cur, sstart, slen, slab, sbits };
+        for (uint32_t i = 0; i < n; ++i) ord[i] = i;
+        msort_idx(ord, tmp, n, cmp_exact, &c);
+        uint32_t blocks = 0, rep = 0;
+        for (uint32_t i = 0; i < n; ++i) {
+            if (i == 0 || cmp_exact(ord[i - 1], ord[i], &c) != 0) { rep = ord[i]; ++blocks; }
+            nxt[ord[i]] = rep;
+        }
+        ++r;
+        if (round_blocks) round_blocks[r] = blocks;
+        uint32_t* sw = cur; cur = nxt; nxt = sw;
+        if (blocks == prev) { status = 0; break; }
+        prev = blocks;
+    }
+    *rounds_out = r;
+    *blocks_out = orc_canonicalize(n, cur, labels_out);
+    free(cur); free(nxt); free(ord); free(tmp); free(sstart); free(slen);
+    free(slab); free(sbits); free(row);
+    return status;
+}
+
+/* The decimal reader of src/part_ref/reader.cc:110-147, which turns the MDP
+ * text's weights into doubles when the minimiser is built with
+ * MDP_weight_is_double: signs, then the integer digits (x10 + d), then each
+ * fractional digit d added as d x scale with scale divided by 10 per digit.
+ * The double it returns is not always the nearest one to the decimal, so the
+ * weights given to the other restatements and to the product come from here.
+ * Returns the number of characters consumed (0 = no digit). */
+size_t orc_reader_decimal(const char* s, double* out)
+{
+    size_t i = 0;
+    int neg = 0;
+    while (s[i] == '+' || s[i] == '-') { if (s[i] == '-') neg = !neg; ++i; }
+    double result = 0.0;
+    int digits = s[i] >= '0' && s[i] <= '9';
+    while (s[i] >= '0' && s[i] <= '9') { result *= 10; result += s[i] - '0'; ++i; }
+    if (s[i] == '.') {
+        ++i;
+        digits |= s[i] >= '0' && s[i] <= '9';
+        double scale = 1.0;
+        while (s[i] >= '0' && s[i] <= '9') { scale /= 10; result += scale * (s[i] - '0'); ++i; }
+    }
+    if (!digits) return 0;
+    *out = neg ? -result : result;
+    return i;
+}
+
+/* ------------------------------------------------------------------ */
 /* arcs-cuda text writer (feeds the reference programs)                */
 /* ------------------------------------------------------------------ */
 

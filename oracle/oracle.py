@@ -30,6 +30,7 @@ LIB_PATH = os.path.join(HERE, "liboracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
 REF_RSC = os.path.join(REF_DIR, "ref_rsc")
 REF_VALMARI = os.path.join(REF_DIR, "ref_valmari")
+REF_VALMARI_F64 = os.path.join(REF_DIR, "ref_valmari_f64")
 REF_RBSC = os.path.join(REF_DIR, "ref_rbsc")
 # decoded copy of the reference's vendored LAW sample (webgraph-rs/data/cnr-2000),
 # made in this container by prepare_law() and carried with the tree
@@ -75,6 +76,7 @@ def load_law():
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
 _u64p = ctypes.POINTER(ctypes.c_uint64)
+_f64p = ctypes.POINTER(ctypes.c_double)
 
 
 def build(ref: str | None = None) -> None:
@@ -121,6 +123,11 @@ def _load():
         lib.orc_free.restype = None
         lib.orc_write_mdp.argtypes = [ctypes.c_char_p, ctypes.c_uint32, _u64p, _u32p, _u64p, _u32p]
         lib.orc_write_mdp.restype = ctypes.c_int
+        lib.orc_refine_f64.argtypes = [ctypes.c_uint32, _u64p, _u32p, _f64p, _u32p, _u32p,
+                                       _u32p, _u32p, _u32p, ctypes.c_uint32]
+        lib.orc_refine_f64.restype = ctypes.c_int
+        lib.orc_reader_decimal.argtypes = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_double)]
+        lib.orc_reader_decimal.restype = ctypes.c_size_t
         _lib = lib
     return _lib
 
@@ -170,6 +177,81 @@ def refine_exact(off, idx, wt=None, init=None, max_rounds: int | None = None) ->
                               ctypes.byref(rounds), ctypes.byref(blocks), _p32(rb), max_rounds)
     return OracleResult(labels[:n].copy(), blocks.value, rounds.value, None,
                         [int(x) for x in rb[: rounds.value + 1]], st)
+
+
+def refine_f64(off, idx, wt, init=None, max_rounds: int | None = None) -> OracleResult:
+    """Exact coarsest stable refinement with double weights, sums into a block
+    rounded to float (oracle.c: orc_refine_f64)."""
+    lib = _load()
+    n = len(off) - 1
+    off, idx, _ = _csr(off, idx, None)
+    w = np.ascontiguousarray(wt, dtype=np.float64)
+    if w.size == 0:
+        w = np.zeros(1, dtype=np.float64)
+    init = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+    if max_rounds is None:
+        max_rounds = n + 2
+    labels = np.zeros(max(n, 1), dtype=np.uint32)
+    rounds = ctypes.c_uint32()
+    blocks = ctypes.c_uint32()
+    rb = np.zeros(max_rounds + 1, dtype=np.uint32)
+    st = lib.orc_refine_f64(n, _p64(off), _p32(idx), w.ctypes.data_as(_f64p), _p32(init), _p32(labels),
+                            ctypes.byref(rounds), ctypes.byref(blocks), _p32(rb), max_rounds)
+    return OracleResult(labels[:n].copy(), blocks.value, rounds.value, None,
+                        [int(x) for x in rb[: rounds.value + 1]], st)
+
+
+def reader_decimals(texts) -> np.ndarray:
+    """Doubles of decimal weight strings as the minimiser's reader computes
+    them (src/part_ref/reader.cc:110-147, restated in oracle.c:
+    orc_reader_decimal)."""
+    lib = _load()
+    out = np.zeros(len(texts), dtype=np.float64)
+    v = ctypes.c_double()
+    for i, t in enumerate(texts):
+        if lib.orc_reader_decimal(t.encode(), ctypes.byref(v)) != len(t):
+            raise ValueError(f"not a decimal: {t!r}")
+        out[i] = v.value
+    return out
+
+
+def mdp_text_f64(off, idx, wt_text, init=None) -> bytes:
+    """Valmari MDP text with decimal weights (the strings themselves, which
+    the double-weight minimiser parses; no merging of parallel arcs)."""
+    off = np.asarray(off, dtype=np.uint64)
+    idx = np.asarray(idx, dtype=np.uint32)
+    n = len(off) - 1
+    m = int(off[-1])
+    if m > n * n:
+        raise ValueError("more transitions than states squared: the reader refuses them")
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64)))
+    blocks = []
+    if init is not None:
+        init = np.asarray(init, dtype=np.uint32)
+        for c in sorted(set(init.tolist()))[1:]:
+            blocks.append(" ".join(map(str, (np.nonzero(init == c)[0] + 1).tolist())) + " 0")
+    out = [f"{n} 0 0 {m} {1 + len(blocks)}\n"]
+    if m:
+        out.append("\n".join(f"{a + 1} {w} {c + 1}" for a, w, c in zip(src.tolist(), wt_text, idx[:m].tolist())))
+        out.append("\n")
+    if blocks:
+        out.append("\n".join(blocks) + "\n")
+    return "".join(out).encode()
+
+
+def run_ref_valmari_f64(off, idx, wt_text, init=None, timeout: float = 600.0) -> OracleResult:
+    """Valmari's minimiser built with double weights (src/part_ref, unmodified,
+    MDP_weight_is_double) on a graph whose weights are decimal strings."""
+    if not os.path.exists(REF_VALMARI_F64):
+        raise FileNotFoundError(REF_VALMARI_F64)
+    txt = subprocess.run([REF_VALMARI_F64], input=mdp_text_f64(off, idx, wt_text, init), capture_output=True,
+                         timeout=timeout, check=True).stdout.decode()
+    t, done, nodes, rounds, labels = _parse_ref_output(txt)
+    n = len(off) - 1
+    lab = _canon_u64(labels) if n else np.zeros(0, dtype=np.uint32)
+    res = OracleResult(lab, nodes, -1, None)
+    res.time_s = t
+    return res
 
 
 @dataclass

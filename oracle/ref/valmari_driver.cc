@@ -7,8 +7,9 @@
 // The reference sources are #included from the reference tree at compile time
 // (oracle/Makefile passes -I<reference>/src/part_ref); none is copied here.
 // The glue below plays the part of src/part_ref/MDPmin.cc:105-170 (integer
-// weights, the store_* name mapping): it has to present the same interface to
-// MDP_read.cc, and is written here in its minimal form.
+// weights, or double weights when built with -DORC_F64; the store_* name
+// mapping): it has to present the same interface to MDP_read.cc, and is
+// written here in its minimal form.
 //
 // Input (stdin): the MDP text of MDP_read.cc:51-63, i.e.
 //   "nr_states 0 0 nr_w_trans nr_blocks", then nr_w_trans lines "tail w head"
@@ -20,9 +21,19 @@
 #include <sstream>
 #include <string>
 
+#ifdef ORC_F64
+// the minimiser's double-weight configuration (MDPmin.cc:107-113): weights
+// read as decimals, block sums rounded to float before they are compared
+#include <cfloat>
+#define MDP_weight_is_double
+typedef double MDP_weight_type;
+const MDP_weight_type MDP_zero_weight = 0.0, MDP_unused_weight = DBL_MAX;
+inline void MDP_round_weight(MDP_weight_type& ww) { ww = float(ww); }
+#else
 typedef int MDP_weight_type;
 const MDP_weight_type MDP_zero_weight = 0, MDP_unused_weight = INT_MIN;
 inline void MDP_round_weight(MDP_weight_type&) {}
+#endif
 
 #include "MDP_minimize.cc"
 

@@ -190,6 +190,22 @@ class Context:
         return (_result(st, None if out is None else out[: c.n]),
                 {k: int(getattr(info, k)) for k, _ in _lib.EdgeBatchInfo._fields_})
 
+    def refine_f64(self, off, idx, wt, init=None, labels: bool = True) -> Result:
+        """Lumping with double weights (rbsc_refine_f64): the rounded-to-float
+        sums into every block decide, as in Valmari's minimiser built with
+        MDP_weight_is_double."""
+        c, keep = _csr(off, idx, None)
+        w = np.ascontiguousarray(wt, dtype=np.float64)
+        if w.size < c.m:
+            raise ValueError("rbsc_refine_f64: fewer weights than arcs")
+        init_a = None if init is None else np.ascontiguousarray(init, dtype=np.uint32)
+        out = np.zeros(max(c.n, 1), dtype=np.uint32) if labels or c.n else None
+        st = _lib.Stats()
+        _check(self._lib, self._lib.rbsc_refine_f64(self._h, ctypes.byref(c), w.ctypes.data if w.size else None,
+                                                    None if init_a is None else init_a.ctypes.data,
+                                                    out.ctypes.data, ctypes.byref(st)), self._h)
+        return _result(st, out[: c.n] if labels else None)
+
     def batch_refine(self, off, idx, graph_nodes, init=None, out=None) -> BatchResult:
         """One-shot refinement of a batch of graphs side by side
         (rbsc_batch_refine).  `out`: optional arrays from batch_buffers."""

@@ -40,7 +40,7 @@ EXPORTED = [
     "rbsc_gen_wl_batch", "rbsc_graph_batch_free", "rbsc_batch_refine", "rbsc_graph_batch_refine",
     "rbsc_gen_er_host", "rbsc_gen_lift_host", "rbsc_refine_edge_batches", "rbsc_graph_upload_streamed",
     "rbsc_gen_rmat_pinned", "rbsc_host_graph_free_pinned", "rbsc_tune_space_default", "rbsc_graph_autotune",
-    "rbsc_bv_load", "rbsc_csr_save", "rbsc_csr_load",
+    "rbsc_bv_load", "rbsc_csr_save", "rbsc_csr_load", "rbsc_refine_f64",
     "rbsc_serve_opts_default", "rbsc_serve_footprint", "rbsc_serve_create", "rbsc_serve_destroy",
     "rbsc_serve_last_error", "rbsc_serve_submit", "rbsc_serve_poll", "rbsc_serve_wait", "rbsc_serve_stats_get",
 ]
@@ -324,6 +324,7 @@ def load():
     lib.rbsc_gen_lift_host.argtypes = [ctypes.c_uint32, ctypes.c_double, ctypes.c_uint32, ctypes.c_uint64,
                                        ctypes.c_int32, P(HostGraph)]
     lib.rbsc_refine_edge_batches.argtypes = [vp, P(Csr), ctypes.c_uint64, ctypes.c_int32, vp, P(Stats), P(EdgeBatchInfo)]
+    lib.rbsc_refine_f64.argtypes = [vp, P(Csr), vp, vp, vp, P(Stats)]
     lib.rbsc_serve_opts_default.argtypes = [P(ServeOpts)]
     lib.rbsc_serve_opts_default.restype = None
     lib.rbsc_serve_footprint.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int32, ctypes.c_uint32]

@@ -23,7 +23,7 @@ CLI = os.path.join(PKG, "rbsc")
 
 NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-CU_SOURCES = ["rbsc.cu", "sortrelabel.cu", "gen.cu", "noalloc.cu", "batch.cu", "serve.cu", "edgebatch.cu"]
+CU_SOURCES = ["rbsc.cu", "sortrelabel.cu", "gen.cu", "noalloc.cu", "batch.cu", "serve.cu", "edgebatch.cu", "lump64.cu"]
 CXX_SOURCES = ["parse.cpp", "wlgen.cpp", "genhost.cpp", "bvgraph.cpp", "csrcache.cpp"]
 NVFLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC,-O3",
            f"-I{os.path.join(ROOT, 'include')}"]

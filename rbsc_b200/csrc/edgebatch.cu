@@ -238,41 +238,6 @@ struct Runs {
     uint64_t* wt = nullptr;  // null: every weight 1
 };
 
-struct Scratch {
-    rbsc_ctx* ctx;
-    std::vector<void*> blocks;
-    explicit Scratch(rbsc_ctx* c) : ctx(c) {}
-    ~Scratch()
-    {
-        for (void*& b : blocks) dev_free(ctx, b);
-    }
-    template <typename T> rbsc_status get(T** p, size_t count)
-    {
-        void* b = nullptr;
-        const rbsc_status st = dev_alloc(ctx, &b, std::max<size_t>(count, 1) * sizeof(T));
-        if (st != RBSC_OK) return st;
-        blocks.push_back(b);
-        *p = static_cast<T*>(b);
-        return RBSC_OK;
-    }
-    void release(void* p)
-    {
-        for (void*& b : blocks)
-            if (b == p) dev_free(ctx, b);
-    }
-};
-
-#define EK(call)                                                              \
-    do {                                                                      \
-        cudaError_t e_ = (call);                                              \
-        if (e_ != cudaSuccess) return rbsc_cuda_fail(ctx, e_, #call, __LINE__); \
-    } while (0)
-#define EKS(call)                      \
-    do {                               \
-        rbsc_status s_ = (call);       \
-        if (s_ != RBSC_OK) return s_;  \
-    } while (0)
-
 // The local graph of runs [k0, k1) over n nodes, refined exactly from the
 // batch's initial colours; canonical labels into lab.
 rbsc_status refine_batch(rbsc_ctx* ctx, const Runs& rs, uint32_t n, uint32_t k0, uint32_t k1, const uint8_t* has, bool first_batch,

@@ -4,6 +4,8 @@
 #include <map>
 #include <string>
 #include <unordered_map>
+#include <vector>
+#include <algorithm>
 #include <cuda_runtime.h>
 
 #include "../../include/rbsc.h"
@@ -167,6 +169,46 @@ rbsc_status graph_prepare(rbsc_ctx* ctx, rbsc_graph* g);
 rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted);
 rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init, uint32_t* d_out, rbsc_stats* stats,
                             rbsc_kernel_times* kt);
+
+// Device scratch of one call: every block is released when it goes out of
+// scope (the modules that build their own working set per call).
+struct Scratch {
+    rbsc_ctx* ctx;
+    std::vector<void*> blocks;
+    explicit Scratch(rbsc_ctx* c) : ctx(c) {}
+    ~Scratch()
+    {
+        for (void*& b : blocks) dev_free(ctx, b);
+    }
+    Scratch(const Scratch&) = delete;
+    Scratch& operator=(const Scratch&) = delete;
+    template <typename T> rbsc_status get(T** p, size_t count)
+    {
+        void* b = nullptr;
+        const rbsc_status st = dev_alloc(ctx, &b, std::max<size_t>(count, 1) * sizeof(T));
+        if (st != RBSC_OK) return st;
+        blocks.push_back(b);
+        *p = static_cast<T*>(b);
+        return RBSC_OK;
+    }
+    void release(void* p)
+    {
+        for (void*& b : blocks)
+            if (b == p) dev_free(ctx, b);
+    }
+};
+
+// Status propagation inside functions that have a `ctx` in scope.
+#define EK(call)                                                              \
+    do {                                                                      \
+        cudaError_t e_ = (call);                                              \
+        if (e_ != cudaSuccess) return rbsc_cuda_fail(ctx, e_, #call, __LINE__); \
+    } while (0)
+#define EKS(call)                      \
+    do {                               \
+        rbsc_status s_ = (call);       \
+        if (s_ != RBSC_OK) return s_;  \
+    } while (0)
 
 // sort-based relabel (sortrelabel.cu)
 rbsc_status ensure_sort_relabel_bufs(rbsc_ctx* ctx, rbsc_graph* g);
