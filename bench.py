@@ -471,6 +471,7 @@ def run_ours(args, rank, world, local_rank):
     served = None if args.serve_requests <= 0 or not single else run_served(args, world, dist, local_rank)
     law = None if args.law_steps <= 0 or not single else run_law(args, ctx)
     streamed = None if args.stream_scale <= 0 or not single else run_streamed(args, ctx, local_rank)
+    lump_f64 = None if args.f64_scale <= 0 or not single else run_lump_f64(args, ctx)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -488,7 +489,8 @@ def run_ours(args, rank, world, local_rank):
                 "phase_ms": {"init": results[-1].init_ms, "loop": results[-1].loop_ms, "verify": results[-1].verify_ms},
                 "wall_ms_per_step": 1000.0 * wall / args.steps, "roofline": roofline, "cpu_baseline": cpu,
                 "e2e": e2e, "gpu_launches": launches, "clocks": clk, "relabel": args.relabel, "autotune": tune, "batched": batched,
-                "served": served, "law_cnr2000": law, "streamed": streamed, "reference_gpu_program": ref_gpu}
+                "served": served, "law_cnr2000": law, "streamed": streamed, "lump_f64": lump_f64,
+                "reference_gpu_program": ref_gpu}
         print(json.dumps(line))
     g.free()
     ctx.close()
@@ -774,6 +776,64 @@ def run_law(args, ctx):
                               "B200 by tests/golden/make_law_golden.py --gpu; compare with e2e_ms"}
 
 
+def run_lump_f64(args, ctx):
+    """Lumping with double weights (rbsc_refine_f64): R-MAT scale
+    args.f64_scale, edge factor 16, every arc weighted k/2 with k uniform in
+    0..8 (decimal texts "0.0" .. "4.0" in the minimiser's MDP text; its reader
+    turns every one of them into exactly k/2).  One-shot calls from host
+    arrays (device time and wall time of the call).  cpu_baseline: Valmari's
+    minimiser built with double weights (oracle/_ref/ref_valmari_f64, compiled
+    unmodified from the reference's src/part_ref), single-threaded, its own
+    timer around minimize(); its partition must equal ours."""
+    import numpy as np
+    import rbsc_b200 as R
+    off, idx = R.gen_rmat_host(args.f64_scale, 16, seed=args.seed)
+    n, m = len(off) - 1, len(idx)
+    rng = np.random.default_rng(args.seed)
+    k = rng.integers(0, 9, m)
+    w = k / 2.0
+    ctx.refine_f64(off, idx, w)
+    res = [ctx.refine_f64(off, idx, w) for _ in range(args.f64_steps)]
+    r0 = res[0]
+    assert all(r.blocks == r0.blocks and r.rounds == r0.rounds and r.verified == 1 for r in res)
+    dev = statistics.median([r.device_ms for r in res])
+    wall = statistics.median([r.time_s for r in res]) * 1e3
+    out = {"workload": f"rmat{args.f64_scale}_ef16, weights k/2 (k uniform 0..8), uniform initial colours",
+           "nodes": n, "arcs": m, "rounds": r0.rounds, "blocks": r0.blocks, "device_ms": dev, "call_ms": wall,
+           "edge_rounds_per_s": m * r0.rounds / (dev / 1e3), "gpu_launches_per_call": int(r0.kernel_launches),
+           "h2d_bytes": int(r0.h2d_bytes), "d2h_bytes": int(r0.d2h_bytes), "cpu_baseline": None}
+    if args.no_cpu_baseline:
+        return out
+    import subprocess
+    from oracle import oracle  # the reference program, as the checker and CPU baseline
+    if not os.path.exists(oracle.REF_VALMARI_F64):
+        out["cpu_baseline"] = {"unavailable": "oracle/_ref/ref_valmari_f64 not built"}
+        return out
+    texts = [f"{x / 2:.1f}" for x in range(9)]
+    lines = [f"{n} 0 0 {m} 1\n"]
+    src = np.repeat(np.arange(n, dtype=np.int64), np.diff(off.astype(np.int64))) + 1
+    tk = np.array(texts)[k]
+    lines.append("\n".join(f"{a} {t} {b}" for a, t, b in zip(src.tolist(), tk.tolist(), (idx.astype(np.int64) + 1).tolist())))
+    lines.append("\n")
+    t0 = time.perf_counter()
+    txt = subprocess.run([oracle.REF_VALMARI_F64], input="".join(lines).encode(), capture_output=True, check=True,
+                         timeout=1800).stdout.decode().split("\n")
+    wall_ref = time.perf_counter() - t0
+    lab = np.array(txt[3].split()[1:], dtype=np.int64)
+    # canonical labels of the minimiser's block numbers: smallest state id
+    first = {}
+    canon = np.empty(n, dtype=np.uint32)
+    for i, b in enumerate(lab.tolist()):
+        canon[i] = first.setdefault(b, i)
+    out_lab = ctx.refine_f64(off, idx, w).labels
+    out["cpu_baseline"] = {"kind": "reference", "program": "Valmari minimiser, MDP_weight_is_double (src/part_ref)",
+                           "cores": 1, "minimize_s": float(txt[0]), "wall_s_with_parse": wall_ref,
+                           "blocks": int(txt[2]), "same_partition": bool(np.array_equal(canon, out_lab)),
+                           "speedup_device": float(txt[0]) * 1e3 / dev, "speedup_call": float(txt[0]) * 1e3 / wall}
+    assert out["cpu_baseline"]["same_partition"], "double-weight lumping differs from the reference minimiser"
+    return out
+
+
 def run_streamed(args, ctx, local_rank):
     """Arcs in host memory (the out-of-HBM configuration): R-MAT scale
     args.stream_scale, edge factor args.stream_ef, generated on the device in
@@ -871,6 +931,8 @@ def main():
     ap.add_argument("--stream-scale", type=int, default=28, help="R-MAT scale of the streamed graph (0: skip)")
     ap.add_argument("--stream-ef", type=int, default=32)
     ap.add_argument("--stream-steps", type=int, default=2)
+    ap.add_argument("--f64-scale", type=int, default=20, help="R-MAT scale of the double-weight lumping (0: skip)")
+    ap.add_argument("--f64-steps", type=int, default=3)
     ap.add_argument("--serve-rate", type=float, default=200.0, help="Poisson arrival rate, requests/s")
     ap.add_argument("--serve-pool", type=int, default=48, help="distinct graphs the requests draw from")
     ap.add_argument("--serve-slots", type=int, default=4)

@@ -273,7 +273,7 @@ rbsc_status rbsc_refine_edge_batches(rbsc_ctx* ctx, const rbsc_csr* host_graph, 
  * every block have equal rounded sums into every block; labels canonical
  * (smallest node id per block), checked exactly before they are returned.
  * host_graph->weights must be NULL: `weights` (host, m doubles, finite, of
- * magnitude below 2^960) replaces it; m < 2^32.  stats: rounds (passes until
+ * magnitude below 2^960) replaces it; m < 2^32, n <= 2^31.  stats: rounds (passes until
  * the block count stopped changing), blocks, verified, repairs, device_ms,
  * round_blocks, kernel_launches.  The minimiser adds a block's weights in
  * the order of the block's members: its float can differ from this one's

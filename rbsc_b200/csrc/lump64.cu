@@ -130,7 +130,7 @@ __global__ void k_l64_sums(const L64Counters* __restrict__ c, uint32_t lb, const
 {
     const uint32_t G = c->groups;
     const uint64_t mask = (1ull << lb) - 1ull;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t b = gstart[g], e = gstart[g + 1];
         double s = 0.0;
         for (uint32_t i = b; i < e; ++i) s += w[vals[i]];
@@ -160,9 +160,9 @@ __global__ void k_l64_insert(uint32_t n, const uint32_t* __restrict__ col, const
                              const uint32_t* __restrict__ aux, uint64_t seed, uint32_t stamp, Entry* __restrict__ tab,
                              uint32_t log2size, uint32_t* __restrict__ slot, L64Counters* __restrict__ c)
 {
-    for (uint32_t base = blockIdx.x * blockDim.x + (threadIdx.x & ~31u); base < n; base += gridDim.x * blockDim.x) {
-        const uint32_t u = base + (threadIdx.x & 31);
-        const bool need = u < n;
+    for (uint64_t base = blockIdx.x * (uint64_t)blockDim.x + (threadIdx.x & ~31u); base < n; base += (uint64_t)gridDim.x * blockDim.x) {
+        const bool need = base + (threadIdx.x & 31) < n;
+        const uint32_t u = (uint32_t)(base + (threadIdx.x & 31));
         uint64_t k1 = 0;
         uint32_t k2 = stamp;
         if (need) {
@@ -185,7 +185,7 @@ __global__ void k_l64_insert(uint32_t n, const uint32_t* __restrict__ col, const
 __global__ void k_l64_relabel(uint32_t n, const Entry* __restrict__ tab, const uint32_t* __restrict__ slot,
                               uint32_t* __restrict__ col)
 {
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t* v = reinterpret_cast<const uint32_t*>(tab + slot[u]) + 3;
         col[u] = __ldg(v) & kLabelMask;
     }
@@ -197,7 +197,7 @@ __global__ void k_l64_nz_count(const L64Counters* __restrict__ c, uint32_t lb, c
                                uint32_t* __restrict__ cnt, uint32_t* __restrict__ nzflag)
 {
     const uint32_t G = c->groups;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x) {
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
         const bool nz = bits[g] != 0u;
         nzflag[g] = nz ? 1u : 0u;
         if (nz) atomicAdd(&cnt[(uint32_t)(keys[gstart[g]] >> lb)], 1u);
@@ -211,7 +211,7 @@ __global__ void k_l64_nz_scatter(const L64Counters* __restrict__ c, uint32_t lb,
 {
     const uint32_t G = c->groups;
     const uint64_t mask = (1ull << lb) - 1ull;
-    for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < G; g += gridDim.x * blockDim.x)
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x)
         if (bits[g]) {
             const uint32_t p = nzpos[g];
             nzlab[p] = (uint32_t)(keys[gstart[g]] & mask);
@@ -224,7 +224,7 @@ __global__ void k_l64_check(uint32_t n, const uint32_t* __restrict__ col, const 
                             const uint32_t* __restrict__ nzlab, const uint32_t* __restrict__ nzbits,
                             uint32_t* __restrict__ fail, L64Counters* __restrict__ c)
 {
-    for (uint32_t u = blockIdx.x * blockDim.x + threadIdx.x; u < n; u += gridDim.x * blockDim.x) {
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t r = col[u];
         bool bad = false;
         if (r != u) {
@@ -249,6 +249,7 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     if (host_graph->m && !weights) return rbsc_fail(ctx, RBSC_ERR_INVALID, "rbsc_refine_f64: null weights");
     if (host_graph->n && !out_labels) return rbsc_fail(ctx, RBSC_ERR_INVALID, "null output");
     if (host_graph->m > 0xffffffffull) return rbsc_fail(ctx, RBSC_ERR_INVALID, "rbsc_refine_f64: more than 2^32 - 1 arcs");
+    if (host_graph->n > (1u << 31)) return rbsc_fail(ctx, RBSC_ERR_INVALID, "rbsc_refine_f64: more than 2^31 nodes");
     auto t0 = std::chrono::steady_clock::now();
     if (stats) std::memset(stats, 0, sizeof *stats);
     const uint64_t lc0 = rbsc::launch_counter();
