@@ -11,24 +11,30 @@
 //
 // Signature passes, as the integer path, but the signature of a node is no
 // longer a sum of per-arc terms (a float-rounded sum is not additive), so a
-// pass first groups the arcs:
-//   1. k_l64_keys: one 64-bit key per arc, (row << lb) | label of its head,
-//      carrying the arc's index;
-//   2. the stable radix sort (radix.cuh) on those 2*lb bits: arcs grouped by
-//      (row, successor block), in arc order inside a group;
-//   3. k_l64_heads, a scan and k_l64_gstart: where every group starts;
-//   4. k_l64_sums: one thread per group adds its weights in arc order (double),
-//      rounds the sum to float; a nonzero sum adds the hash of (block, float
-//      bits) to the row's signature (wrap-around 64 + 32-bit sums, so the
-//      order of the adds does not matter);
-//   5. k_l64_insert + k_l64_relabel: classes of (label, signature) in the
+// pass first groups the arcs by (successor block, row):
+//   1. k_l64_rep_flags + a scan + k_l64_block_ids: the dense id of every
+//      block (its rank among the blocks' smallest nodes), per node;
+//   2. k_l64_keys: one 64-bit key per arc, (block id of its head << lb) | row,
+//      carrying the arc's weight;
+//   3. the stable radix sort (radix.cuh) on the block-id bits only (the
+//      rows are in order already and the sort is stable): arcs grouped by
+//      (block, row), in arc order inside a group.  The first pass of a
+//      uniform start (one block) sorts nothing;
+//   4. k_l64_heads, a scan and k_l64_gstart: where every group starts;
+//   5. k_l64_sums: one thread per group adds its weights in arc order (double,
+//      read in sorted order), rounds the sum to float; a nonzero sum adds the
+//      hash of (block, float bits) to the row's signature (wrap-around 64 +
+//      32-bit sums, so the order of the adds does not matter; neighbouring
+//      groups belong to different rows);
+//   6. k_l64_insert + k_l64_relabel: classes of (label, signature) in the
 //      stamped 16-byte relabel table of the integer path, new label = smallest
 //      member;
-//   6. the host reads the class count: unchanged = fixpoint.
+//   7. the host reads the class count: unchanged = fixpoint.
 // Exact check at the fixpoint (the groups of the last pass are those of the
-// final partition, whose canonical labels the pass left unchanged): every
-// node's list of (block, float bits) over its nonzero groups must equal that
-// of its block's smallest node.  Nodes that differ are split off (key =
+// final partition, whose canonical labels the pass left unchanged): the
+// nonzero groups are compacted and re-sorted by row (stable, row bits only),
+// and every node's list of (block, float bits) must equal that of its
+// block's smallest node.  Nodes that differ are split off (key =
 // (label, failed)) and the passes resume; the result is returned only once
 // the check passed.  Weights must be finite with magnitude below 2^960 (so no
 // sum of up to 2^32 of them overflows a double).
@@ -64,7 +70,8 @@ struct L64Counters {
     uint32_t failed;   // nodes that failed the exact check
     uint32_t nonzero;  // groups with a nonzero rounded sum
     uint32_t error;    // kErr* bits
-    uint32_t pad[3];
+    uint32_t long_groups;  // groups of more than kShortGroup arcs, listed for k_l64_long_sums
+    uint32_t pad[2];
 };
 
 constexpr uint32_t kL64BadWeight = 32u;  // a weight that is not finite or not below 2^960
@@ -87,16 +94,32 @@ __global__ void k_l64_rows(uint32_t n, const uint64_t* __restrict__ off, uint32_
         for (uint64_t a = off[u] + lane; a < off[u + 1]; a += 32) src[a] = (uint32_t)u;
 }
 
+// flag[u] = u is the smallest node of its block
+__global__ void k_l64_rep_flags(uint32_t n, const uint32_t* __restrict__ col, uint32_t* __restrict__ flag)
+{
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x)
+        flag[u] = col[u] == (uint32_t)u ? 1u : 0u;
+}
+
+// bid[u] = dense id of u's block (rank[] = exclusive scan of the flags)
+__global__ void k_l64_block_ids(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ rank,
+                                uint32_t* __restrict__ bid)
+{
+    for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x)
+        bid[u] = rank[col[u]];
+}
+
 __global__ void k_l64_keys(uint64_t m, uint32_t lb, const uint32_t* __restrict__ src, const uint32_t* __restrict__ idx,
-                           const uint32_t* __restrict__ col, unsigned long long* __restrict__ keys, uint32_t* __restrict__ vals)
+                           const uint32_t* __restrict__ bid, const unsigned long long* __restrict__ w,
+                           unsigned long long* __restrict__ keys, unsigned long long* __restrict__ vals)
 {
     for (uint64_t a = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; a < m; a += (uint64_t)gridDim.x * blockDim.x) {
-        keys[a] = ((unsigned long long)src[a] << lb) | col[idx[a]];
-        vals[a] = (uint32_t)a;
+        keys[a] = ((unsigned long long)bid[idx[a]] << lb) | src[a];
+        vals[a] = w[a];
     }
 }
 
-// flag[i] = position i starts a (row, block) group
+// flag[i] = position i starts a (block, row) group
 __global__ void k_l64_heads(uint64_t m, const unsigned long long* __restrict__ keys, uint32_t* __restrict__ flag)
 {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
@@ -120,36 +143,91 @@ __device__ __forceinline__ void group_hash(uint32_t lab, uint32_t bits, uint64_t
     h2 = fmix32((lab * 0x9e3779b1u) ^ fmix32(bits ^ salt2));
 }
 
-// One thread per group: the double sum of its weights in arc order, rounded
-// to float; bits[g] = the float's bits, 0 for a sum that rounds to zero (of
-// either sign), whose group adds nothing.
-__global__ void k_l64_sums(const L64Counters* __restrict__ c, uint32_t lb, const uint32_t* __restrict__ gstart,
-                           const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ vals,
-                           const double* __restrict__ w, uint64_t salt1, uint32_t salt2, int hash_bits,
-                           Sig* __restrict__ sig, uint32_t* __restrict__ bits)
+// The rounded sum of one group, its bits and its signature term.
+__device__ __forceinline__ void group_done(uint64_t g, double s, unsigned long long k, uint32_t lb, uint64_t salt1,
+                                           uint32_t salt2, int hash_bits, Sig* __restrict__ sig, uint32_t* __restrict__ bits)
+{
+    const float f = __double2float_rn(s);
+    const uint32_t fb = f != 0.0f ? __float_as_uint(f) : 0u;
+    bits[g] = fb;
+    if (fb) {
+        uint64_t h1;
+        uint32_t h2;
+        group_hash((uint32_t)(k >> lb), fb, salt1, salt2, h1, h2);
+        if (hash_bits) {  // test hook: truncated (or no) signatures
+            h1 = (hash_bits >= 64 || hash_bits < 0) ? 0ull : (h1 & ((1ull << hash_bits) - 1ull));
+            h2 = 0u;
+        }
+        const uint32_t row = (uint32_t)(k & ((1ull << lb) - 1ull));
+        atomicAdd(&sig[row].s1, (unsigned long long)h1);
+        atomicAdd(&sig[row].s2, h2);
+    }
+}
+
+// One thread per group of at most kShortGroup arcs: the double sum of its
+// weights in arc order (the sort kept it), rounded to float; bits[g] = the
+// float's bits, 0 for a sum that rounds to zero (of either sign), whose group
+// adds nothing.  Longer groups are listed for k_l64_long_sums.
+constexpr uint32_t kShortGroup = 32;
+
+__global__ void k_l64_sums(L64Counters* __restrict__ c, uint32_t lb, const uint32_t* __restrict__ gstart,
+                           const unsigned long long* __restrict__ keys, const unsigned long long* __restrict__ vals,
+                           uint64_t salt1, uint32_t salt2, int hash_bits, Sig* __restrict__ sig, uint32_t* __restrict__ bits,
+                           uint32_t* __restrict__ long_list)
 {
     const uint32_t G = c->groups;
-    const uint64_t mask = (1ull << lb) - 1ull;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t b = gstart[g], e = gstart[g + 1];
-        double s = 0.0;
-        for (uint32_t i = b; i < e; ++i) s += w[vals[i]];
-        const float f = __double2float_rn(s);
-        const uint32_t fb = f != 0.0f ? __float_as_uint(f) : 0u;
-        bits[g] = fb;
-        if (fb) {
-            const unsigned long long k = keys[b];
-            uint64_t h1;
-            uint32_t h2;
-            group_hash((uint32_t)(k & mask), fb, salt1, salt2, h1, h2);
-            if (hash_bits) {  // test hook: truncated (or no) signatures
-                h1 = (hash_bits >= 64 || hash_bits < 0) ? 0ull : (h1 & ((1ull << hash_bits) - 1ull));
-                h2 = 0u;
-            }
-            const uint32_t row = (uint32_t)(k >> lb);
-            atomicAdd(&sig[row].s1, (unsigned long long)h1);
-            atomicAdd(&sig[row].s2, h2);
+        if (e - b > kShortGroup) {
+            long_list[atomicAdd(&c->long_groups, 1u)] = (uint32_t)g;
+            continue;
         }
+        double s = 0.0;
+        uint32_t i = b;
+        // the loads of four weights side by side; the adds stay in order
+        for (; i + 4u <= e; i += 4u) {
+            const double w0 = __longlong_as_double((long long)vals[i]), w1 = __longlong_as_double((long long)vals[i + 1]);
+            const double w2 = __longlong_as_double((long long)vals[i + 2]), w3 = __longlong_as_double((long long)vals[i + 3]);
+            s += w0;
+            s += w1;
+            s += w2;
+            s += w3;
+        }
+        for (; i < e; ++i) s += __longlong_as_double((long long)vals[i]);
+        group_done(g, s, keys[b], lb, salt1, salt2, hash_bits, sig, bits);
+    }
+}
+
+// One warp per long group: the lanes load 32 weights at a time (the next 32
+// while lane 0 adds the current ones, handed over by shuffles in lane order),
+// so the sum is the same arc-order double sum as k_l64_sums', at the pace of
+// the dependent adds rather than of one load per few weights.
+__global__ void __launch_bounds__(kT) k_l64_long_sums(const L64Counters* __restrict__ c, uint32_t lb,
+                                                      const uint32_t* __restrict__ gstart,
+                                                      const unsigned long long* __restrict__ keys,
+                                                      const unsigned long long* __restrict__ vals, uint64_t salt1,
+                                                      uint32_t salt2, int hash_bits, Sig* __restrict__ sig,
+                                                      uint32_t* __restrict__ bits, const uint32_t* __restrict__ long_list)
+{
+    const uint32_t L = c->long_groups;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
+    for (uint64_t i = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < L; i += warps) {
+        const uint32_t g = long_list[i];
+        const uint32_t b = gstart[g], e = gstart[g + 1];
+        double s = 0.0;
+        double x = b + lane < e ? __longlong_as_double((long long)vals[b + lane]) : 0.0;
+        for (uint32_t a0 = b; a0 < e; a0 += 32) {
+            const uint32_t a1 = a0 + 32;
+            const double nx = a1 + lane < e ? __longlong_as_double((long long)vals[a1 + lane]) : 0.0;
+            const uint32_t cnt = min(32u, e - a0);
+            for (uint32_t j = 0; j < cnt; ++j) {
+                const double v = __shfl_sync(0xffffffffu, x, j);
+                if (lane == 0) s += v;
+            }
+            x = nx;
+        }
+        if (lane == 0) group_done(g, s, keys[b], lb, salt1, salt2, hash_bits, sig, bits);
     }
 }
 
@@ -191,39 +269,42 @@ __global__ void k_l64_relabel(uint32_t n, const Entry* __restrict__ tab, const u
     }
 }
 
-// nonzero groups per row (cnt zeroed before) and their flags
-__global__ void k_l64_nz_count(const L64Counters* __restrict__ c, uint32_t lb, const uint32_t* __restrict__ gstart,
-                               const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ bits,
-                               uint32_t* __restrict__ cnt, uint32_t* __restrict__ nzflag)
+// nzflag[g] = group g has a nonzero rounded sum
+__global__ void k_l64_nz_flags(const L64Counters* __restrict__ c, const uint32_t* __restrict__ bits,
+                               uint32_t* __restrict__ nzflag)
 {
     const uint32_t G = c->groups;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
-        const bool nz = bits[g] != 0u;
-        nzflag[g] = nz ? 1u : 0u;
-        if (nz) atomicAdd(&cnt[(uint32_t)(keys[gstart[g]] >> lb)], 1u);
-    }
+    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x)
+        nzflag[g] = bits[g] != 0u ? 1u : 0u;
 }
 
-// the nonzero groups, compacted in (row, block) order
-__global__ void k_l64_nz_scatter(const L64Counters* __restrict__ c, uint32_t lb, const uint32_t* __restrict__ gstart,
+// the nonzero groups, compacted: ckey = (row << cw) | block id, cval = float
+// bits; cnt[row] counts them (zeroed before)
+__global__ void k_l64_nz_compact(const L64Counters* __restrict__ c, uint32_t lb, uint32_t cw, const uint32_t* __restrict__ gstart,
                                  const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ bits,
-                                 const uint32_t* __restrict__ nzpos, uint32_t* __restrict__ nzlab, uint32_t* __restrict__ nzbits)
+                                 const uint32_t* __restrict__ nzpos, unsigned long long* __restrict__ ckey,
+                                 uint32_t* __restrict__ cval, uint32_t* __restrict__ cnt)
 {
     const uint32_t G = c->groups;
     const uint64_t mask = (1ull << lb) - 1ull;
     for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x)
         if (bits[g]) {
+            const unsigned long long k = keys[gstart[g]];
+            const uint32_t row = (uint32_t)(k & mask);
             const uint32_t p = nzpos[g];
-            nzlab[p] = (uint32_t)(keys[gstart[g]] & mask);
-            nzbits[p] = bits[g];
+            ckey[p] = ((unsigned long long)row << cw) | (k >> lb);
+            cval[p] = bits[g];
+            atomicAdd(&cnt[row], 1u);
         }
 }
 
-// fail[u] = u's (block, float bits) list differs from its block's smallest node's
-__global__ void k_l64_check(uint32_t n, const uint32_t* __restrict__ col, const uint32_t* __restrict__ first,
-                            const uint32_t* __restrict__ nzlab, const uint32_t* __restrict__ nzbits,
+// fail[u] = u's (block, float bits) list differs from its block's smallest
+// node's; the lists are the row-sorted compacted groups [first[u], first[u+1])
+__global__ void k_l64_check(uint32_t n, uint32_t cw, const uint32_t* __restrict__ col, const uint32_t* __restrict__ first,
+                            const unsigned long long* __restrict__ ckey, const uint32_t* __restrict__ cval,
                             uint32_t* __restrict__ fail, L64Counters* __restrict__ c)
 {
+    const unsigned long long bmask = (1ull << cw) - 1ull;
     for (uint64_t u = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; u < n; u += (uint64_t)gridDim.x * blockDim.x) {
         const uint32_t r = col[u];
         bool bad = false;
@@ -231,7 +312,7 @@ __global__ void k_l64_check(uint32_t n, const uint32_t* __restrict__ col, const 
             const uint32_t bu = first[u], eu = first[u + 1], br = first[r], er = first[r + 1];
             bad = eu - bu != er - br;
             for (uint32_t i = 0; !bad && i < eu - bu; ++i)
-                bad = nzlab[bu + i] != nzlab[br + i] || nzbits[bu + i] != nzbits[br + i];
+                bad = (ckey[bu + i] & bmask) != (ckey[br + i] & bmask) || cval[bu + i] != cval[br + i];
         }
         fail[u] = bad ? 1u : 0u;
         if (bad) atomicAdd(&c->failed, 1u);
@@ -272,12 +353,13 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     }
     const double* w = reinterpret_cast<const double*>(g->d_wt);
     Scratch sc(ctx);
-    const uint32_t lb = N > 1 ? 32u - (uint32_t)__builtin_clz(N - 1u) : 1u;
+    const auto bits_of = [](uint64_t v) -> uint32_t { return v ? 64u - (uint32_t)__builtin_clzll(v) : 0u; };
+    const uint32_t lb = std::max(1u, bits_of(N - 1u));  // row bits of a key
     uint32_t log2tab = 10;
     while (log2tab < 33 && (1ull << log2tab) < 2ull * N) ++log2tab;
-    uint32_t *col = nullptr, *slot = nullptr, *fail = nullptr, *first = nullptr, *src = nullptr, *vals = nullptr,
-             *vals_alt = nullptr, *gid = nullptr, *gstart = nullptr, *bits = nullptr, *nzlab = nullptr, *nzbits = nullptr;
-    unsigned long long *keys = nullptr, *keys_alt = nullptr;
+    uint32_t *col = nullptr, *slot = nullptr, *fail = nullptr, *first = nullptr, *bid = nullptr, *src = nullptr,
+             *gid = nullptr, *gstart = nullptr, *bits = nullptr, *cval = nullptr, *cval_alt = nullptr;
+    unsigned long long *keys = nullptr, *keys_alt = nullptr, *vals = nullptr, *vals_alt = nullptr;
     Sig* sig = nullptr;
     Entry* tab = nullptr;
     L64Counters* dc = nullptr;
@@ -286,6 +368,7 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     EKS(sc.get(&slot, N));
     EKS(sc.get(&fail, N));
     EKS(sc.get(&first, (size_t)N + 1));
+    EKS(sc.get(&bid, N));
     EKS(sc.get(&sig, N));
     EKS(sc.get(&tab, (size_t)1 << log2tab));
     EKS(sc.get(&dc, 1));
@@ -297,8 +380,8 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     EKS(sc.get(&gid, M + 1));
     EKS(sc.get(&gstart, M + 1));
     EKS(sc.get(&bits, M));
-    EKS(sc.get(&nzlab, M));
-    EKS(sc.get(&nzbits, M));
+    EKS(sc.get(&cval, M));
+    EKS(sc.get(&cval_alt, M));
     const uint64_t big = std::max<uint64_t>(M, N) + 1;
     EKS(sc.get((char**)&tmp, std::max(radix_temp_bytes(M), scan_temp_bytes<uint32_t>(big)) + 1024));
     EK(cudaMemsetAsync(dc, 0, sizeof(L64Counters), s));
@@ -343,7 +426,6 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
         if (stamp == 1u) EK(cudaMemsetAsync(tab, 0, sizeof(Entry) << log2tab, s));
         return RBSC_OK;
     };
-    auto dev0 = std::chrono::steady_clock::now();
     cudaEvent_t e0 = ctx->ev[0], e1 = ctx->ev[1];
     EK(cudaEventRecord(e0, s));
     EKS(relabel(1, d_init));
@@ -355,28 +437,40 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     uint32_t rounds = 0, repairs = 0;
     bool verified = false;
     const int hash_bits = ctx->opts.test_hash_bits;
+    const unsigned long long* w64 = reinterpret_cast<const unsigned long long*>(g->d_wt);
+    const unsigned long_grid = (unsigned)ctx->sm_count * 8;
     for (;;) {
-        // one signature pass
+        // one signature pass; prev = the current number of blocks
+        const uint32_t cb = bits_of(prev - 1u);  // block-id bits of a key
         bool in_alt = false;
         if (M) {
             ++rbsc::launch_counter();
-            k_l64_keys<<<grid_of(M), kT, 0, s>>>(M, lb, src, g->d_idx, col, keys, vals);
+            k_l64_rep_flags<<<grid_of(N), kT, 0, s>>>(N, col, first);
+            EK((exclusive_scan<uint32_t, uint32_t>(first, first, N, (uint32_t*)nullptr, tmp, s)));
+            ++rbsc::launch_counter();
+            k_l64_block_ids<<<grid_of(N), kT, 0, s>>>(N, col, first, bid);
+            ++rbsc::launch_counter();
+            k_l64_keys<<<grid_of(M), kT, 0, s>>>(M, lb, src, g->d_idx, bid, w64, keys, vals);
             EK(cudaGetLastError());
-            EK(radix_sort<uint32_t>(keys, keys_alt, vals, vals_alt, M, 0, (int)(2 * lb), tmp, s, &in_alt));
+            EK(radix_sort<unsigned long long>(keys, keys_alt, vals, vals_alt, M, (int)lb, (int)(lb + cb), tmp, s, &in_alt));
         }
         const unsigned long long* sk = in_alt ? keys_alt : keys;
-        const uint32_t* sv = in_alt ? vals_alt : vals;
+        const unsigned long long* sv = in_alt ? vals_alt : vals;
         EK(cudaMemsetAsync(sig, 0, sizeof(Sig) * N, s));
         EK(cudaMemsetAsync(&dc->groups, 0, 4, s));
+        EK(cudaMemsetAsync(&dc->long_groups, 0, 4, s));
         if (M) {
+            const uint64_t salt1 = pass_salt1(ctx->opts.seed, rounds);
+            const uint32_t salt2 = pass_salt2(ctx->opts.seed, rounds);
             ++rbsc::launch_counter();
             k_l64_heads<<<grid_of(M), kT, 0, s>>>(M, sk, gid);
             EK((exclusive_scan<uint32_t, uint32_t>(gid, gid, M, &dc->groups, tmp, s)));
             ++rbsc::launch_counter();
             k_l64_gstart<<<grid_of(M), kT, 0, s>>>(M, sk, gid, dc, gstart);
             ++rbsc::launch_counter();
-            k_l64_sums<<<grid_of(M), kT, 0, s>>>(dc, lb, gstart, sk, sv, w, pass_salt1(ctx->opts.seed, rounds),
-                                                 pass_salt2(ctx->opts.seed, rounds), hash_bits, sig, bits);
+            k_l64_sums<<<grid_of(M), kT, 0, s>>>(dc, lb, gstart, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
+            ++rbsc::launch_counter();
+            k_l64_long_sums<<<long_grid, kT, 0, s>>>(dc, lb, gstart, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
             EK(cudaGetLastError());
         }
         EKS(relabel(0, nullptr));
@@ -390,19 +484,37 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
             continue;
         }
         if (!ctx->opts.verify) break;
-        // exact check over this pass's groups (the final partition's)
+        // exact check over this pass's groups (the final partition's): the
+        // nonzero ones compacted into the key buffers the sort did not end in,
+        // then sorted by row (stable: block order kept inside a row)
+        unsigned long long* ck = in_alt ? keys : keys_alt;
+        unsigned long long* ck_alt = in_alt ? keys_alt : keys;
+        const uint32_t cw = std::max(1u, cb);
         EK(cudaMemsetAsync(first, 0, 4ull * (N + 1), s));
         EK(cudaMemsetAsync(&dc->failed, 0, 4, s));
+        EK(cudaMemsetAsync(&dc->nonzero, 0, 4, s));
+        const uint32_t* cv = cval;
         if (M) {
             ++rbsc::launch_counter();
-            k_l64_nz_count<<<grid_of(M), kT, 0, s>>>(dc, lb, gstart, sk, bits, first, gid);
-            EK((exclusive_scan<uint32_t, uint32_t>(gid, gid, M, &dc->nonzero, tmp, s)));
+            k_l64_nz_flags<<<grid_of(M), kT, 0, s>>>(dc, bits, gid);
+            EK((exclusive_scan<uint32_t, uint32_t>(gid, gid, M, (uint32_t*)nullptr, tmp, s)));
             ++rbsc::launch_counter();
-            k_l64_nz_scatter<<<grid_of(M), kT, 0, s>>>(dc, lb, gstart, sk, bits, gid, nzlab, nzbits);
+            k_l64_nz_compact<<<grid_of(M), kT, 0, s>>>(dc, lb, cw, gstart, sk, bits, gid, ck, cval, first);
+            EK(cudaGetLastError());
+            // nonzero groups = the per-row counts' total (read back for the sort's size)
+            EK((exclusive_scan<uint32_t, uint32_t>(first, first, (uint64_t)N + 1, &dc->nonzero, tmp, s)));
+            EKS(read_counters());
+            bool c_alt = false;
+            EK(radix_sort<uint32_t>(ck, ck_alt, cval, cval_alt, hc.nonzero, (int)cw, (int)(cw + lb), tmp, s, &c_alt));
+            if (c_alt) {
+                ck = ck_alt;
+                cv = cval_alt;
+            }
+        } else {
+            EK((exclusive_scan<uint32_t, uint32_t>(first, first, (uint64_t)N + 1, (uint32_t*)nullptr, tmp, s)));
         }
-        EK((exclusive_scan<uint32_t, uint32_t>(first, first, (uint64_t)N + 1, (uint32_t*)nullptr, tmp, s)));
         ++rbsc::launch_counter();
-        k_l64_check<<<grid_of(N), kT, 0, s>>>(N, col, first, nzlab, nzbits, fail, dc);
+        k_l64_check<<<grid_of(N), kT, 0, s>>>(N, cw, col, first, ck, cv, fail, dc);
         EK(cudaGetLastError());
         EKS(read_counters());
         if (hc.failed == 0) {
@@ -421,7 +533,6 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     EK(cudaStreamSynchronize(s));
     float dev_ms = 0.f;
     cudaEventElapsedTime(&dev_ms, e0, e1);
-    (void)dev0;
     if (stats) {
         stats->rounds = rounds;
         stats->blocks = prev;
