@@ -6,8 +6,9 @@
 //
 // Per pass: k_rs_hist counts the digits of a tile of 4096 keys per CTA into
 // hist[digit][tile]; an exclusive scan over that digit-major array gives every
-// (digit, tile) its output base; k_rs_scatter re-reads the tile and writes each
-// key to base + its stable rank.  Stability inside a tile: warp w owns keys
+// (digit, tile) its output base; k_rs_scatter re-reads the tile, stages it in
+// shared memory in digit order and writes each digit's run to its base
+// (coalesced stores).  Stability inside a tile: warp w owns keys
 // [w*512, (w+1)*512) of the tile, walks them 32 at a time in memory order, and
 // ranks equal digits with __match_any_sync.
 #pragma once
@@ -46,61 +47,100 @@ static __global__ void __launch_bounds__(kRsThreads) k_rs_hist(const unsigned lo
     hist[(uint64_t)threadIdx.x * ntiles + blockIdx.x] = s_hist[threadIdx.x];
 }
 
+// The tile's keys are first ranked (stable: the rank of a key among the equal
+// digits of its warp, warps in order), then staged in shared memory in digit
+// order, then written out from there: consecutive threads write consecutive
+// positions of a digit's run, so the stores coalesce (a warp's 32 keys span a
+// few runs instead of 32 buckets).  The values follow through the same
+// staging buffer.  Keys and values are read from global memory twice (ranking,
+// staging); the second read of a 4096-key tile hits L2.  Registers hold only
+// the ranks and destinations, so more CTAs fit per SM.
 template <typename V, bool HAS_V>
-static __global__ void __launch_bounds__(kRsThreads) k_rs_scatter(const unsigned long long* __restrict__ keys_in, const V* __restrict__ vals_in,
+static __global__ void __launch_bounds__(kRsThreads, 4) k_rs_scatter(const unsigned long long* __restrict__ keys_in, const V* __restrict__ vals_in,
                                                            unsigned long long* __restrict__ keys_out, V* __restrict__ vals_out, uint64_t n,
                                                            int shift, const uint32_t* __restrict__ hist_scan, uint32_t ntiles)
 {
     __shared__ uint32_t s_cnt[kRsWarps][kRsBins];
+    __shared__ uint32_t s_start[kRsBins];  // tile-local start of each digit's run
+    __shared__ uint32_t s_base[kRsBins];   // global position of that run
+    __shared__ unsigned long long s_stage[kRsTile];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads) (&s_cnt[0][0])[i] = 0;
     __syncthreads();
 
-    const uint64_t wbase = (uint64_t)blockIdx.x * kRsTile + (uint64_t)warp * (kRsIters * 32);
-    unsigned long long k[kRsIters];
-    V v[kRsIters];
-    uint32_t rank[kRsIters];
+    const uint64_t tbase = (uint64_t)blockIdx.x * kRsTile;
+    const uint32_t cnt = (uint32_t)(n - tbase < kRsTile ? n - tbase : kRsTile);
+    const uint64_t wbase = tbase + (uint64_t)warp * (kRsIters * 32);
+    uint32_t pos[kRsIters];  // rank among the warp's equal digits, then tile-local position
     const unsigned lt = (1u << lane) - 1u;
 #pragma unroll
     for (int it = 0; it < kRsIters; ++it) {
         const uint64_t i = wbase + (uint64_t)it * 32 + lane;
         const bool valid = i < n;
-        k[it] = valid ? keys_in[i] : ~0ull;
-        if (HAS_V) v[it] = valid ? vals_in[i] : V(0);
         const unsigned act = __ballot_sync(0xffffffffu, valid);
-        rank[it] = 0;
+        pos[it] = 0;
         if (valid) {
-            const uint32_t d = (uint32_t)(k[it] >> shift) & 0xffu;
+            const uint32_t d = (uint32_t)(keys_in[i] >> shift) & 0xffu;
             const unsigned peers = __match_any_sync(act, d);
             // rank among equal digits of this warp so far; leader bumps the count
             const uint32_t before = s_cnt[warp][d];
-            rank[it] = before + __popc(peers & lt);
+            pos[it] = before + __popc(peers & lt);
             __syncwarp(act);
             if (lane == __ffs(peers) - 1) s_cnt[warp][d] = before + __popc(peers);
             __syncwarp(act);
         }
     }
     __syncthreads();
-    // per digit: prefix over warps + this tile's global base
+    // per digit: prefix over warps, the digit's tile-local start and global base
     {
         const int d = threadIdx.x;  // kRsThreads == kRsBins
-        uint32_t run = hist_scan[(uint64_t)d * ntiles + blockIdx.x];
+        uint32_t run = 0;
 #pragma unroll
         for (int w = 0; w < kRsWarps; ++w) {
             const uint32_t c = s_cnt[w][d];
             s_cnt[w][d] = run;
             run += c;
         }
+        uint32_t total;
+        s_start[d] = block_excl_scan<uint32_t>(run, &total);
+        s_base[d] = hist_scan[(uint64_t)d * ntiles + blockIdx.x];
     }
     __syncthreads();
 #pragma unroll
     for (int it = 0; it < kRsIters; ++it) {
         const uint64_t i = wbase + (uint64_t)it * 32 + lane;
         if (i < n) {
-            const uint32_t d = (uint32_t)(k[it] >> shift) & 0xffu;
-            const uint32_t pos = s_cnt[warp][d] + rank[it];
-            keys_out[pos] = k[it];
-            if (HAS_V) vals_out[pos] = v[it];
+            const unsigned long long k = keys_in[i];
+            const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+            pos[it] += s_start[d] + s_cnt[warp][d];
+            s_stage[pos[it]] = k;
+        }
+    }
+    __syncthreads();
+    uint32_t dst[kRsIters];
+#pragma unroll
+    for (int q = 0; q < kRsIters; ++q) {
+        const uint32_t j = (uint32_t)q * kRsThreads + threadIdx.x;
+        if (j < cnt) {
+            const unsigned long long k = s_stage[j];
+            const uint32_t d = (uint32_t)(k >> shift) & 0xffu;
+            dst[q] = s_base[d] + (j - s_start[d]);
+            keys_out[dst[q]] = k;
+        }
+    }
+    if (HAS_V) {
+        V* s_val = reinterpret_cast<V*>(s_stage);
+        __syncthreads();
+#pragma unroll
+        for (int it = 0; it < kRsIters; ++it) {
+            const uint64_t i = wbase + (uint64_t)it * 32 + lane;
+            if (i < n) s_val[pos[it]] = vals_in[i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < kRsIters; ++q) {
+            const uint32_t j = (uint32_t)q * kRsThreads + threadIdx.x;
+            if (j < cnt) vals_out[dst[q]] = s_val[j];
         }
     }
 }
