@@ -20,16 +20,16 @@
 //      rows are in order already and the sort is stable): arcs grouped by
 //      (block, row), in arc order inside a group.  The first pass of a
 //      uniform start (one block) sorts nothing;
-//   4. k_l64_heads, a scan and k_l64_gstart: where every group starts;
-//   5. k_l64_sums: one thread per group adds its weights in arc order (double,
-//      read in sorted order), rounds the sum to float; a nonzero sum adds the
-//      hash of (block, float bits) to the row's signature (wrap-around 64 +
-//      32-bit sums, so the order of the adds does not matter; neighbouring
+//   4. k_l64_sums: the thread of a group's first position adds its weights in
+//      arc order (double, read in sorted order; a warp per group of more than
+//      32 arcs, k_l64_long_sums), rounds the sum to float; a nonzero sum adds
+//      the hash of (block, float bits) to the row's signature (wrap-around 64
+//      + 32-bit sums, so the order of the adds does not matter; neighbouring
 //      groups belong to different rows);
-//   6. k_l64_insert + k_l64_relabel: classes of (label, signature) in the
+//   5. k_l64_insert + k_l64_relabel: classes of (label, signature) in the
 //      stamped 16-byte relabel table of the integer path, new label = smallest
 //      member;
-//   7. the host reads the class count: unchanged = fixpoint.
+//   6. the host reads the class count: unchanged = fixpoint.
 // Exact check at the fixpoint (the groups of the last pass are those of the
 // final partition, whose canonical labels the pass left unchanged): the
 // nonzero groups are compacted and re-sorted by row (stable, row bits only),
@@ -65,13 +65,12 @@ unsigned grid_of(uint64_t n, unsigned t = kT)
 
 // Device counters of one call.
 struct L64Counters {
-    uint32_t groups;   // (row, block) groups of the pass
     uint32_t classes;  // classes made by the last insert
     uint32_t failed;   // nodes that failed the exact check
     uint32_t nonzero;  // groups with a nonzero rounded sum
     uint32_t error;    // kErr* bits
     uint32_t long_groups;  // groups of more than kShortGroup arcs, listed for k_l64_long_sums
-    uint32_t pad[2];
+    uint32_t pad[3];
 };
 
 constexpr uint32_t kL64BadWeight = 32u;  // a weight that is not finite or not below 2^960
@@ -119,23 +118,6 @@ __global__ void k_l64_keys(uint64_t m, uint32_t lb, const uint32_t* __restrict__
     }
 }
 
-// flag[i] = position i starts a (block, row) group
-__global__ void k_l64_heads(uint64_t m, const unsigned long long* __restrict__ keys, uint32_t* __restrict__ flag)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
-        flag[i] = (i == 0 || keys[i] != keys[i - 1]) ? 1u : 0u;
-}
-
-// gstart[g] = first position of group g (gid = exclusive scan of the flags);
-// gstart[groups] = m
-__global__ void k_l64_gstart(uint64_t m, const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ gid,
-                             const L64Counters* __restrict__ c, uint32_t* __restrict__ gstart)
-{
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
-        if (i == 0 || keys[i] != keys[i - 1]) gstart[gid[i]] = (uint32_t)i;
-    if (blockIdx.x == 0 && threadIdx.x == 0) gstart[c->groups] = (uint32_t)m;
-}
-
 __device__ __forceinline__ void group_hash(uint32_t lab, uint32_t bits, uint64_t salt1, uint32_t salt2, uint64_t& h1,
                                            uint32_t& h2)
 {
@@ -164,46 +146,41 @@ __device__ __forceinline__ void group_done(uint64_t g, double s, unsigned long l
     }
 }
 
-// One thread per group of at most kShortGroup arcs: the double sum of its
-// weights in arc order (the sort kept it), rounded to float; bits[g] = the
-// float's bits, 0 for a sum that rounds to zero (of either sign), whose group
-// adds nothing.  Longer groups are listed for k_l64_long_sums.
+// One thread per sorted position; the first position of each (block, row)
+// group adds the group's weights in arc order (the sort kept it) in double and
+// rounds the sum to float.  bits[i] = the float's bits at a group's first
+// position (0 for a sum that rounds to zero, of either sign: the group adds
+// nothing), 0 at every other position.  Groups of more than kShortGroup arcs
+// are listed (by first position) for k_l64_long_sums.
 constexpr uint32_t kShortGroup = 32;
 
-__global__ void k_l64_sums(L64Counters* __restrict__ c, uint32_t lb, const uint32_t* __restrict__ gstart,
-                           const unsigned long long* __restrict__ keys, const unsigned long long* __restrict__ vals,
-                           uint64_t salt1, uint32_t salt2, int hash_bits, Sig* __restrict__ sig, uint32_t* __restrict__ bits,
-                           uint32_t* __restrict__ long_list)
+__global__ void k_l64_sums(L64Counters* __restrict__ c, uint64_t m, uint32_t lb, const unsigned long long* __restrict__ keys,
+                           const unsigned long long* __restrict__ vals, uint64_t salt1, uint32_t salt2, int hash_bits,
+                           Sig* __restrict__ sig, uint32_t* __restrict__ bits, uint32_t* __restrict__ long_list)
 {
-    const uint32_t G = c->groups;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t b = gstart[g], e = gstart[g + 1];
-        if (e - b > kShortGroup) {
-            long_list[atomicAdd(&c->long_groups, 1u)] = (uint32_t)g;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x) {
+        const unsigned long long k = keys[i];
+        if (i > 0 && keys[i - 1] == k) {
+            bits[i] = 0u;
             continue;
         }
+        const uint64_t end = min(m, i + kShortGroup + 1);
         double s = 0.0;
-        uint32_t i = b;
-        // the loads of four weights side by side; the adds stay in order
-        for (; i + 4u <= e; i += 4u) {
-            const double w0 = __longlong_as_double((long long)vals[i]), w1 = __longlong_as_double((long long)vals[i + 1]);
-            const double w2 = __longlong_as_double((long long)vals[i + 2]), w3 = __longlong_as_double((long long)vals[i + 3]);
-            s += w0;
-            s += w1;
-            s += w2;
-            s += w3;
+        uint64_t j = i;
+        for (; j < end && keys[j] == k; ++j) s += __longlong_as_double((long long)vals[j]);
+        if (j - i > kShortGroup) {
+            long_list[atomicAdd(&c->long_groups, 1u)] = (uint32_t)i;
+            continue;
         }
-        for (; i < e; ++i) s += __longlong_as_double((long long)vals[i]);
-        group_done(g, s, keys[b], lb, salt1, salt2, hash_bits, sig, bits);
+        group_done(i, s, k, lb, salt1, salt2, hash_bits, sig, bits);
     }
 }
 
-// One warp per long group: the lanes load 32 weights at a time (the next 32
-// while lane 0 adds the current ones, handed over by shuffles in lane order),
-// so the sum is the same arc-order double sum as k_l64_sums', at the pace of
-// the dependent adds rather than of one load per few weights.
-__global__ void __launch_bounds__(kT) k_l64_long_sums(const L64Counters* __restrict__ c, uint32_t lb,
-                                                      const uint32_t* __restrict__ gstart,
+// One warp per long group: the lanes load 32 keys and weights at a time (the
+// next 32 while lane 0 adds the current ones, handed over by shuffles in lane
+// order), so the sum is the same arc-order double sum as k_l64_sums', at the
+// pace of the dependent adds rather than of one load per weight.
+__global__ void __launch_bounds__(kT) k_l64_long_sums(const L64Counters* __restrict__ c, uint64_t m, uint32_t lb,
                                                       const unsigned long long* __restrict__ keys,
                                                       const unsigned long long* __restrict__ vals, uint64_t salt1,
                                                       uint32_t salt2, int hash_bits, Sig* __restrict__ sig,
@@ -212,22 +189,27 @@ __global__ void __launch_bounds__(kT) k_l64_long_sums(const L64Counters* __restr
     const uint32_t L = c->long_groups;
     const uint32_t lane = threadIdx.x & 31;
     const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x >> 5);
-    for (uint64_t i = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); i < L; i += warps) {
-        const uint32_t g = long_list[i];
-        const uint32_t b = gstart[g], e = gstart[g + 1];
+    for (uint64_t t = blockIdx.x * (uint64_t)(blockDim.x >> 5) + (threadIdx.x >> 5); t < L; t += warps) {
+        const uint64_t b = long_list[t];
+        const unsigned long long k = keys[b];
         double s = 0.0;
-        double x = b + lane < e ? __longlong_as_double((long long)vals[b + lane]) : 0.0;
-        for (uint32_t a0 = b; a0 < e; a0 += 32) {
-            const uint32_t a1 = a0 + 32;
-            const double nx = a1 + lane < e ? __longlong_as_double((long long)vals[a1 + lane]) : 0.0;
-            const uint32_t cnt = min(32u, e - a0);
+        bool in = b + lane < m && keys[b + lane] == k;
+        double x = in ? __longlong_as_double((long long)vals[b + lane]) : 0.0;
+        for (uint64_t a0 = b;; a0 += 32) {
+            // the group is contiguous: its lanes of this chunk are a prefix
+            const uint32_t cnt = (uint32_t)__popc(__ballot_sync(0xffffffffu, in));
+            const uint64_t a1 = a0 + 32;
+            const bool nin = cnt == 32u && a1 + lane < m && keys[a1 + lane] == k;
+            const double nx = nin ? __longlong_as_double((long long)vals[a1 + lane]) : 0.0;
             for (uint32_t j = 0; j < cnt; ++j) {
                 const double v = __shfl_sync(0xffffffffu, x, j);
                 if (lane == 0) s += v;
             }
+            if (cnt < 32u) break;
+            in = nin;
             x = nx;
         }
-        if (lane == 0) group_done(g, s, keys[b], lb, salt1, salt2, hash_bits, sig, bits);
+        if (lane == 0) group_done(b, s, k, lb, salt1, salt2, hash_bits, sig, bits);
     }
 }
 
@@ -269,31 +251,27 @@ __global__ void k_l64_relabel(uint32_t n, const Entry* __restrict__ tab, const u
     }
 }
 
-// nzflag[g] = group g has a nonzero rounded sum
-__global__ void k_l64_nz_flags(const L64Counters* __restrict__ c, const uint32_t* __restrict__ bits,
-                               uint32_t* __restrict__ nzflag)
+// nzflag[i] = position i starts a group with a nonzero rounded sum
+__global__ void k_l64_nz_flags(uint64_t m, const uint32_t* __restrict__ bits, uint32_t* __restrict__ nzflag)
 {
-    const uint32_t G = c->groups;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x)
-        nzflag[g] = bits[g] != 0u ? 1u : 0u;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        nzflag[i] = bits[i] != 0u ? 1u : 0u;
 }
 
 // the nonzero groups, compacted: ckey = (row << cw) | block id, cval = float
 // bits; cnt[row] counts them (zeroed before)
-__global__ void k_l64_nz_compact(const L64Counters* __restrict__ c, uint32_t lb, uint32_t cw, const uint32_t* __restrict__ gstart,
-                                 const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ bits,
-                                 const uint32_t* __restrict__ nzpos, unsigned long long* __restrict__ ckey,
-                                 uint32_t* __restrict__ cval, uint32_t* __restrict__ cnt)
+__global__ void k_l64_nz_compact(uint64_t m, uint32_t lb, uint32_t cw, const unsigned long long* __restrict__ keys,
+                                 const uint32_t* __restrict__ bits, const uint32_t* __restrict__ nzpos,
+                                 unsigned long long* __restrict__ ckey, uint32_t* __restrict__ cval, uint32_t* __restrict__ cnt)
 {
-    const uint32_t G = c->groups;
     const uint64_t mask = (1ull << lb) - 1ull;
-    for (uint64_t g = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; g < G; g += (uint64_t)gridDim.x * blockDim.x)
-        if (bits[g]) {
-            const unsigned long long k = keys[gstart[g]];
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < m; i += (uint64_t)gridDim.x * blockDim.x)
+        if (bits[i]) {
+            const unsigned long long k = keys[i];
             const uint32_t row = (uint32_t)(k & mask);
-            const uint32_t p = nzpos[g];
+            const uint32_t p = nzpos[i];
             ckey[p] = ((unsigned long long)row << cw) | (k >> lb);
-            cval[p] = bits[g];
+            cval[p] = bits[i];
             atomicAdd(&cnt[row], 1u);
         }
 }
@@ -358,7 +336,7 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     uint32_t log2tab = 10;
     while (log2tab < 33 && (1ull << log2tab) < 2ull * N) ++log2tab;
     uint32_t *col = nullptr, *slot = nullptr, *fail = nullptr, *first = nullptr, *bid = nullptr, *src = nullptr,
-             *gid = nullptr, *gstart = nullptr, *bits = nullptr, *cval = nullptr, *cval_alt = nullptr;
+             *gid = nullptr, *bits = nullptr, *cval = nullptr, *cval_alt = nullptr;
     unsigned long long *keys = nullptr, *keys_alt = nullptr, *vals = nullptr, *vals_alt = nullptr;
     Sig* sig = nullptr;
     Entry* tab = nullptr;
@@ -378,7 +356,6 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
     EKS(sc.get(&vals, M));
     EKS(sc.get(&vals_alt, M));
     EKS(sc.get(&gid, M + 1));
-    EKS(sc.get(&gstart, M + 1));
     EKS(sc.get(&bits, M));
     EKS(sc.get(&cval, M));
     EKS(sc.get(&cval_alt, M));
@@ -457,20 +434,14 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
         const unsigned long long* sk = in_alt ? keys_alt : keys;
         const unsigned long long* sv = in_alt ? vals_alt : vals;
         EK(cudaMemsetAsync(sig, 0, sizeof(Sig) * N, s));
-        EK(cudaMemsetAsync(&dc->groups, 0, 4, s));
         EK(cudaMemsetAsync(&dc->long_groups, 0, 4, s));
         if (M) {
             const uint64_t salt1 = pass_salt1(ctx->opts.seed, rounds);
             const uint32_t salt2 = pass_salt2(ctx->opts.seed, rounds);
             ++rbsc::launch_counter();
-            k_l64_heads<<<grid_of(M), kT, 0, s>>>(M, sk, gid);
-            EK((exclusive_scan<uint32_t, uint32_t>(gid, gid, M, &dc->groups, tmp, s)));
+            k_l64_sums<<<grid_of(M), kT, 0, s>>>(dc, M, lb, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
             ++rbsc::launch_counter();
-            k_l64_gstart<<<grid_of(M), kT, 0, s>>>(M, sk, gid, dc, gstart);
-            ++rbsc::launch_counter();
-            k_l64_sums<<<grid_of(M), kT, 0, s>>>(dc, lb, gstart, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
-            ++rbsc::launch_counter();
-            k_l64_long_sums<<<long_grid, kT, 0, s>>>(dc, lb, gstart, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
+            k_l64_long_sums<<<long_grid, kT, 0, s>>>(dc, M, lb, sk, sv, salt1, salt2, hash_bits, sig, bits, cval_alt);
             EK(cudaGetLastError());
         }
         EKS(relabel(0, nullptr));
@@ -496,10 +467,10 @@ extern "C" rbsc_status rbsc_refine_f64(rbsc_ctx* ctx, const rbsc_csr* host_graph
         const uint32_t* cv = cval;
         if (M) {
             ++rbsc::launch_counter();
-            k_l64_nz_flags<<<grid_of(M), kT, 0, s>>>(dc, bits, gid);
+            k_l64_nz_flags<<<grid_of(M), kT, 0, s>>>(M, bits, gid);
             EK((exclusive_scan<uint32_t, uint32_t>(gid, gid, M, (uint32_t*)nullptr, tmp, s)));
             ++rbsc::launch_counter();
-            k_l64_nz_compact<<<grid_of(M), kT, 0, s>>>(dc, lb, cw, gstart, sk, bits, gid, ck, cval, first);
+            k_l64_nz_compact<<<grid_of(M), kT, 0, s>>>(M, lb, cw, sk, bits, gid, ck, cval, first);
             EK(cudaGetLastError());
             // nonzero groups = the per-row counts' total (read back for the sort's size)
             EK((exclusive_scan<uint32_t, uint32_t>(first, first, (uint64_t)N + 1, &dc->nonzero, tmp, s)));
