@@ -466,8 +466,11 @@ def run_ours(args, rank, world, local_rank):
 
     batched = None if args.batch_graphs <= 0 else run_batched(args, ctx, world, dist)
     # the served, LAW and streamed sections describe one GPU (the streamed one
-    # alone pins 36 GB of host memory): they run at N = 1 only
+    # alone pins 36 GB of host memory): they run at N = 1 only.  The main
+    # context's cached buffers go back to CUDA first: the server sizes its
+    # budget and its slots' buffer caches from the free device memory
     single = world == 1
+    ctx.trim()
     served = None if args.serve_requests <= 0 or not single else run_served(args, world, dist, local_rank)
     law = None if args.law_steps <= 0 or not single else run_law(args, ctx)
     streamed = None if args.stream_scale <= 0 or not single else run_streamed(args, ctx, local_rank)

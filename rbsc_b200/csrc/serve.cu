@@ -444,8 +444,10 @@ extern "C" rbsc_status rbsc_serve_create(const rbsc_serve_opts* opts, rbsc_serve
                 delete srv;
                 return s;
             }
-            // unused cached blocks of a slot count against nobody's budget: keep them few
-            sl->ctx->dpool.cap = std::max<size_t>((size_t)64 << 20, o.hbm_budget / (4 * (uint64_t)o.slots));
+            // unused cached blocks of a slot count against nobody's budget, but
+            // giving them back costs a cudaFree, which waits for every slot's
+            // work on the device: a slot keeps up to its share of the budget
+            sl->ctx->dpool.cap = std::max<size_t>((size_t)64 << 20, o.hbm_budget / (uint64_t)o.slots);
         }
     }
     for (Slot* sl : srv->slots) sl->th = std::thread(slot_main, srv, sl);
