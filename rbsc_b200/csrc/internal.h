@@ -31,7 +31,9 @@ struct rbsc_ctx {
     MemPool hpool{true};
     rbsc_opts opts{};
     cudaStream_t stream = nullptr;
-    cudaEvent_t ev[6] = {};
+    // [0]..[5] timing marks of a refinement; [6] the end of its initial pass
+    // and setup kernels; [7] the copy of the state after the initial pass
+    cudaEvent_t ev[8] = {};
     cudaEvent_t ev_sig[2] = {};  // around the host-launched first signature kernel
     // a pass clears the list table's window on this stream beside its
     // signature kernel (fork / join events, no timing)
@@ -156,6 +158,14 @@ struct rbsc_graph {
     // reads them; until then d_idx is only partly filled
     bool stream_upload = false;
     const uint32_t* h_upload = nullptr;
+    // the one-shot call's host colours, already copied into d_init by the load
+    const uint32_t* h_init_loaded = nullptr;
+    // a page-locked source: every chunk's copy is issued when the graph is
+    // loaded, so the host link stays busy through the set-up kernels and the
+    // initial pass; chunk c's copy completes ev_chunk[c]
+    bool upload_issued = false;
+    static constexpr int kUploadChunks = 8;
+    cudaEvent_t ev_chunk[kUploadChunks] = {};
 };
 
 rbsc_status rbsc_fail(rbsc_ctx* ctx, rbsc_status code, const char* fmt, ...);

@@ -345,6 +345,8 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
         if (g->ev_copied[i]) cudaEventDestroy(g->ev_copied[i]);
         if (g->ev_used[i]) cudaEventDestroy(g->ev_used[i]);
     }
+    for (auto& ev : g->ev_chunk)
+        if (ev) cudaEventDestroy(ev);
     if (g->copy_stream) cudaStreamDestroy(g->copy_stream);
     if (g->host_arcs) {
         if (g->reg_idx) cudaHostUnregister(g->reg_idx);
@@ -519,7 +521,7 @@ rbsc_status graph_alloc_csr(rbsc_ctx* ctx, rbsc_graph* g, bool weighted)
 // the first pass that reads them (stream_signature's upload mode), which
 // overlaps their copy with the initial colours, the setup and that pass.
 static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device, rbsc_graph** out, double* h2d_ms,
-                              uint64_t* h2d_bytes, bool defer_heads = false)
+                              uint64_t* h2d_bytes, bool defer_heads = false, const uint32_t* h_init = nullptr)
 {
     *out = nullptr;
     CKS(check_csr_args(ctx, c));
@@ -560,12 +562,43 @@ static rbsc_status graph_load(rbsc_ctx* ctx, const rbsc_csr* c, bool from_device
         dev_free(ctx, tmp);
     }
     defer_heads = defer_heads && !from_device && !c->weights && c->m > 0;
+    // the one-shot call's initial colours: copied right behind the offsets,
+    // ahead of the heads, whose early copies (below) would otherwise hold
+    // them back on the host link
+    if (e == cudaSuccess && defer_heads && h_init && c->n) {
+        st = dev_alloc(ctx, (void**)&g->d_init, 4 * (size_t)c->n);
+        if (st != RBSC_OK) {
+            rbsc_graph_free(g);
+            return st;
+        }
+        e = cudaMemcpyAsync(g->d_init, h_init, 4 * (size_t)c->n, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) g->h_init_loaded = h_init;
+    }
     if (defer_heads) {
         g->stream_upload = true;
         g->h_upload = c->indices;
         g->chunk_tiles = (uint32_t)std::max<uint64_t>(1, ceil_div<uint64_t>(ceil_div<uint64_t>(c->m, kTileEdges), 8));
         if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g->copy_stream, cudaStreamNonBlocking);
         for (int i = 0; i < 2 && e == cudaSuccess; ++i) e = cudaEventCreateWithFlags(&g->ev_copied[i], cudaEventDisableTiming);
+        // a page-locked source: issue every chunk's copy now, behind the
+        // offsets (a pageable one is copied chunk by chunk in the first pass:
+        // its copies would hold the host here)
+        cudaPointerAttributes pa{};
+        const cudaError_t qe = e == cudaSuccess ? cudaPointerGetAttributes(&pa, c->indices) : cudaSuccess;
+        if (qe != cudaSuccess) cudaGetLastError();  // not a pointer CUDA knows: no early copies
+        const uint64_t nt = ceil_div<uint64_t>(c->m, kTileEdges);
+        if (e == cudaSuccess && qe == cudaSuccess && pa.type == cudaMemoryTypeHost &&
+            ceil_div<uint64_t>(nt, g->chunk_tiles) <= (uint64_t)rbsc_graph::kUploadChunks) {
+            int k = 0;
+            for (uint64_t t = 0; t < nt && e == cudaSuccess; t += g->chunk_tiles, ++k) {
+                const uint64_t a0 = t * kTileEdges, a1 = std::min<uint64_t>(c->m, (t + g->chunk_tiles) * kTileEdges);
+                e = cudaEventCreateWithFlags(&g->ev_chunk[k], cudaEventDisableTiming);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(g->d_idx + a0, c->indices + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream);
+                if (e == cudaSuccess) e = cudaEventRecord(g->ev_chunk[k], g->copy_stream);
+            }
+            g->upload_issued = e == cudaSuccess;
+        }
     } else if (e == cudaSuccess && c->m) {
         e = cudaMemcpyAsync(g->d_idx, c->indices, sizeof(uint32_t) * c->m, kind, s);
     }
@@ -928,16 +961,21 @@ static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s
         const uint32_t t1 = (uint32_t)std::min<uint64_t>(ntiles, (uint64_t)t0 + g->chunk_tiles);
         const uint64_t a0 = (uint64_t)t0 * kTileEdges, a1 = std::min<uint64_t>(m, (uint64_t)t1 * kTileEdges);
         const int slot = (int)(c & 1u);
-        if (upload) {
-            CK(cudaMemcpyAsync(g->d_idx + a0, g->h_upload + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+        if (upload && g->upload_issued) {
+            // copied since the load (the same chunks, in order)
+            CK(cudaStreamWaitEvent(s, g->ev_chunk[c], 0));
         } else {
-            CK(cudaStreamWaitEvent(g->copy_stream, g->ev_used[slot], 0));
-            CK(cudaMemcpyAsync(g->d_chunk[slot], g->d_idx + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
-            if (g->weighted)
-                CK(cudaMemcpyAsync(g->d_chunk_wt[slot], g->d_wt + a0, 8 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+            if (upload) {
+                CK(cudaMemcpyAsync(g->d_idx + a0, g->h_upload + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+            } else {
+                CK(cudaStreamWaitEvent(g->copy_stream, g->ev_used[slot], 0));
+                CK(cudaMemcpyAsync(g->d_chunk[slot], g->d_idx + a0, 4 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+                if (g->weighted)
+                    CK(cudaMemcpyAsync(g->d_chunk_wt[slot], g->d_wt + a0, 8 * (a1 - a0), cudaMemcpyHostToDevice, g->copy_stream));
+            }
+            CK(cudaEventRecord(g->ev_copied[slot], g->copy_stream));
+            CK(cudaStreamWaitEvent(s, g->ev_copied[slot], 0));
         }
-        CK(cudaEventRecord(g->ev_copied[slot], g->copy_stream));
-        CK(cudaStreamWaitEvent(s, g->ev_copied[slot], 0));
         if (upload) {
             ++rbsc::launch_counter();
             k_validate_heads<<<persistent_grid(ctx, ceil_div<uint64_t>(a1 - a0, 256), 1), 256, 0, s>>>(a0, a1, g->n, g->d_idx,
@@ -970,7 +1008,15 @@ static rbsc_status stream_signature(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s
 static rbsc_status finish_upload(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
 {
     if (g->m) {
-        CK(cudaMemcpyAsync(g->d_idx, g->h_upload, 4 * g->m, cudaMemcpyHostToDevice, s));
+        if (g->upload_issued) {
+            // the chunks were copied in order on copy_stream: the last one's
+            // event covers them all
+            int last = rbsc_graph::kUploadChunks - 1;
+            while (last > 0 && !g->ev_chunk[last]) --last;
+            CK(cudaStreamWaitEvent(s, g->ev_chunk[last], 0));
+        } else {
+            CK(cudaMemcpyAsync(g->d_idx, g->h_upload, 4 * g->m, cudaMemcpyHostToDevice, s));
+        }
         ++rbsc::launch_counter();
         k_validate_heads<<<persistent_grid(ctx, ceil_div<uint64_t>(g->m, 256), 1), 256, 0, s>>>(0, g->m, g->n, g->d_idx, g->d_st);
         CK(cudaGetLastError());
@@ -1580,14 +1626,20 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         k_strip_labels<<<grid_for(n, 256), 256, 0, s>>>(n, g->d_col[0], g->d_initlab);
         CK(cudaGetLastError());
     }
-    CKS(read_state(ctx, g));
-    const uint32_t initial_blocks = hs.prev;
+    // The state after the initial pass (its block count picks the first
+    // pass's gather width) comes back while the setup kernels run: the host
+    // waits for that copy (ev[7]), not for the setup.  The profile path keeps
+    // a synchronisation between the phases to time each.
     if (kt) {
+        CKS(read_state(ctx, g));
         CK(cudaEventRecord(ctx->ev[4], s));
         CK(cudaEventSynchronize(ctx->ev[4]));
         float ms = 0.f;
         cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[4]);
         kt->init_ms = ms;
+    } else {
+        CK(cudaMemcpyAsync(g->h_st, g->d_st, sizeof(RoundState), cudaMemcpyDeviceToHost, s));
+        CK(cudaEventRecord(ctx->ev[7], s));
     }
     CKS(init_active_set(ctx, g));
     if (kt) {
@@ -1597,10 +1649,9 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         cudaEventElapsedTime(&ms, ctx->ev[4], ctx->ev[5]);
         kt->setup_ms = ms;
     }
-    CK(cudaEventRecord(ctx->ev[4], s));
-    CK(cudaEventSynchronize(ctx->ev[4]));
-    float init_ms = 0.f;
-    cudaEventElapsedTime(&init_ms, ctx->ev[0], ctx->ev[4]);
+    CK(cudaEventRecord(ctx->ev[6], s));  // end of init + setup, read after the refinement
+    if (!kt) CK(cudaEventSynchronize(ctx->ev[7]));
+    const uint32_t initial_blocks = hs.prev;
 
     // first pass: few initial classes -> gather their dense ranks (1 or 2
     // bytes per node); one class -> no gather at all
@@ -1687,8 +1738,9 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     }
     CK(cudaEventRecord(ctx->ev[1], s));
     CK(cudaEventSynchronize(ctx->ev[1]));
-    float total_ms = 0.f;
+    float total_ms = 0.f, init_ms = 0.f;
     cudaEventElapsedTime(&total_ms, ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&init_ms, ctx->ev[0], ctx->ev[6]);
     if (stats) {
         stats->rounds = hs.round;
         stats->blocks = hs.prev;
@@ -1740,7 +1792,10 @@ extern "C" rbsc_status rbsc_graph_refine(rbsc_ctx* ctx, rbsc_graph* g, const uin
     CKS(ensure_refine_bufs(ctx, g));
     double h2d = 0, d2h = 0;
     const uint32_t* d_init = nullptr;
-    if (init_colors && g->n) {
+    if (init_colors && g->n && init_colors == g->h_init_loaded) {
+        d_init = g->d_init;  // copied with the graph (one-shot call)
+        g->h_init_loaded = nullptr;
+    } else if (init_colors && g->n) {
         if (!g->d_init) CKS(dev_alloc(ctx, (void**)&g->d_init, 4 * (size_t)g->n));
         auto a = std::chrono::steady_clock::now();
         CK(cudaMemcpyAsync(g->d_init, init_colors, 4 * (size_t)g->n, cudaMemcpyHostToDevice, ctx->stream));
@@ -1775,7 +1830,7 @@ extern "C" rbsc_status rbsc_refine(rbsc_ctx* ctx, const rbsc_csr* host_graph, co
     uint64_t up_bytes = 0;
     // large unweighted graphs: the heads' copy overlaps the refinement
     const bool defer = host_graph && !host_graph->weights && host_graph->m >= (1ull << 22);
-    CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes, defer));
+    CKS(graph_load(ctx, host_graph, false, &g, &up_ms, &up_bytes, defer, init_colors));
     g->oneshot = true;
     rbsc_status st = rbsc_graph_refine(ctx, g, init_colors, out_labels, stats);
     rbsc_graph_free(g);

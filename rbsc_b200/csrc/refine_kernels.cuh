@@ -1920,9 +1920,11 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
     for (uint32_t base = (blockIdx.x * wpb + (threadIdx.x >> 5)) * 32u; base < K; base += nwarps * 32u) {
         const uint32_t k = base + lane;
         uint64_t b = 0, e = 0;
+        uint32_t node = 0;
         if (k < K) {
             b = r64 ? roff64[k] : (uint64_t)roff32[k];
             e = r64 ? roff64[k + 1] : (uint64_t)roff32[k + 1];
+            node = rows[k];  // issued beside the offsets: the store at the end waits for no load
         }
         const bool longrow = e - b > kRowLong;
         if (k < K && !longrow) {
@@ -1951,7 +1953,7 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
                     s2 += t2;
                 }
             }
-            sig_store(&sig[rows[k]], s1, s2);
+            sig_store(&sig[node], s1, s2);
         }
         unsigned lm = __ballot_sync(0xffffffffu, k < K && longrow);
         while (lm) {
@@ -1977,7 +1979,7 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
                 s1 += __shfl_xor_sync(0xffffffffu, s1, d);
                 s2 += __shfl_xor_sync(0xffffffffu, s2, d);
             }
-            if (lane == (uint32_t)src) sig_store(&sig[rows[k]], s1, s2);
+            if (lane == (uint32_t)src) sig_store(&sig[node], s1, s2);
         }
     }
 }

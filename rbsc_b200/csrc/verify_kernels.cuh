@@ -40,7 +40,7 @@ struct VerifyLists {
 // nodes, and no block-wide barrier is needed.  It also writes every node's
 // canonical label to `out` (the refinement's result when the check passes,
 // so no separate pass over the colours is needed then).
-static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, const uint32_t* __restrict__ col,
+static __global__ void __launch_bounds__(256, 2) k_verify_classify(uint32_t n, const uint32_t* __restrict__ col,
                                                                 const uint32_t* __restrict__ initlab,
                                                                 const uint64_t* __restrict__ off, int weighted, VerifyLists vl,
                                                                 uint32_t* __restrict__ vflag, uint32_t* __restrict__ fail,
@@ -53,16 +53,45 @@ static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, cons
     uint32_t* bl = s_buf[warp][2];
     uint32_t c8 = 0, c32 = 0, cl = 0, nbad = 0;
     const uint32_t nwarps = gridDim.x * (256u / 32u);
-    for (uint32_t base = (blockIdx.x * (256u / 32u) + warp) * 32u; base < n; base += nwarps * 32u) {
-        const uint32_t u = base + lane;
-        bool t8 = false, t32 = false, tl = false, bad = false;
-        if (u < n) {
-            const uint32_t c = col[u];
-            const uint32_t r = c & kLabelMask;
-            out[u] = r;  // the canonical labels, final when the check passes
-            if (!(c & kSingleton) && r != u) {
-                const uint64_t du = off[u + 1] - off[u], dr = off[r + 1] - off[r];
-                if (initlab[u] != initlab[r]) bad = true;
+    // U x 32 consecutive nodes per warp and step: the colour loads of U nodes
+    // per lane, then their offset and label loads, are issued side by side,
+    // so U dependent chains overlap
+    constexpr int U = 4;
+    for (uint32_t base = (blockIdx.x * (256u / 32u) + warp) * 32u * U; base < n; base += nwarps * 32u * U) {
+        uint32_t c[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + 32u * j + lane;
+            c[j] = u < n ? col[u] : kSingleton;
+        }
+        bool check[U];
+        uint64_t ou0[U], ou1[U], or0[U], or1[U];
+        uint32_t lu[U], lr[U];
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + 32u * j + lane;
+            const uint32_t r = c[j] & kLabelMask;
+            if (u < n) out[u] = r;  // the canonical labels, final when the check passes
+            check[j] = u < n && !(c[j] & kSingleton) && r != u;
+            ou0[j] = ou1[j] = or0[j] = or1[j] = 0ull;
+            lu[j] = lr[j] = 0u;
+            if (check[j]) {
+                ou0[j] = off[u];
+                ou1[j] = off[u + 1];
+                or0[j] = off[r];
+                or1[j] = off[r + 1];
+                lu[j] = initlab[u];
+                lr[j] = initlab[r];
+            }
+        }
+#pragma unroll
+        for (int j = 0; j < U; ++j) {
+            const uint32_t u = base + 32u * j + lane;
+            const uint32_t r = c[j] & kLabelMask;
+            bool t8 = false, t32 = false, tl = false, bad = false;
+            if (check[j]) {
+                const uint64_t du = ou1[j] - ou0[j], dr = or1[j] - or0[j];
+                if (lu[j] != lr[j]) bad = true;
                 else if (weighted) tl = du > 0 || dr > 0;
                 else if (du != dr) bad = true;
                 else if (du == 0) {}
@@ -75,11 +104,11 @@ static __global__ void __launch_bounds__(256) k_verify_classify(uint32_t n, cons
                 }
                 if (bad) fail[u] = 1u;
             }
+            warp_append(t8, u, b8, c8, &vl.counts[0], vl.l8);
+            warp_append(t32, u, b32, c32, &vl.counts[1], vl.l32);
+            warp_append(tl, u, bl, cl, &vl.counts[2], vl.llong);
+            nbad += bad ? 1u : 0u;
         }
-        warp_append(t8, u, b8, c8, &vl.counts[0], vl.l8);
-        warp_append(t32, u, b32, c32, &vl.counts[1], vl.l32);
-        warp_append(tl, u, bl, cl, &vl.counts[2], vl.llong);
-        nbad += bad ? 1u : 0u;
     }
     warp_append_flush(b8, c8, &vl.counts[0], vl.l8);
     warp_append_flush(b32, c32, &vl.counts[1], vl.l32);

@@ -154,6 +154,38 @@ def test_one_shot_upload_overlapped_with_the_first_pass(ctx):
         assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
 
 
+def test_one_shot_upload_from_page_locked_heads(ctx):
+    """A page-locked source: every chunk's copy is issued when the graph is
+    loaded (before the set-up kernels).  Same result as the resident graph and
+    as the oracle, with degree classes, with one initial class (a uniform first
+    pass: the upload is awaited whole) and twice in a row (reused buffers)."""
+    off, idx = R.gen_rmat_host(18, 20, seed=6)
+    assert len(idx) >= (1 << 22)
+    poff, toff = _pinned_copy(off)
+    pidx, tidx = _pinned_copy(idx)
+    for init in (R.degree_bucket_colors(off), None, R.degree_bucket_colors(off)):
+        ref = ctx.upload(off, idx).refine(init)
+        r = ctx.refine(poff, pidx, init=init)
+        assert r.blocks == ref.blocks and r.rounds == ref.rounds and np.array_equal(r.labels, ref.labels)
+    ex = oracle.refine_exact(off, idx, init=R.degree_bucket_colors(off))
+    assert r.blocks == ex.blocks and r.rounds == ex.rounds and np.array_equal(r.labels, ex.labels)
+    del toff, tidx
+
+
+def test_one_shot_upload_from_page_locked_heads_rejects_a_bad_head(ctx):
+    off, idx = R.gen_rmat_host(18, 20, seed=7)
+    pidx, tidx = _pinned_copy(idx)
+    pidx[len(pidx) * 3 // 4] = len(off) - 1 + 5  # a head >= N in the seventh chunk
+    for init in (R.degree_bucket_colors(off), None):
+        with pytest.raises(R.RbscError) as e:
+            ctx.refine(off, pidx, init=init)
+        assert e.value.status == -1
+    pidx[len(pidx) * 3 // 4] = idx[len(idx) * 3 // 4]
+    r = ctx.refine(off, pidx)  # the context is still usable
+    assert r.done == 1
+    del tidx
+
+
 def test_one_shot_upload_rejects_a_bad_head(ctx):
     off, idx = R.gen_rmat_host(18, 20, seed=7)
     bad = idx.copy()
