@@ -336,6 +336,9 @@ extern "C" void rbsc_graph_free(rbsc_graph* g)
     if (!g) return;
     cudaSetDevice(g->ctx->device);
     cudaStreamSynchronize(g->ctx->stream);
+    // a refinement that stopped early may leave side-stream clears of its
+    // buffers unjoined
+    cudaStreamSynchronize(g->ctx->side);
     graph_release_refine(g);
     dev_free(g->ctx, (void*&)g->d_off);
     if (g->copy_stream) cudaStreamSynchronize(g->copy_stream);
@@ -1385,10 +1388,26 @@ static rbsc_status run_passes(rbsc_ctx* ctx, rbsc_graph* g, rbsc_kernel_times* k
     return RBSC_OK;
 }
 
+// Clears what the set-up of the active set expects to be clear: the words of
+// the arc-less groups (k_group_reps) and the signatures of the rows that
+// cross a tile edge (the first pass adds into them).
+static rbsc_status clear_setup_words(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s)
+{
+    if (g->nsplit) {
+        ++rbsc::launch_counter();
+        k_zero_rows<<<grid_for(g->nsplit, 256), 256, 0, s>>>(g->d_split, g->nsplit, g->d_sig);
+        CK(cudaGetLastError());
+    }
+    CK(cudaMemsetAsync(g->d_grep, 0xff, 4 * (size_t)g->n, s));
+    CK(cudaMemsetAsync(g->d_gcnt, 0, 4 * (size_t)g->n, s));
+    return RBSC_OK;
+}
+
 // Resets the active set to the whole graph and builds the node list and the
 // follower pairs from the current colouring (after the initial or a repair
-// pass).
-static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
+// pass).  side_cleared: clear_setup_words ran on the side stream, which
+// recorded ev_join after it.
+static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g, bool side_cleared = false)
 {
     cudaStream_t s = ctx->stream;
     const uint32_t n = g->n;
@@ -1413,12 +1432,8 @@ static rbsc_status init_active_set(rbsc_ctx* ctx, rbsc_graph* g)
     g->arcs_on_host = g->host_arcs;
     *g->h_as = a;
     CK(cudaMemcpyAsync(g->d_as, g->h_as, sizeof a, cudaMemcpyHostToDevice, s));
-    if (g->nsplit) {
-        ++rbsc::launch_counter();
-        k_zero_rows<<<grid_for(g->nsplit, 256), 256, 0, s>>>(g->d_split, g->nsplit, g->d_sig);
-    }
-    CK(cudaMemsetAsync(g->d_grep, 0xff, 4 * (size_t)n, s));
-    CK(cudaMemsetAsync(g->d_gcnt, 0, 4 * (size_t)n, s));
+    if (side_cleared) CK(cudaStreamWaitEvent(s, ctx->ev_join, 0));
+    else CKS(clear_setup_words(ctx, g, s));
     const unsigned lgrid = (unsigned)std::min<uint64_t>((uint64_t)ctx->sm_count * 8, ceil_div<uint64_t>(n, 256));
     ++rbsc::launch_counter();
     k_group_reps<<<lgrid, 256, 0, s>>>(n, g->d_off, g->d_initlab, g->d_grep, g->d_gcnt);
@@ -1594,7 +1609,14 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
     g->first_sig_arcs = 0;
     g->streamed_bytes = 0;
     g->streamed_passes = 0;
-    CK(cudaMemsetAsync(g->d_joined, 0, 4 * (size_t)n, s));
+    // the joined flags, the arc-less groups' words and the split rows'
+    // signatures are cleared on the side stream beside the initial pass
+    // (k_insert_init is bound by issue, not by HBM); the set-up waits for them
+    CK(cudaEventRecord(ctx->ev_fork, s));
+    CK(cudaStreamWaitEvent(ctx->side, ctx->ev_fork, 0));
+    CK(cudaMemsetAsync(g->d_joined, 0, 4 * (size_t)n, ctx->side));
+    CKS(clear_setup_words(ctx, g, ctx->side));
+    CK(cudaEventRecord(ctx->ev_join, ctx->side));
     RoundState& hs = *g->h_st;
     std::memset(&hs, 0, sizeof hs);
     hs.max_rounds = ctx->opts.max_rounds ? ctx->opts.max_rounds : (n + 1u);
@@ -1641,7 +1663,7 @@ rbsc_status refine_resident(rbsc_ctx* ctx, rbsc_graph* g, const uint32_t* d_init
         CK(cudaMemcpyAsync(g->h_st, g->d_st, sizeof(RoundState), cudaMemcpyDeviceToHost, s));
         CK(cudaEventRecord(ctx->ev[7], s));
     }
-    CKS(init_active_set(ctx, g));
+    CKS(init_active_set(ctx, g, true));
     if (kt) {
         CK(cudaEventRecord(ctx->ev[5], s));
         CK(cudaEventSynchronize(ctx->ev[5]));
