@@ -472,7 +472,7 @@ def run_ours(args, rank, world, local_rank):
     single = world == 1
     ctx.trim()
     served = None if args.serve_requests <= 0 or not single else run_served(args, world, dist, local_rank)
-    law = None if args.law_steps <= 0 or not single else run_law(args, ctx)
+    law = None if args.law_steps <= 0 or not single else run_law(args, local_rank)
     streamed = None if args.stream_scale <= 0 or not single else run_streamed(args, ctx, local_rank)
     lump_f64 = None if args.f64_scale <= 0 or not single else run_lump_f64(args, ctx)
 
@@ -738,19 +738,30 @@ def run_served(args, world, dist, local_rank):
     return out
 
 
-def run_law(args, ctx):
+def run_law(args, local_rank):
     """The reference's own LAW sample, cnr-2000 (325,557 nodes, 3,216,152 arcs,
     173 rounds), decoded from its BV files by rbsc_bv_load at build time
     (oracle/_ref/cnr-2000.npz; absent -> section skipped).  Uniform initial
     colours, as the reference programs run it.  Resident refinement (device
     time) and the one-shot call from page-locked host arrays; the partition is
     checked against the reference programs' (tests/golden/law_cnr2000.json),
-    whose recorded reference-GPU-program time on a B200 is quoted beside."""
-    import hashlib
+    whose recorded reference-GPU-program time on a B200 is quoted beside.
+    A context of its own with the library's default knobs: the main context
+    carries the knobs that the autotuner chose for the batch of small graphs
+    (with its hand-off limit of 2^18 arcs, cnr-2000's passes stayed in the
+    pass loop longer instead of the persistent kernel: 15.5 ms instead of 7.2
+    in one run)."""
+    import rbsc_b200 as R
     from oracle import oracle  # the decoded graph only; nothing under oracle/ runs here
     g0 = oracle.load_law()
     if g0 is None:
         return None
+    with R.Context(local_rank) as ctx:
+        return _run_law(args, ctx, g0)
+
+
+def _run_law(args, ctx, g0):
+    import hashlib
     fx = json.load(open(os.path.join(ROOT, "tests", "golden", "law_cnr2000.json")))
     off, idx = _pinned_copy(g0[0]), _pinned_copy(g0[1])
     m = len(idx)

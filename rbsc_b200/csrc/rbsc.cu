@@ -1097,9 +1097,9 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
             else
                 k_signature<false, uint16_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, cr, g->d_sig);
         } else if (g->weighted) {
-            k_signature<true, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
+            k_signature_auto<true><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
         } else {
-            k_signature<false, uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
+            k_signature_auto<false><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig);
         }
     }
     if (t) CK(cudaEventRecord(t->ev[2], s));

@@ -392,17 +392,24 @@ __device__ __forceinline__ void signature_fold(uint32_t lane, uint32_t a, uint32
     uint64_t pre1 = 0, cur1 = 0;
     uint32_t pre2 = 0, cur2 = 0;
     uint32_t nh = 0;
+    // running sums: a row's sum is the difference of the running sums at its
+    // two ends (wrap-around arithmetic); every arc adds unconditionally
+    uint64_t run1 = 0, last1 = 0;
+    uint32_t run2 = 0, last2 = 0;
 #pragma unroll
     for (int i = 0; i < kEdgesPerThread; ++i) {
         if ((uint32_t)i < cnt) {
             if ((hb >> i) & 1u) {
                 if (nh > 0) {
                     const uint32_t node = rows[kbase + nh];
-                    sig_store(&sig[node], cur1, cur2);
+                    sig_store(&sig[node], run1 - last1, run2 - last2);
+                } else {
+                    pre1 = run1;
+                    pre2 = run2;
                 }
+                last1 = run1;
+                last2 = run2;
                 ++nh;
-                cur1 = 0;
-                cur2 = 0;
             }
             uint64_t t1;
             uint32_t t2;
@@ -411,14 +418,16 @@ __device__ __forceinline__ void signature_fold(uint32_t lane, uint32_t a, uint32
                 t1 *= w[i];
                 t2 *= (uint32_t)w[i];
             }
-            if (nh == 0) {
-                pre1 += t1;
-                pre2 += t2;
-            } else {
-                cur1 += t1;
-                cur2 += t2;
-            }
+            run1 += t1;
+            run2 += t2;
         }
+    }
+    if (nh == 0) {
+        pre1 = run1;
+        pre2 = run2;
+    } else {
+        cur1 = run1 - last1;
+        cur2 = run2 - last2;
     }
 
     // warp inclusive segmented scan of the lanes' trailing parts (a
@@ -1891,19 +1900,22 @@ struct PersistArgs {
     uint32_t* joined;
 };
 
-// Signatures of the small tail, one row per lane: a warp takes 32 consecutive
-// rows of the active arc set; each lane folds its row's arcs four at a time
-// (rows of at most kRowLong arcs), and the rows longer than that are folded by the whole warp
-// afterwards, one at a time (a strided loop and a shuffle reduction).  The
-// sums are the tiled kernel's (wrap-around sums of the same per-arc terms, in
-// another order), and every row is written whole, with no atomics.  Few
-// registers: the persistent kernel that runs it keeps more warps resident than
-// one built around the 16-arcs-per-lane tile fold.  Colours are read at L2:
-// the same launch rewrites them between its phases.
+// Signatures one row per lane, for active sets of short rows (the small tail,
+// and a pass kernel's passes whose rows average at most 4 arcs): a warp takes
+// 32 consecutive rows of the active arc set; each lane folds its row's arcs
+// four at a time (rows of at most kRowLong arcs), and the rows longer than
+// that are folded by the whole warp afterwards, one at a time (a strided loop
+// and a shuffle reduction).  The sums are the tiled kernel's (wrap-around sums
+// of the same per-arc terms, in another order), and every row is written
+// whole, with no atomics.  Few registers: the persistent kernel that runs it
+// keeps more warps resident than one built around the 16-arcs-per-lane tile
+// fold.  NC false (the persistent kernel): colours are read at L2, since the
+// same launch rewrites them between its phases; a pass kernel reads them
+// through the read-only path.
 constexpr uint32_t kRowLong = 32;
 constexpr int kPersistBlocksPerSM = 4;  // 4 x 256 threads resident per SM (64 registers, no spills)
 
-template <bool WEIGHTED>
+template <bool WEIGHTED, bool NC = false>
 __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__ as, const uint32_t* __restrict__ col,
                                                    Sig* __restrict__ sig, uint64_t salt)
 {
@@ -1937,7 +1949,7 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
 #pragma unroll
                 for (int j = 0; j < 4; ++j) h[j] = a + j < e ? idx[a + j] : 0u;
 #pragma unroll
-                for (int j = 0; j < 4; ++j) c[j] = a + j < e ? __ldcg(col + h[j]) : 0u;
+                for (int j = 0; j < 4; ++j) c[j] = a + j < e ? gather_col<NC>(col + h[j]) : 0u;
 #pragma unroll
                 for (int j = 0; j < 4; ++j) {
                     if (a + j >= e) break;
@@ -1965,7 +1977,7 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
             for (uint64_t a = bb + lane; a < ee; a += 32) {
                 uint64_t t1;
                 uint32_t t2;
-                arc_terms(__ldcg(col + idx[a]), salt, t1, t2);
+                arc_terms(gather_col<NC>(col + idx[a]), salt, t1, t2);
                 if (WEIGHTED) {
                     const uint64_t w = wt[a];
                     t1 *= w;
@@ -1982,6 +1994,20 @@ __device__ __forceinline__ void row_signature_body(const ActiveSet* __restrict__
             if (lane == (uint32_t)src) sig_store(&sig[node], s1, s2);
         }
     }
+}
+
+// A pass's signatures by the shape of its active rows: one row per lane when
+// they are short (at most 4 arcs on average, where a tile fold's lanes would
+// each close several rows), else the 512-arc tile fold.  Both write the same
+// sums.
+template <bool WEIGHTED>
+static __global__ void __launch_bounds__(kTileThreads) k_signature_auto(const ActiveSet* __restrict__ as,
+                                                                        const RoundState* __restrict__ st,
+                                                                        const uint32_t* __restrict__ col,
+                                                                        Sig* __restrict__ sig)
+{
+    if (as->m <= 4ull * as->K) row_signature_body<WEIGHTED, true>(as, col, sig, pass_salt1(st->seed, st->round));
+    else signature_body<WEIGHTED, uint32_t>(as, st, col, sig);
 }
 
 // Per pass: [table clear when the stamp wrapped] + signatures | inserts |
