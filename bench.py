@@ -406,12 +406,17 @@ def run_ours(args, rank, world, local_rank):
     sig_bytes_all = sum(8 * p["arcs"] for p in per_pass) + len(per_pass) * n * (ob + 8)
     sig_ms_all = sum(p["signature_ms"] for p in per_pass)
     hot = results[0].first_signature_hot
-    kname = "k_signature_hot" if hot else "k_signature"
+    # the hot first pass by tensor copies (the default, sig_kernel 0 or 4) or
+    # by 16-byte loads (sig_kernel 3), as the options in effect choose
+    sigk = (tune or {}).get("best", {}).get("sig_kernel", 0)
+    kname = ("k_signature_hot_tma" if sigk in (0, 4) else "k_signature_hot") if hot else "k_signature"
     tpa = signature_traffic_per_arc(kname)
     round_bytes = 8 * m + n * (ob + 28)
     ach = sig_bytes_p1 / (sig_ms1 / 1e3) / 1e9
     kdesc = (f"{kname} (first pass: every arc; the class ranks of the {hot} most pointed-to nodes "
-             "read from shared memory)" if hot else f"{kname} (first pass: every arc)")
+             "read from shared memory" + ("; each warp's tile of heads brought into shared memory by the tensor "
+                                          "memory accelerator)" if kname == "k_signature_hot_tma" else ")")
+             if hot else f"{kname} (first pass: every arc)")
     roofline = {"bound": "hbm", "kernel": kdesc,
                 "achieved": ach, "peak": peak, "unit": "GB/s", "frac": ach / peak, "peak_kind": f"{peak_kind} hbm_gbs",
                 "traffic": None if tpa is None else tpa * arcs1,

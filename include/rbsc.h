@@ -77,12 +77,16 @@ typedef struct {
                                  (0 = default 22)                                       */
     int32_t grid_per_sm;      /* blocks per SM of the pass kernels' grids (0 = 16)      */
     int32_t sig_kernel;       /* signature kernel over device arcs: 0 = default (hot
-                                 heads where they apply, else plain loads), 1 = plain
+                                 heads where they apply, by tensor copies (4) when the
+                                 driver makes their tensor map, else plain loads), 1 = plain
                                  loads, 2 = staged (each warp's tiles copied to shared
                                  memory by cp.async.bulk; unweighted), 3 = hot heads:
                                  the first pass of a resident graph with >= 2^22 arcs
                                  and <= 256 initial classes reads the class ranks of
-                                 the most pointed-to nodes from shared memory          */
+                                 the most pointed-to nodes from shared memory, 4 = hot
+                                 heads with each warp's tile of heads brought into
+                                 shared memory by the tensor memory accelerator
+                                 (128-byte swizzled boxes)                              */
     int32_t hot_log2;         /* hot heads: at most 2^hot_log2 nodes, those with the
                                  most in-arcs (0 = default 17; 10..17)                  */
     int32_t persist_bps;      /* blocks of 256 threads per SM of the persistent tail
@@ -300,7 +304,7 @@ typedef struct {
     int32_t use_graph[RBSC_TUNE_MAX];     /* CUDA-graph loop 1 / host loop 0                */
     uint32_t n_use_graph;
     int32_t sig_kernel[RBSC_TUNE_MAX];    /* signature kernels to try (1 plain, 2 staged,
-                                             3 hot heads)                              */
+                                             3 hot heads, 4 hot heads by tensor copies) */
     uint32_t n_sig_kernel;
     uint32_t reps;                        /* timed refinements per candidate (0 = 3)         */
 } rbsc_tune_space;

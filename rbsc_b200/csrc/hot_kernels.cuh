@@ -22,6 +22,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "common.cuh"
 #include "refine_kernels.cuh"
@@ -129,6 +130,126 @@ static __global__ void __launch_bounds__(kHotThreads, 1)
     __syncthreads();
     signature_body<WEIGHTED, uint8_t, true, false, true, kHotThreads / 32>(
         as, st, rank, sig, TileRange{0u, 0u, nullptr, nullptr, 0ull}, hot_idx, s_hot);
+}
+
+// ---------------------------------------------------------------------------
+// k_signature_hot_tma: the hot first pass with each warp's tile of heads
+// brought into shared memory by the tensor memory accelerator instead of
+// 16-byte global loads.  The hot-head copy is viewed as a 2-D tensor of
+// 128-byte rows (32 heads); one tile (512 arcs) is a 16-row box, loaded with
+// the 128-byte swizzle: lane l reads its 16 heads (logical bytes 64l .. 64l+63)
+// as four 16-byte words whose physical offsets are the logical ones with bits
+// 4-6 XORed by bits 7-9, so the 32 lanes of each read spread over all banks
+// (4 wavefronts for 512 bytes).  The loads themselves take no L1 wavefronts.
+// One buffer per warp: a lane copies its heads into registers, the warp
+// synchronises, and lane 0 asks for the warp's next tile into the same
+// buffer, which then arrives while this tile's ranks are gathered and folded.
+// Waits are bounded (kErrStage).  Heads beyond the last arc of the last tile
+// are loaded from the padded copy and never used.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kTmaTileBytes = kTileEdges * 4u;  // 2 KB of heads: 16 rows of 128 B
+
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, uint32_t row, uint32_t bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(bar)
+        : "memory");
+}
+
+template <bool WEIGHTED>
+static __global__ void __launch_bounds__(kHotThreads, 1)
+    k_signature_hot_tma(const __grid_constant__ CUtensorMap heads, const ActiveSet* __restrict__ as,
+                        RoundState* __restrict__ st, const uint8_t* __restrict__ rank,
+                        const uint8_t* __restrict__ hot_rank, uint32_t hot_bytes, Sig* __restrict__ sig)
+{
+    constexpr uint32_t W = kHotThreads / 32;
+    extern __shared__ __align__(16) uint8_t s_dyn[];
+    __shared__ __align__(8) uint64_t s_bar[W];
+    // the staged table, then one 1024-byte aligned 2 KB buffer per warp (the
+    // 128-byte swizzle repeats every 1024 bytes of shared memory)
+    uint8_t* s_hot = s_dyn;
+    const uint32_t dyn = smem_u32(s_dyn);
+    const uint32_t stage0 = (dyn + hot_bytes + 1023u) & ~1023u;
+    const uint32_t lane = threadIdx.x & 31, wi = threadIdx.x >> 5;
+    const uint32_t stage = stage0 + wi * kTmaTileBytes;
+    const uint8_t* s_stage = s_dyn + (stage - dyn);
+    const uint32_t bar = smem_u32(&s_bar[wi]);
+    {
+        const uint4* __restrict__ src = reinterpret_cast<const uint4*>(hot_rank);
+        uint4* dst = reinterpret_cast<uint4*>(s_hot);
+        for (uint32_t i = threadIdx.x; i < hot_bytes / 16u; i += blockDim.x) dst[i] = src[i];
+    }
+    if (lane == 0) {
+        mbar_init(&s_bar[wi], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (*(const volatile uint32_t*)&st->error) return;
+
+    const uint32_t ntiles = as->ntiles;
+    const uint64_t m = as->m;
+    const uint32_t* __restrict__ rows = as->rows;
+    const uint32_t* __restrict__ tile_row = as->tile_row;
+    const uint8_t* __restrict__ head8 = as->head8;
+    const uint64_t* __restrict__ wt = as->wt;
+    const uint64_t salt = pass_salt1(st->seed, st->round);
+    const uint32_t warps = gridDim.x * W;
+    uint32_t tile = blockIdx.x * W + wi;
+    if (tile < ntiles && lane == 0) {
+        mbar_expect_tx(&s_bar[wi], kTmaTileBytes);
+        tma_load_tile(stage, &heads, tile * 16u, bar);
+    }
+    // this lane's four 16-byte words of the tile, at their swizzled offsets
+    uint32_t off[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint32_t o = lane * 64u + (uint32_t)j * 16u;
+        off[j] = o ^ (((o >> 7) & 7u) << 4);
+    }
+    uint32_t phase = 0;
+    for (; tile < ntiles; tile += warps) {
+        const bool ok = mbar_wait_bounded(&s_bar[wi], phase);
+        if (!__all_sync(0xffffffffu, ok)) {
+            if (lane == 0) atomicOr(&st->error, kErrStage);
+            return;
+        }
+        phase ^= 1u;
+        const uint4 q0 = *reinterpret_cast<const uint4*>(s_stage + off[0]);
+        const uint4 q1 = *reinterpret_cast<const uint4*>(s_stage + off[1]);
+        const uint4 q2 = *reinterpret_cast<const uint4*>(s_stage + off[2]);
+        const uint4 q3 = *reinterpret_cast<const uint4*>(s_stage + off[3]);
+        __syncwarp();
+        const uint32_t next = tile + warps;
+        if (next < ntiles && lane == 0) {
+            // the generic-proxy reads of the buffer above come before the
+            // asynchronous write of the next tile
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_expect_tx(&s_bar[wi], kTmaTileBytes);
+            tma_load_tile(stage, &heads, next * 16u, bar);
+        }
+        const uint64_t tbeg = (uint64_t)tile * kTileEdges;
+        const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
+        const uint64_t tend = tbeg + tlen;
+        const uint32_t k0 = tile_row[tile];
+        const uint32_t h0 = head8[tbeg >> 3] & 1u;
+        const uint32_t a = lane * kEdgesPerThread;
+        const uint32_t cnt = a < tlen ? min((uint32_t)kEdgesPerThread, tlen - a) : 0u;
+        uint32_t hb = cnt ? (uint32_t)*reinterpret_cast<const uint16_t*>(head8 + ((tbeg + a) >> 3)) : 0u;
+        if (cnt < (uint32_t)kEdgesPerThread) hb &= (1u << cnt) - 1u;
+        const uint32_t h[kEdgesPerThread] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w,
+                                             q2.x, q2.y, q2.z, q2.w, q3.x, q3.y, q3.z, q3.w};
+        uint32_t c[kEdgesPerThread];
+        uint64_t w[kEdgesPerThread];
+#pragma unroll
+        for (int i = 0; i < kEdgesPerThread; ++i)
+            c[i] = (uint32_t)i < cnt ? gather_head<true, uint8_t, true>(rank, s_hot, h[i]) : 0u;
+        if (WEIGHTED) {
+#pragma unroll
+            for (int i = 0; i < kEdgesPerThread; ++i) w[i] = (uint32_t)i < cnt ? __ldcs(wt + tbeg + a + i) : 0ull;
+        }
+        signature_fold<WEIGHTED>(lane, a, cnt, tlen, tend, m, k0, h0, hb, c, w, salt, rows, head8, sig);
+    }
 }
 
 }  // namespace rbsc

@@ -6,6 +6,7 @@
 #include <unordered_map>
 #include <vector>
 #include <algorithm>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "../../include/rbsc.h"
@@ -77,6 +78,9 @@ struct rbsc_graph {
     uint32_t hot_n = 0;              // hot slots
     uint32_t hot_bytes = 0;          // staged table: hot_n rounded up to 16
     int hot_state = 0;               // 0 not built, 1 built, -1 not applicable (no skew, no memory)
+    CUtensorMap hot_tmap{};          // d_hot_idx as rows of 128 B, 16-row boxes, 128-byte swizzle
+    bool hot_tma = false;            // hot_tmap encoded (k_signature_hot_tma can run)
+    int hot_tma_err = 0;             // why not: -1 no driver entry point, -2 too many rows, else the CUresult
     uint32_t hot_log2 = 0;           // the size limit it was built (or rejected) for
     bool hot_active = false;         // the running refinement's first pass uses it
     uint32_t* d_srank = nullptr;     // rank of the initial class claimed at each table slot

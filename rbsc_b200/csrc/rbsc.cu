@@ -803,7 +803,7 @@ static uint32_t hot_limit_log2(const rbsc_ctx* ctx)
 static bool hot_wanted(const rbsc_ctx* ctx, const rbsc_graph* g)
 {
     const int32_t k = ctx->opts.sig_kernel;
-    return (k == 0 || k == 3) && !g->host_arcs && !g->oneshot && !g->stream_upload && g->m >= (1ull << 22) && g->n > 1;
+    return (k == 0 || k == 3 || k == 4) && !g->host_arcs && !g->oneshot && !g->stream_upload && g->m >= (1ull << 22) && g->n > 1;
 }
 
 // In-degree threshold that at most `limit` nodes reach, from the binned
@@ -823,6 +823,52 @@ static uint32_t hot_threshold(const uint32_t* bins, uint64_t limit)
 // Builds the hot heads of a graph once per size limit: in-degrees, the
 // threshold, the slots, the encoded copy of the heads.  false (nothing kept)
 // when no node qualifies or device memory is short: the plain kernel runs.
+// cuTensorMapEncodeTiled from the driver, looked up once (the library links
+// the runtime statically, not libcuda).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
+                                  const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled()
+{
+    static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        return reinterpret_cast<EncodeTiledFn>(p);
+    }();
+    return fn;
+}
+
+// The hot-head copy as a tensor for k_signature_hot_tma: 32 heads (128 B) a
+// row, mpad / 32 rows, boxes of 16 rows (one 512-arc tile), 128-byte
+// swizzle.  Tile t is the box at row 16 t, an int32 coordinate.
+static bool encode_hot_tmap(rbsc_graph* g)
+{
+    g->hot_tma = false;
+    const EncodeTiledFn enc = encode_tiled();
+    const uint64_t rows = (uint64_t)g->ntiles * (kTileEdges / 32);
+    g->hot_tma_err = !enc ? -1 : -2;
+    if (!enc || !g->d_hot_idx || rows == 0 || rows >= (1ull << 31)) return false;
+    const cuuint64_t dims[2] = {32, rows};
+    const cuuint64_t strides[1] = {128};
+    const cuuint32_t box[2] = {32, kTileEdges / 32};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult r = enc(&g->hot_tmap, CU_TENSOR_MAP_DATA_TYPE_UINT32, 2, g->d_hot_idx, dims, strides, box, estr,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    g->hot_tma = r == CUDA_SUCCESS;
+    g->hot_tma_err = (int)r;
+    return g->hot_tma;
+}
+
+// Dynamic shared memory of k_signature_hot_tma: the staged table, 1 KB of
+// alignment slack, one 2 KB buffer per warp.
+static size_t hot_tma_smem(uint32_t hot_bytes) { return (size_t)hot_bytes + 1024 + (kHotThreads / 32) * kTmaTileBytes; }
+
 static rbsc_status build_hot(rbsc_ctx* ctx, rbsc_graph* g, bool* ready)
 {
     const uint32_t lim = hot_limit_log2(ctx);
@@ -894,6 +940,15 @@ static rbsc_status build_hot(rbsc_ctx* ctx, rbsc_graph* g, bool* ready)
     CK(cudaGetLastError());
     CK(cudaFuncSetAttribute(k_signature_hot<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1 << kHotMaxLog2));
     CK(cudaFuncSetAttribute(k_signature_hot<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 1 << kHotMaxLog2));
+    if (encode_hot_tmap(g)) {
+        const int smax = (int)hot_tma_smem(1u << kHotMaxLog2);
+        if (cudaFuncSetAttribute(k_signature_hot_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess ||
+            cudaFuncSetAttribute(k_signature_hot_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smax) != cudaSuccess) {
+            cudaGetLastError();
+            g->hot_tma = false;
+            g->hot_tma_err = -3;
+        }
+    }
     CK(cudaStreamSynchronize(s));
     drop();
     g->hot_n = hot_n;
@@ -1075,6 +1130,20 @@ static rbsc_status launch_pass(rbsc_ctx* ctx, rbsc_graph* g, cudaStream_t s, cud
                     g->d_as, g->d_st, reinterpret_cast<const uint16_t*>(g->d_rank), g->d_sig, all, 0);
             else
                 k_signature_staged<uint32_t><<<blocks, kTileThreads, 0, s>>>(g->d_as, g->d_st, g->d_col[0], g->d_sig, all, 0);
+        } else if (first == kPassRank8 && g->hot_active && (ctx->opts.sig_kernel == 4 || (ctx->opts.sig_kernel == 0 && g->hot_tma))) {
+            // the default when the tensor map could be made; asked for
+            // explicitly, its absence is an error
+            if (!g->hot_tma)
+                return rbsc_fail(ctx, RBSC_ERR_CUDA, "sig_kernel 4: no tensor map for the hot heads (%d)", g->hot_tma_err);
+            const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
+            const unsigned hgrid = std::min<unsigned>((unsigned)ctx->sm_count, ceil_div<uint32_t>(g->ntiles, kHotThreads / 32));
+            const size_t smem = hot_tma_smem(g->hot_bytes);
+            if (g->weighted)
+                k_signature_hot_tma<true><<<hgrid, kHotThreads, smem, s>>>(g->hot_tmap, g->d_as, g->d_st, cr, g->d_hot_rank,
+                                                                           g->hot_bytes, g->d_sig);
+            else
+                k_signature_hot_tma<false><<<hgrid, kHotThreads, smem, s>>>(g->hot_tmap, g->d_as, g->d_st, cr, g->d_hot_rank,
+                                                                            g->hot_bytes, g->d_sig);
         } else if (first == kPassRank8 && g->hot_active) {
             const uint8_t* cr = reinterpret_cast<const uint8_t*>(g->d_rank);
             const unsigned hgrid = std::min<unsigned>((unsigned)ctx->sm_count, ceil_div<uint32_t>(g->ntiles, kHotThreads / 32));
@@ -1893,6 +1962,7 @@ extern "C" void rbsc_tune_space_default(rbsc_tune_space* sp)
     sp->sig_kernel[sp->n_sig_kernel++] = 1;
     sp->sig_kernel[sp->n_sig_kernel++] = 2;
     sp->sig_kernel[sp->n_sig_kernel++] = 3;
+    sp->sig_kernel[sp->n_sig_kernel++] = 4;
     sp->reps = 3;
 }
 

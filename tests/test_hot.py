@@ -50,11 +50,28 @@ def test_hot_heads_equal_the_oracle(rmat18, weighted):
         _same(r, ex)
 
 
+@pytest.mark.parametrize("weighted", [False, True], ids=["unweighted", "weighted"])
+def test_hot_heads_by_tensor_copies_equal_the_oracle(rmat18, weighted):
+    """sig_kernel 4: each warp's tile of heads is brought into shared memory
+    by the tensor memory accelerator (128-byte swizzled boxes); the last tile
+    is partial (the arc count is not a multiple of 512)."""
+    off, idx = rmat18
+    assert len(idx) % 512 != 0
+    wt = np.random.default_rng(5).integers(1, 4, len(idx), dtype=np.uint64) if weighted else None
+    init = R.degree_bucket_colors(off)
+    ex = oracle.refine_exact(off, idx, wt, init)
+    t1, t2 = _resident(off, idx, wt, init, sig_kernel=4)
+    assert 0 < t1.first_signature_hot <= (1 << 17)
+    for r in (t1, t2):
+        _same(r, ex)
+
+
+@pytest.mark.parametrize("sig_kernel", [3, 4])
 @pytest.mark.parametrize("hot_log2", [10, 13, 17])
-def test_hot_table_sizes(rmat18, hot_log2):
+def test_hot_table_sizes(rmat18, hot_log2, sig_kernel):
     off, idx = rmat18
     init = R.degree_bucket_colors(off)
-    h, _ = _resident(off, idx, None, init, sig_kernel=3, hot_log2=hot_log2)
+    h, _ = _resident(off, idx, None, init, sig_kernel=sig_kernel, hot_log2=hot_log2)
     p, _ = _resident(off, idx, None, init, sig_kernel=1)
     assert 0 < h.first_signature_hot <= (1 << hot_log2)
     assert np.array_equal(h.labels, p.labels) and h.rounds == p.rounds and h.blocks == p.blocks
