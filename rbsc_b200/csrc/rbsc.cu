@@ -820,9 +820,6 @@ static uint32_t hot_threshold(const uint32_t* bins, uint64_t limit)
     return thr;
 }
 
-// Builds the hot heads of a graph once per size limit: in-degrees, the
-// threshold, the slots, the encoded copy of the heads.  false (nothing kept)
-// when no node qualifies or device memory is short: the plain kernel runs.
 // cuTensorMapEncodeTiled from the driver, looked up once (the library links
 // the runtime statically, not libcuda).
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*, const cuuint64_t*,
@@ -869,6 +866,10 @@ static bool encode_hot_tmap(rbsc_graph* g)
 // alignment slack, one 2 KB buffer per warp.
 static size_t hot_tma_smem(uint32_t hot_bytes) { return (size_t)hot_bytes + 1024 + (kHotThreads / 32) * kTmaTileBytes; }
 
+// Builds the hot heads of a graph once per size limit: in-degrees, the
+// threshold, the slots, the encoded copy of the heads.  false (nothing kept)
+// when no node qualifies or device memory is short: the plain kernel runs.
+// The tensor map of the copy is made here too (k_signature_hot_tma).
 static rbsc_status build_hot(rbsc_ctx* ctx, rbsc_graph* g, bool* ready)
 {
     const uint32_t lim = hot_limit_log2(ctx);
