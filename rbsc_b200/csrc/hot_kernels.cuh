@@ -149,11 +149,21 @@ static __global__ void __launch_bounds__(kHotThreads, 1)
 // ---------------------------------------------------------------------------
 constexpr uint32_t kTmaTileBytes = kTileEdges * 4u;  // 2 KB of heads: 16 rows of 128 B
 
-__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, uint32_t row, uint32_t bar)
+// The heads are read once per pass: the copies carry an evict-first L2
+// policy (as the 16-byte loads' .cs), so the stream of heads does not push
+// the class ranks and the signatures out of L2.
+__device__ __forceinline__ uint64_t l2_evict_first_policy()
+{
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ void tma_load_tile(uint32_t dst, const CUtensorMap* map, uint32_t row, uint32_t bar, uint64_t policy)
 {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(bar)
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, %3}], [%4], %5;" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(row), "r"(bar), "l"(policy)
         : "memory");
 }
 
@@ -196,9 +206,10 @@ static __global__ void __launch_bounds__(kHotThreads, 1)
     const uint64_t salt = pass_salt1(st->seed, st->round);
     const uint32_t warps = gridDim.x * W;
     uint32_t tile = blockIdx.x * W + wi;
+    const uint64_t policy = l2_evict_first_policy();
     if (tile < ntiles && lane == 0) {
         mbar_expect_tx(&s_bar[wi], kTmaTileBytes);
-        tma_load_tile(stage, &heads, tile * 16u, bar);
+        tma_load_tile(stage, &heads, tile * 16u, bar, policy);
     }
     // this lane's four 16-byte words of the tile, at their swizzled offsets
     uint32_t off[4];
@@ -226,7 +237,7 @@ static __global__ void __launch_bounds__(kHotThreads, 1)
             // asynchronous write of the next tile
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             mbar_expect_tx(&s_bar[wi], kTmaTileBytes);
-            tma_load_tile(stage, &heads, next * 16u, bar);
+            tma_load_tile(stage, &heads, next * 16u, bar, policy);
         }
         const uint64_t tbeg = (uint64_t)tile * kTileEdges;
         const uint32_t tlen = (uint32_t)min((uint64_t)kTileEdges, m - tbeg);
