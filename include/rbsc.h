@@ -442,7 +442,10 @@ rbsc_status rbsc_graph_batch_refine(rbsc_ctx* ctx, rbsc_graph* g, const uint64_t
  * it is started together with the other small jobs waiting behind it, up to
  * pack_max_graphs jobs and pack_arc_budget arcs, as one batch refinement of
  * their disjoint union (rbsc_batch_refine): every job still gets exactly the
- * labels and block count a refinement of its graph alone gives.
+ * labels and block count a refinement of its graph alone gives.  With two or
+ * more slots, large jobs occupy at most all slots but one while small jobs
+ * wait: when every other slot runs a large job, the idle one goes to the
+ * oldest small job before the oldest large one.
  *
  * A job's host buffers (CSR, initial colours, output labels) belong to the
  * caller and must stay valid and unchanged until the job's result has been

@@ -8,7 +8,12 @@
 // whenever an executor finishes:
 //
 //   while an executor is idle and jobs wait:
-//     head = the oldest waiting job
+//     head = the oldest waiting job; but when head is large, every other
+//            executor runs a large job and a small job waits, head = the
+//            oldest small job (a lane for small jobs: with two or more
+//            executors, large jobs hold at most all but one while small jobs
+//            wait, so a burst of large jobs does not hold up the small ones;
+//            large jobs still start in arrival order as executors free up)
 //     head small -> take it and the small jobs waiting behind it, in arrival
 //                   order (large ones are passed over), up to the pack limits
 //     otherwise  -> take head alone
@@ -86,6 +91,7 @@ struct Slot {
     std::thread th;
     std::condition_variable cv;
     bool busy = false;            // work handed over and not finished
+    bool large = false;           // the work is one large job
     std::vector<Job*> work;
     uint64_t footprint = 0;
     void* stage = nullptr;        // pinned staging of packed batches
@@ -104,6 +110,7 @@ struct rbsc_server {
     uint64_t next_id = 1;
     bool stopping = false;
     uint32_t busy = 0;
+    uint32_t busy_large = 0;      // executors running one large job
     rbsc_serve_stats st{};
 };
 
@@ -312,7 +319,9 @@ void slot_main(rbsc_server* srv, Slot* sl)
         srv->st.reserved -= fp;
         srv->st.running -= work.size();
         --srv->busy;
+        if (sl->large) --srv->busy_large;
         sl->busy = false;
+        sl->large = false;
         dispatch(srv);
         srv->cv_done.notify_all();
     }
@@ -325,11 +334,20 @@ void dispatch(rbsc_server* srv)
     for (Slot* sl : srv->slots) {
         if (sl->busy) continue;
         if (srv->queue.empty()) return;
-        Job* head = srv->queue.front();
-        std::vector<size_t> take{0};
+        size_t h = 0;  // queue position of the work's first job
+        if (!srv->queue.front()->small && srv->slots.size() >= 2 && srv->busy_large + 1 >= srv->slots.size()) {
+            // the last executor goes to the oldest small job, if one waits
+            for (size_t i = 1; i < srv->queue.size(); ++i)
+                if (srv->queue[i]->small) {
+                    h = i;
+                    break;
+                }
+        }
+        Job* head = srv->queue[h];
+        std::vector<size_t> take{h};
         std::vector<uint64_t> cn{head->g.n}, cm{head->g.m};  // running totals
         if (head->small && srv->o.pack_max_graphs > 1) {
-            for (size_t i = 1; i < srv->queue.size() && take.size() < srv->o.pack_max_graphs; ++i) {
+            for (size_t i = h + 1; i < srv->queue.size() && take.size() < srv->o.pack_max_graphs; ++i) {
                 const Job* j = srv->queue[i];
                 if (!j->small) continue;
                 if (cm.back() + j->g.m > srv->o.pack_arc_budget || cn.back() + j->g.n > srv->o.pack_arc_budget) continue;
@@ -345,7 +363,7 @@ void dispatch(rbsc_server* srv)
             fp = rbsc_serve_footprint(cn[k - 1], cm[k - 1], head->g.weights != nullptr, (uint32_t)k);
             if (srv->st.reserved + fp <= srv->o.hbm_budget) break;
         }
-        if (k == 0) return;  // the oldest job waits for memory
+        if (k == 0) return;  // the chosen job waits for memory (nothing else overtakes it)
         take.resize(k);
         std::vector<Job*> work;
         work.reserve(k);
@@ -370,6 +388,8 @@ void dispatch(rbsc_server* srv)
         if (work.size() > 1) srv->st.packed_jobs += work.size();
         ++srv->busy;
         srv->st.peak_busy_slots = std::max(srv->st.peak_busy_slots, srv->busy);
+        sl->large = !head->small;
+        if (sl->large) ++srv->busy_large;
         sl->work.swap(work);
         sl->footprint = fp;
         sl->busy = true;

@@ -85,6 +85,30 @@ def test_large_jobs_are_not_packed(er2k):
             assert r.packed == 1
 
 
+def test_small_jobs_do_not_wait_behind_a_burst_of_large_ones():
+    """With every executor but one running a large job, the last one goes to
+    the small jobs that wait, before the next large job (which still starts
+    as soon as they leave it free).  Two executors: a short large job, a long
+    large job, then a third large job and three small ones."""
+    short_l = R.gen_er_host(1000, 4.0, seed=21)
+    long_l = R.gen_er_host(10000, 4.0, seed=22)
+    big = R.gen_er_host(2000, 4.0, seed=23)
+    tiny = R.gen_er_host(30, 2.0, seed=24)
+    with R.Server(slots=2, pack_max_arcs=1 << 10, pack_max_graphs=8, dry_run_ns_per_arc=2000) as srv:
+        t_sub, ids = [], []
+        for off, idx in (short_l, long_l, big, tiny, tiny, tiny):
+            t_sub.append(time.perf_counter() * 1e3)
+            ids.append(srv.submit(off, idx))
+        res = [srv.wait(i) for i in ids]
+    assert all(r.status == 0 for r in res)
+    start = [t + r.queue_ms for t, r in zip(t_sub, res)]
+    assert res[2].packed == 1 and all(r.packed >= 1 for r in res[3:])
+    # the small jobs started before the third large job, which did not wait
+    # for the long one to finish
+    assert max(start[3:]) < start[2]
+    assert start[2] < start[1] + res[1].service_ms
+
+
 def test_weighted_jobs_run_alone():
     off, idx = R.gen_er_host(60, 2.0, seed=3)
     wt = np.ones(len(idx), dtype=np.uint64)
