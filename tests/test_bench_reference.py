@@ -81,3 +81,17 @@ def test_cpu_baseline_has_the_reference_and_an_all_cores_port():
     if c["kind"] == "reference":
         assert c["cores"] == 1 and len(c["round_s"]) == 2
         assert p["rounds"] == c["rsc_own_timer"]["rounds"] and p["blocks"] == c["rsc_own_timer"]["blocks"]
+
+
+def test_roofline_traffic_is_committed_for_every_first_pass_kernel():
+    """The bench's roofline `traffic` comes from the committed R-MAT-24 ncu
+    summary of the first pass's kernel (profiles/<kernel>_rmat24.md, line
+    'traffic_bytes_per_arc: X'): each kernel the bench can name has one, with
+    a per-arc figure in the range a gather of 1-byte ranks over 4-byte heads
+    gives (below the 8 algorithmic bytes per arc)."""
+    sys.path.insert(0, ROOT)
+    import bench
+    for kernel in ("k_signature", "k_signature_hot", "k_signature_hot_tma"):
+        tpa = bench.signature_traffic_per_arc(kernel)
+        assert tpa is not None, kernel
+        assert 4.0 < tpa < 8.0, (kernel, tpa)
