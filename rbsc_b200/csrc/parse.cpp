@@ -65,25 +65,23 @@ struct Run {
     uint64_t at, cnt, row_at;
 };
 
-// One thread's share of the lines.  Heads in input order, sources as runs,
-// weights only from the first weight other than 1 on (earlier ones are 1).
+// One thread's share of the lines.  Heads in input order, written straight
+// into the shared heads array at the chunk's line offset (dst, cap lines of
+// room); sources as runs; weights only from the first weight other than 1 on
+// (earlier ones are 1).
 struct Chunk {
-    uint32_t* dst = nullptr;
+    uint32_t* dst = nullptr;  // not owned: a stretch of the heads array
+    uint64_t cap = 0;         // lines in the chunk: an upper bound of its arcs
     uint64_t* wt = nullptr;
     uint64_t n = 0;
     std::vector<Run> runs;
     bool ok = true;
     std::string err;
-    ~Chunk()
-    {
-        std::free(dst);
-        std::free(wt);
-    }
+    ~Chunk() { std::free(wt); }
 };
 
-void parse_chunk(Chunk& c, const char* q, const char* e, uint64_t N)
+uint64_t count_lines(const char* q, const char* e)
 {
-    // lines in the chunk: an upper bound of its arcs
     uint64_t cap = 1;
     for (const char* r = q; r < e;) {
         const void* nl = std::memchr(r, '\n', (size_t)(e - r));
@@ -91,12 +89,12 @@ void parse_chunk(Chunk& c, const char* q, const char* e, uint64_t N)
         ++cap;
         r = static_cast<const char*>(nl) + 1;
     }
-    c.dst = static_cast<uint32_t*>(std::malloc(sizeof(uint32_t) * cap));
-    if (!c.dst) {
-        c.ok = false;
-        c.err = "out of host memory";
-        return;
-    }
+    return cap;
+}
+
+void parse_chunk(Chunk& c, const char* q, const char* e, uint64_t N)
+{
+    const uint64_t cap = c.cap;
     uint64_t cur = UINT64_MAX;
     while (q < e) {
         // skip blank lines
@@ -175,31 +173,48 @@ extern "C" rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_g
         while (q < end && *(q - 1) != '\n') ++q;
         cut[t] = q;
     }
+    // every chunk parses into its own stretch of one heads array, at its
+    // first line's position: input already in source order (the usual case)
+    // is then the CSR's heads without a copy
     std::vector<Chunk> ch(T);
+    parallel_for(T, [&](int t) { ch[t].cap = count_lines(cut[t], cut[t + 1]); });
+    uint64_t lines = 0;
+    std::vector<uint64_t> at(T, 0);
+    for (int t = 0; t < T; ++t) {
+        at[t] = lines;
+        lines += ch[t].cap;
+    }
+    uint32_t* heads = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(lines, 1));
+    if (!heads) return rbsc_fail(nullptr, RBSC_ERR_OOM, "out of host memory");
+    for (int t = 0; t < T; ++t) ch[t].dst = heads + at[t];
     parallel_for(T, [&](int t) { parse_chunk(ch[t], cut[t], cut[t + 1], N); });
     uint64_t total = 0;
     bool unit = true;
     std::vector<uint64_t> base(T + 1, 0);
     for (int t = 0; t < T; ++t) {
-        if (!ch[t].ok) return rbsc_fail(nullptr, ch[t].err == "out of host memory" ? RBSC_ERR_OOM : RBSC_ERR_PARSE, "%s",
-                                        ch[t].err.c_str());
+        if (!ch[t].ok) {
+            std::free(heads);
+            return rbsc_fail(nullptr, ch[t].err == "out of host memory" ? RBSC_ERR_OOM : RBSC_ERR_PARSE, "%s",
+                             ch[t].err.c_str());
+        }
         base[t] = total;
         total += ch[t].n;
         unit = unit && !ch[t].wt;
     }
     base[T] = total;
-    if (total != M)
+    if (total != M) {
+        std::free(heads);
         return rbsc_fail(nullptr, RBSC_ERR_PARSE, "header announces %llu arcs, input holds %llu", (unsigned long long)M,
                          (unsigned long long)total);
+    }
 
     // arcs must be grouped by source: every source starts exactly one run
     // (a run cut by a chunk boundary continues in the next chunk)
     uint64_t* off = (uint64_t*)std::calloc(N + 1, sizeof(uint64_t));
-    uint32_t* idx = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(M, 1));
     uint64_t* wt = unit ? nullptr : (uint64_t*)std::malloc(sizeof(uint64_t) * std::max<uint64_t>(M, 1));
     std::vector<uint8_t> seen(N, 0);
-    if (!off || !idx || (!unit && !wt)) {
-        std::free(off); std::free(idx); std::free(wt);
+    if (!off || (!unit && !wt)) {
+        std::free(off); std::free(heads); std::free(wt);
         return rbsc_fail(nullptr, RBSC_ERR_OOM, "out of host memory");
     }
     int64_t prev = -1;
@@ -213,7 +228,7 @@ extern "C" rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_g
                 continue;
             }
             if (seen[r.u]) {
-                std::free(off); std::free(idx); std::free(wt);
+                std::free(off); std::free(heads); std::free(wt);
                 return rbsc_fail(nullptr, RBSC_ERR_PARSE, "arcs of node %u are not contiguous (input must be grouped by source)", r.u);
             }
             seen[r.u] = 1;
@@ -225,11 +240,23 @@ extern "C" rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_g
     for (uint64_t u = 0; u < N; ++u) off[u + 1] += off[u];
 
     // heads (and weights) to their rows: in source order the input already is
-    // the CSR, chunk by chunk; otherwise run by run
+    // the CSR, chunk by chunk (the heads stay where they were parsed; chunks
+    // with blank lines left gaps, closed in chunk order, each stretch moving
+    // towards the front); otherwise run by run into a new array
+    uint32_t* idx = heads;
+    if (sorted) {
+        for (int t = 0; t < T; ++t)
+            if (ch[t].n && heads + base[t] != ch[t].dst) std::memmove(heads + base[t], ch[t].dst, sizeof(uint32_t) * ch[t].n);
+    } else {
+        idx = (uint32_t*)std::malloc(sizeof(uint32_t) * std::max<uint64_t>(M, 1));
+        if (!idx) {
+            std::free(off); std::free(heads); std::free(wt);
+            return rbsc_fail(nullptr, RBSC_ERR_OOM, "out of host memory");
+        }
+    }
     parallel_for(T, [&](int t) {
         const Chunk& c = ch[t];
         if (sorted) {
-            if (c.n) std::memcpy(idx + base[t], c.dst, sizeof(uint32_t) * c.n);
             if (wt)
                 for (uint64_t i = 0; i < c.n; ++i) wt[base[t] + i] = c.wt ? c.wt[i] : 1u;
             return;
@@ -241,6 +268,7 @@ extern "C" rbsc_status rbsc_parse_arcs(const char* text, size_t len, rbsc_host_g
                 for (uint64_t i = 0; i < r.cnt; ++i) wt[to + i] = c.wt ? c.wt[from + i] : 1u;
         }
     });
+    if (!sorted) std::free(heads);
     out->n = (uint32_t)N;
     out->m = M;
     out->offsets = off;

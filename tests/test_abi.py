@@ -207,3 +207,30 @@ def test_csr_cache_reads_version_1_files(tmp_path):
     open(p, "wb").write(head + payload)
     with pytest.raises(R.RbscError):
         R.load_csr(p)
+
+
+@pytest.mark.parametrize("weighted", [False, True], ids=["unit", "weighted"])
+def test_parse_large_sorted_input_with_blank_lines(weighted):
+    """More than 1 MB of text in source order, parsed by several threads
+    straight into the heads array, with blank (and blank-looking) lines
+    sprinkled through every chunk: the gaps they leave are closed and the CSR
+    equals the one without them."""
+    rng = np.random.default_rng(8)
+    n = 60000
+    rows = [(u, rng.integers(0, n, size=int(rng.integers(1, 9)))) for u in range(n)]
+    wfun = (lambda u, j: (u + j) % 3 + 1) if weighted else None
+    lines = _arcs_text(n, rows, wfun).decode().split("\n")
+    body = []
+    for k, ln in enumerate(lines[2:]):
+        body.append(ln)
+        if k % 97 == 0:
+            body.append("" if k % 2 else "  \t")
+    text = ("\n".join(lines[:2] + body)).encode()
+    assert len(text) > (1 << 20)
+    off, idx, wt = R.parse_arcs(text)
+    eo, ei, ew = _csr_of(n, rows, wfun)
+    assert np.array_equal(off, eo) and np.array_equal(idx, ei)
+    if weighted:
+        assert np.array_equal(wt, ew)
+    else:
+        assert wt is None
